@@ -1,0 +1,360 @@
+"""Benchmark: spectral paths/s of the hdcx CUDA integrator on B200.
+
+One step = one Render call of the 1.0M-triangle heavy-geometry workload
+(1920x1080, 64 spp, 8 bounces, lat-long HDR dome; seeded synthetic scene, see
+hdcodex_b200/workloads.py): 398,131,200 spectral paths (pixels x spp x 3
+wavelength lanes). With N ranks every rank renders its own sample range of the
+same frame on its own GPU (weak scaling, no collective on the data path).
+
+Printed JSON line:
+  value       - spectral paths/s of all ranks, device time of the K timed
+                renders (CUDA events on the tracer's stream, max over ranks),
+                scene and image resident in HBM;
+  e2e         - the same metric through the C ABI call a caller makes
+                (hdcx_render) with the image copied to a pinned host buffer
+                every step, wall clock around the call;
+  roofline    - the closest-hit traversal kernel: algorithmic bytes per ray
+                (32 B ray + 16 B hit + 80 B per wide node visited + 36 B per
+                triangle tested, visits counted by a counting pass) over its
+                CUDA-event time, against the measured HBM copy bandwidth;
+  cpu_baseline- the CPU oracle on the host cores on a centre crop.
+`--impl reference` times the CPU restatement of the reference integrator (the
+oracle) on the same workload and metric, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "spectral paths/s"
+UNIT = "spectral paths/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hdcx", choices=["hdcx", "reference"])
+    ap.add_argument("--workload", default="heavy", choices=["heavy", "box"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name):
+    from hdcodex_b200 import workloads
+    if name == "box":
+        return workloads.closed_box()
+    return workloads.heavy_geometry()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def traffic_from_profile():
+    """dram bytes per closest-hit launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "extend_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        cmd = ["nvidia-smi", "-i", str(self.index),
+               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+               "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(s[0]) for s in self.samples if num(s[0])]
+        mx = [num(s[1]) for s in self.samples if num(s[1])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier_sync(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(value, world):
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(wl, target_seconds, rank0=True):
+    """The oracle on the host cores over a centre crop, sized to ~target_seconds."""
+    import oracle as O
+    O.build()
+    t = O.OracleTracer()
+    t.set_scene(wl.scene)
+    threads = os.cpu_count() or 1
+    cx, cy = wl.width // 2, wl.height // 2
+    side = 16
+    t0 = time.perf_counter()
+    t.render(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp,
+             crop=(cx - side // 2, cy - side // 2, cx + side // 2, cy + side // 2), threads=threads)
+    calib = max(time.perf_counter() - t0, 1e-3)
+    rate = side * side / calib
+    side = int(max(16, min(wl.width, wl.height, (rate * target_seconds) ** 0.5)))
+    x0, y0 = cx - side // 2, cy - side // 2
+    t0 = time.perf_counter()
+    t.render(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp, crop=(x0, y0, x0 + side, y0 + side),
+             threads=threads)
+    secs = time.perf_counter() - t0
+    paths = side * side * wl.spp * 3
+    ext, sh, ss = t.last_counters
+    return {"value": paths / secs, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{side}x{side} centre crop of the {wl.width}x{wl.height} frame at {wl.spp} spp "
+                      f"({paths} spectral paths, {secs:.1f} s)",
+            "rays_per_s": (ext + sh + ss) / secs}
+
+
+def run_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return  # rank 0 alone times the CPU reference
+    wl = make_workload(args.workload)
+    import oracle as O
+    O.build()
+    t = O.OracleTracer()
+    t.set_scene(wl.scene)
+    threads = os.cpu_count() or 1
+    side = 32
+    cx, cy = wl.width // 2, wl.height // 2
+    crop = (cx - side // 2, cy - side // 2, cx + side // 2, cy + side // 2)
+    for i in range(args.warmup):
+        t.render(wl.camera, wl.width, wl.height, i * wl.spp, wl.max_bounces, wl.spp, crop=crop, threads=threads)
+    times = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        t.render(wl.camera, wl.width, wl.height, (args.warmup + i) * wl.spp, wl.max_bounces, wl.spp, crop=crop,
+                 threads=threads)
+        times.append(time.perf_counter() - t0)
+    paths = side * side * wl.spp * 3 * args.steps
+    value = paths / sum(times)
+    sample = f"{side}x{side} centre crop of the {wl.width}x{wl.height} frame at {wl.spp} spp per step"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
+                   "max_bounces": wl.max_bounces},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_hdcx(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    from hdcodex_b200 import PathTracer, workloads
+    from hdcodex_b200.tracer import PROFILE_COUNT_TRAVERSAL, PROFILE_STAGE_TIMES
+
+    wl = make_workload(args.workload)
+    tracer = PathTracer(local)
+    tracer.set_scene(wl.scene)
+    tri_count = workloads.triangle_count(wl.scene)
+    paths_per_step = wl.spectral_paths
+
+    def sample_index(step):
+        return (step * world + rank) * wl.spp
+
+    # Warm-up, then one counting pass for the roofline's algorithmic bytes.
+    for i in range(args.warmup):
+        tracer.render_device(wl.camera, wl.width, wl.height, sample_index(i), wl.max_bounces, wl.spp)
+    tracer.set_profiling(PROFILE_COUNT_TRAVERSAL)
+    tracer.render_device(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp)
+    counted = tracer.stats()
+    tracer.set_profiling(PROFILE_STAGE_TIMES)
+
+    # Timed region 1: device time, image resident in HBM.
+    sampler = ClockSampler(local)
+    barrier_sync(world)
+    sampler.start()
+    wall0 = time.perf_counter()
+    render_ms, extend_ms, extend_launches, ext_rays, sh_rays, ss_rays, launches = 0.0, 0.0, 0, 0, 0, 0, 0
+    for i in range(args.steps):
+        tracer.render_device(wl.camera, wl.width, wl.height, sample_index(args.warmup + i), wl.max_bounces, wl.spp)
+        st = tracer.stats()
+        render_ms += st["render_ms"]
+        extend_ms += st["extend_ms"]
+        extend_launches += st["extend_launches"]
+        ext_rays += st["extension_rays"]
+        sh_rays += st["shadow_rays"]
+        ss_rays += st["subsurface_rays"]
+        launches += st["kernel_launches"]
+    barrier_sync(world)
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop()
+    tracer.set_profiling(0)
+    total_ms = max_over_ranks(render_ms, world)
+    value = paths_per_step * world * args.steps / (total_ms / 1000.0)
+
+    # Timed region 2: end to end through hdcx_render with a pinned host image.
+    host = torch.empty((wl.height, wl.width, 4), dtype=torch.float32, pin_memory=True)
+    for i in range(max(1, args.warmup)):
+        tracer.render(wl.camera, wl.width, wl.height, sample_index(i), wl.max_bounces, wl.spp, out=host.data_ptr())
+    barrier_sync(world)
+    e2e_wall = 0.0
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        tracer.render(wl.camera, wl.width, wl.height, sample_index(args.warmup + i), wl.max_bounces, wl.spp,
+                      out=host.data_ptr())
+        e2e_wall += time.perf_counter() - t0
+    barrier_sync(world)
+    e2e_wall = max_over_ranks(e2e_wall, world)
+    e2e_value = paths_per_step * world * args.steps / e2e_wall
+    image = host.numpy()
+    finite = bool(np.isfinite(image).all())
+
+    # Roofline of the closest-hit traversal kernel.
+    rays_c = max(counted["extension_rays"], 1)
+    nodes_per_ray = counted["extension_node_visits"] / rays_c
+    tris_per_ray = counted["extension_triangle_tests"] / rays_c
+    bytes_per_ray = 32 + 16 + 80 * nodes_per_ray + 36 * tris_per_ray
+    achieved_gbs = ext_rays * bytes_per_ray / (extend_ms / 1000.0) / 1e9 if extend_ms > 0 else None
+    peak, peak_kind = measured_peaks()
+    traffic = traffic_from_profile()
+    roofline = {
+        "kernel": "extendKernel (closest-hit traversal)",
+        "bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+        "frac": (achieved_gbs / peak) if achieved_gbs else None, "peak_source": peak_kind,
+        "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+        "algorithmic_bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray,
+        "triangles_per_ray": tris_per_ray, "extend_ms_per_step": extend_ms / args.steps,
+        "extend_launches_per_step": extend_launches / args.steps,
+        "extend_share_of_step": extend_ms / render_ms if render_ms else None,
+    }
+
+    baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            baseline = cpu_baseline(wl, args.cpu_seconds)
+        except Exception as exc:  # the baseline is reported, never required
+            baseline = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                        "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl.name, "triangles": tri_count, "width": wl.width, "height": wl.height,
+                       "spp": wl.spp, "max_bounces": wl.max_bounces, "spectral_lanes": 3,
+                       "spectral_paths_per_step_per_gpu": paths_per_step,
+                       "l2": "inputs larger than L2 (scene + BVH + dome + per-wave path state)",
+                       "parallelism": f"replicas x{world}, disjoint sample ranges"},
+            "rays_per_s": (ext_rays + sh_rays + ss_rays) * world / (total_ms / 1000.0),
+            "extension_rays_per_step": ext_rays / args.steps, "shadow_rays_per_step": sh_rays / args.steps,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48,
+                    "d2h_bytes_per_step": wl.width * wl.height * 16, "image_finite": finite},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "cpu_baseline": baseline,
+            "clocks": clocks,
+            "wall_s_timed": wall,
+        }
+        print(json.dumps(line), flush=True)
+    tracer.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_hdcx(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,504 @@
+// bvh_build.cu - on-GPU BVH construction for the hdcx tracer.
+//
+// Replaces the closed driver build behind vkCmdBuildAccelerationStructuresKHR
+// (src/gpu/vulkan_path_tracer.cpp:3032-3127: one BLAS over all flattened
+// triangles, one identity TLAS). Steps, all on the device:
+//   1. triangle boxes and the scene box;
+//   2. 63-bit Morton codes of the box centres, sorted with their triangle ids;
+//   3. the binary radix tree of Karras, "Maximizing Parallelism in the
+//      Construction of BVHs, Octrees, and k-d Trees", HPG 2012 (equal codes are
+//      split by index);
+//   4. bottom-up boxes, triangle counts and surface areas;
+//   5. a top-down collapse into 8-wide nodes: each wide node repeatedly opens
+//      its largest child that is too big for a leaf, then opens small subtrees
+//      while slots remain; children take the octant slot their centre points
+//      to, so traversal visits them nearest first; child boxes are quantised to
+//      8 bits per plane against a power-of-two step, padded by one step on
+//      every side; leaf triangles are copied in leaf order.
+#include "bvh_build.h"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace hdcx {
+namespace {
+
+constexpr int kMaxLeafTriangles = 3;
+constexpr int kMaxDepth = 64;
+constexpr int kBlock = 256;
+
+#define CUDA_OK(expr)                                                                               \
+    do {                                                                                            \
+        cudaError_t err__ = (expr);                                                                 \
+        if (err__ != cudaSuccess) throw std::runtime_error(std::string("BVH build: ") + #expr + ": " + \
+                                                           cudaGetErrorString(err__));              \
+    } while (0)
+
+struct Box {
+    float3 lo;
+    float3 hi;
+};
+
+__device__ __forceinline__ uint32_t floatToOrdered(float f)
+{
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float orderedToFloat(uint32_t u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__global__ void triangleBoxesKernel(const float4* vertices, const uint32_t* indices, uint32_t n, float4* boxLo,
+                                    float4* boxHi, uint32_t* sceneBounds)
+{
+    __shared__ uint32_t sb[6];
+    if (threadIdx.x < 6) sb[threadIdx.x] = threadIdx.x < 3 ? 0xffffffffu : 0u;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float4 a = vertices[indices[3 * i + 0]];
+        const float4 b = vertices[indices[3 * i + 1]];
+        const float4 c = vertices[indices[3 * i + 2]];
+        const float3 lo = make_float3(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)));
+        const float3 hi = make_float3(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)));
+        boxLo[i] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+        boxHi[i] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+        // Scene bounds of the box centres (for the Morton grid).
+        const float cx = 0.5f * (lo.x + hi.x), cy = 0.5f * (lo.y + hi.y), cz = 0.5f * (lo.z + hi.z);
+        atomicMin(&sb[0], floatToOrdered(cx));
+        atomicMin(&sb[1], floatToOrdered(cy));
+        atomicMin(&sb[2], floatToOrdered(cz));
+        atomicMax(&sb[3], floatToOrdered(cx));
+        atomicMax(&sb[4], floatToOrdered(cy));
+        atomicMax(&sb[5], floatToOrdered(cz));
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&sceneBounds[threadIdx.x], sb[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&sceneBounds[threadIdx.x], sb[threadIdx.x]);
+}
+
+__device__ __forceinline__ uint64_t spreadBits21(uint64_t v)
+{
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void mortonKernel(const float4* boxLo, const float4* boxHi, uint32_t n, const uint32_t* sceneBounds,
+                             uint64_t* keys, uint32_t* ids)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float3 lo = make_float3(orderedToFloat(sceneBounds[0]), orderedToFloat(sceneBounds[1]), orderedToFloat(sceneBounds[2]));
+    const float3 hi = make_float3(orderedToFloat(sceneBounds[3]), orderedToFloat(sceneBounds[4]), orderedToFloat(sceneBounds[5]));
+    const float4 a = boxLo[i], b = boxHi[i];
+    const float c[3] = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z)};
+    const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+    uint64_t q[3];
+    for (int k = 0; k < 3; ++k) {
+        const float extent = h[k] - l[k];
+        float u = extent > 0.0f ? (c[k] - l[k]) / extent : 0.5f;
+        u = fminf(fmaxf(u, 0.0f), 1.0f);
+        q[k] = static_cast<uint64_t>(fminf(u * 2097152.0f, 2097151.0f));
+    }
+    keys[i] = (spreadBits21(q[0]) << 2) | (spreadBits21(q[1]) << 1) | spreadBits21(q[2]);
+    ids[i] = i;
+}
+
+__device__ __forceinline__ int delta(const uint64_t* keys, int n, int i, int j)
+{
+    if (j < 0 || j >= n) return -1;
+    const uint64_t a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz(static_cast<uint32_t>(i ^ j));
+    return __clzll(static_cast<long long>(a ^ b));
+}
+
+// Binary node ids: internal 0..n-2, leaf k -> (n-1)+k.
+__global__ void karrasKernel(const uint64_t* keys, int n, int* left, int* right, int* parent)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int deltaMin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > deltaMin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2) {
+        if (delta(keys, n, i, i + (l + t) * d) > deltaMin) l += t;
+    }
+    const int j = i + l * d;
+    const int deltaNode = delta(keys, n, i, j);
+    int s = 0;
+    for (int div = 2;; div *= 2) {
+        const int t = (l + div - 1) / div;
+        if (delta(keys, n, i, i + (s + t) * d) > deltaNode) s += t;
+        if (t <= 1) break;
+    }
+    const int gamma = i + s * d + min(d, 0);
+    const int lo = min(i, j), hi = max(i, j);
+    const int leftNode = (lo == gamma) ? (n - 1) + gamma : gamma;
+    const int rightNode = (hi == gamma + 1) ? (n - 1) + gamma + 1 : gamma + 1;
+    left[i] = leftNode;
+    right[i] = rightNode;
+    parent[leftNode] = i;
+    parent[rightNode] = i;
+}
+
+__global__ void bottomUpKernel(int n, const uint32_t* sortedIds, const float4* triLo, const float4* triHi, const int* left,
+                               const int* right, const int* parent, float4* nodeLo, float4* nodeHi, uint32_t* visits)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int node = (n - 1) + k;
+    const uint32_t prim = sortedIds[k];
+    float4 lo = triLo[prim], hi = triHi[prim];
+    lo.w = 1.0f;  // triangle count in .w of lo
+    nodeLo[node] = lo;
+    nodeHi[node] = hi;
+    __threadfence();
+    while (true) {
+        const int p = parent[node];
+        if (p < 0) break;
+        if (atomicAdd(&visits[p], 1u) == 0u) break;  // the sibling finishes the parent
+        __threadfence();
+        const int a = left[p], b = right[p];
+        const float4 la = __ldcg(nodeLo + a), lb = __ldcg(nodeLo + b);
+        const float4 ha = __ldcg(nodeHi + a), hb = __ldcg(nodeHi + b);
+        const float4 l2 = make_float4(fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z), la.w + lb.w);
+        const float4 h2 = make_float4(fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z), 0.0f);
+        nodeLo[p] = l2;
+        nodeHi[p] = h2;
+        __threadfence();
+        node = p;
+    }
+}
+
+struct CollapseItem {
+    int binaryNode;
+    uint32_t wideIndex;
+    uint32_t depth;
+    uint32_t pad;
+};
+
+__device__ __forceinline__ float surfaceArea(float4 lo, float4 hi)
+{
+    const float dx = fmaxf(hi.x - lo.x, 0.0f), dy = fmaxf(hi.y - lo.y, 0.0f), dz = fmaxf(hi.z - lo.z, 0.0f);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__device__ __forceinline__ int ceilLog2Double(double x)
+{
+    int e;
+    const double m = frexp(x, &e);  // x = m * 2^e, m in [0.5, 1)
+    return m == 0.5 ? e - 1 : e;
+}
+
+struct CollapseArgs {
+    int n;
+    const int* left;
+    const int* right;
+    const float4* nodeLo;
+    const float4* nodeHi;
+    const uint32_t* sortedIds;
+    const float4* vertices;
+    const uint32_t* indices;
+    float sceneScale;  // max |coordinate| and scene extent, for the padding floor
+    WideNode* wide;
+    float4* triVerts;
+    uint32_t* wideCounter;
+    uint32_t* triCounter;
+    uint32_t* errorFlag;
+};
+
+__global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32_t itemCount, CollapseItem* nextItems,
+                               uint32_t* nextCount)
+{
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= itemCount) return;
+    const CollapseItem item = items[w];
+    const int leafBase = a.n - 1;
+    auto isLeaf = [&](int b) { return b >= leafBase; };
+    auto count = [&](int b) { return static_cast<int>(a.nodeLo[b].w); };
+
+    int entries[8];
+    int m = 0;
+    if (isLeaf(item.binaryNode)) {
+        entries[m++] = item.binaryNode;
+    } else {
+        entries[m++] = a.left[item.binaryNode];
+        entries[m++] = a.right[item.binaryNode];
+    }
+    // Phase 1: open the largest child that cannot be a leaf.
+    while (m < 8) {
+        int best = -1;
+        float bestArea = -1.0f;
+        for (int i = 0; i < m; ++i) {
+            const int b = entries[i];
+            if (!isLeaf(b) && count(b) > kMaxLeafTriangles) {
+                const float area = surfaceArea(a.nodeLo[b], a.nodeHi[b]);
+                if (area > bestArea) { bestArea = area; best = i; }
+            }
+        }
+        if (best < 0) break;
+        const int b = entries[best];
+        entries[best] = a.left[b];
+        entries[m++] = a.right[b];
+    }
+    // Phase 2: open small subtrees while slots remain (tighter leaf boxes).
+    bool anyLarge = false;
+    for (int i = 0; i < m; ++i) anyLarge |= (!isLeaf(entries[i]) && count(entries[i]) > kMaxLeafTriangles);
+    while (m < 8 && !anyLarge) {
+        int best = -1;
+        float bestArea = -1.0f;
+        for (int i = 0; i < m; ++i) {
+            const int b = entries[i];
+            if (!isLeaf(b)) {
+                const float area = surfaceArea(a.nodeLo[b], a.nodeHi[b]);
+                if (area > bestArea) { bestArea = area; best = i; }
+            }
+        }
+        if (best < 0) break;
+        const int b = entries[best];
+        entries[best] = a.left[b];
+        entries[m++] = a.right[b];
+    }
+
+    // Node box and octant slot assignment.
+    float4 lo = a.nodeLo[entries[0]], hi = a.nodeHi[entries[0]];
+    for (int i = 1; i < m; ++i) {
+        const float4 l = a.nodeLo[entries[i]], h = a.nodeHi[entries[i]];
+        lo = make_float4(fminf(lo.x, l.x), fminf(lo.y, l.y), fminf(lo.z, l.z), 0.0f);
+        hi = make_float4(fmaxf(hi.x, h.x), fmaxf(hi.y, h.y), fmaxf(hi.z, h.z), 0.0f);
+    }
+    const float cx = 0.5f * (lo.x + hi.x), cy = 0.5f * (lo.y + hi.y), cz = 0.5f * (lo.z + hi.z);
+    int slotOf[8];
+    int entryOfSlot[8];
+    for (int i = 0; i < 8; ++i) { slotOf[i] = -1; entryOfSlot[i] = -1; }
+    for (int round = 0; round < m; ++round) {
+        float bestScore = -3.4e38f;
+        int be = -1, bs = -1;
+        for (int i = 0; i < m; ++i) {
+            if (slotOf[i] >= 0) continue;
+            const float4 l = a.nodeLo[entries[i]], h = a.nodeHi[entries[i]];
+            const float vx = 0.5f * (l.x + h.x) - cx, vy = 0.5f * (l.y + h.y) - cy, vz = 0.5f * (l.z + h.z) - cz;
+            for (int s = 0; s < 8; ++s) {
+                if (entryOfSlot[s] >= 0) continue;
+                const float score = ((s & 1) ? vx : -vx) + ((s & 2) ? vy : -vy) + ((s & 4) ? vz : -vz);
+                if (score > bestScore) { bestScore = score; be = i; bs = s; }
+            }
+        }
+        if (be < 0) {  // non-finite boxes: first free entry into the first free slot
+            for (int i = 0; i < m && be < 0; ++i) if (slotOf[i] < 0) be = i;
+            for (int q = 0; q < 8 && bs < 0; ++q) if (entryOfSlot[q] < 0) bs = q;
+        }
+        slotOf[be] = bs;
+        entryOfSlot[bs] = be;
+    }
+
+    // Quantisation grid per axis.
+    const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z};
+    float origin[3];
+    double step[3];
+    uint8_t biased[3];
+    for (int k = 0; k < 3; ++k) {
+        const double extent = static_cast<double>(h3[k]) - static_cast<double>(l3[k]);
+        const double floorStep = fmax(fmax(fabs(static_cast<double>(l3[k])), fabs(static_cast<double>(h3[k]))),
+                                      static_cast<double>(a.sceneScale)) * (1.0 / 65536.0);
+        double q = fmax(fmax(extent / 252.0, floorStep), 1e-30);
+        int e = ceilLog2Double(q);
+        e = max(-126, min(127, e));
+        step[k] = ldexp(1.0, e);
+        biased[k] = static_cast<uint8_t>(e + 127);
+        origin[k] = __double2float_rd(static_cast<double>(l3[k]) - step[k]);
+    }
+
+    // Allocate internal children and leaf triangles.
+    int internalCount = 0, triangleCount = 0;
+    for (int s = 0; s < 8; ++s) {
+        const int i = entryOfSlot[s];
+        if (i < 0) continue;
+        const int b = entries[i];
+        if (!isLeaf(b) && count(b) > kMaxLeafTriangles) internalCount++;
+        else triangleCount += isLeaf(b) ? 1 : count(b);
+    }
+    const uint32_t childBase = internalCount ? atomicAdd(a.wideCounter, static_cast<uint32_t>(internalCount)) : 0u;
+    const uint32_t triBase = triangleCount ? atomicAdd(a.triCounter, static_cast<uint32_t>(triangleCount)) : 0u;
+    if (item.depth + 1 >= kMaxDepth && internalCount) atomicOr(a.errorFlag, 1u);
+
+    WideNode node;
+    node.px = origin[0];
+    node.py = origin[1];
+    node.pz = origin[2];
+    node.ex = biased[0];
+    node.ey = biased[1];
+    node.ez = biased[2];
+    node.imask = 0;
+    node.childBase = childBase;
+    node.triBase = triBase;
+    int internalRank = 0, triOffset = 0;
+    for (int s = 0; s < 8; ++s) {
+        const int i = entryOfSlot[s];
+        node.meta[s] = 0;
+        node.qlox[s] = node.qloy[s] = node.qloz[s] = 0;
+        node.qhix[s] = node.qhiy[s] = node.qhiz[s] = 0;
+        if (i < 0) continue;
+        const int b = entries[i];
+        const float4 cl = a.nodeLo[b], ch = a.nodeHi[b];
+        const float cl3[3] = {cl.x, cl.y, cl.z}, ch3[3] = {ch.x, ch.y, ch.z};
+        uint8_t ql[3], qh[3];
+        for (int k = 0; k < 3; ++k) {
+            const double lo_q = floor((static_cast<double>(cl3[k]) - origin[k]) / step[k]) - 1.0;
+            const double hi_q = ceil((static_cast<double>(ch3[k]) - origin[k]) / step[k]) + 1.0;
+            ql[k] = static_cast<uint8_t>(fmin(fmax(lo_q, 0.0), 255.0));
+            qh[k] = static_cast<uint8_t>(fmin(fmax(hi_q, 0.0), 255.0));
+        }
+        node.qlox[s] = ql[0]; node.qloy[s] = ql[1]; node.qloz[s] = ql[2];
+        node.qhix[s] = qh[0]; node.qhiy[s] = qh[1]; node.qhiz[s] = qh[2];
+        if (!isLeaf(b) && count(b) > kMaxLeafTriangles) {
+            node.imask |= static_cast<uint8_t>(1u << s);
+            node.meta[s] = 0xffu;
+            const uint32_t slot = atomicAdd(nextCount, 1u);
+            nextItems[slot] = CollapseItem{b, childBase + static_cast<uint32_t>(internalRank), item.depth + 1u, 0u};
+            internalRank++;
+        } else {
+            // Leaf slot: its triangles in subtree order.
+            int stack[8];
+            int sp = 0;
+            stack[sp++] = b;
+            int written = 0;
+            while (sp > 0) {
+                const int x = stack[--sp];
+                if (isLeaf(x)) {
+                    const uint32_t prim = a.sortedIds[x - leafBase];
+                    const uint32_t dst = triBase + static_cast<uint32_t>(triOffset + written);
+                    const float4 v0 = a.vertices[a.indices[3 * prim + 0]];
+                    const float4 v1 = a.vertices[a.indices[3 * prim + 1]];
+                    const float4 v2 = a.vertices[a.indices[3 * prim + 2]];
+                    a.triVerts[3 * dst + 0] = make_float4(v0.x, v0.y, v0.z, __uint_as_float(prim));
+                    a.triVerts[3 * dst + 1] = make_float4(v1.x, v1.y, v1.z, 0.0f);
+                    a.triVerts[3 * dst + 2] = make_float4(v2.x, v2.y, v2.z, 0.0f);
+                    written++;
+                } else if (sp + 2 <= 8) {
+                    stack[sp++] = a.right[x];
+                    stack[sp++] = a.left[x];
+                }
+            }
+            const uint32_t unary = written >= 3 ? 7u : (written == 2 ? 3u : 1u);
+            node.meta[s] = static_cast<uint8_t>((unary << 5) | static_cast<uint32_t>(triOffset));
+            triOffset += written;
+        }
+    }
+    a.wide[item.wideIndex] = node;
+}
+
+template <typename T>
+T* deviceAlloc(size_t count)
+{
+    void* p = nullptr;
+    CUDA_OK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    return static_cast<T*>(p);
+}
+
+}  // namespace
+
+WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t triangleCount, float sceneScale,
+                     cudaStream_t stream)
+{
+    WideBvh out;
+    if (triangleCount == 0) return out;
+    const int n = static_cast<int>(triangleCount);
+    const int blocks = (n + kBlock - 1) / kBlock;
+    std::vector<void*> temps;
+    auto tmp = [&](size_t bytes) {
+        void* p = nullptr;
+        CUDA_OK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+        temps.push_back(p);
+        return p;
+    };
+    try {
+        float4* triLo = static_cast<float4*>(tmp(sizeof(float4) * n));
+        float4* triHi = static_cast<float4*>(tmp(sizeof(float4) * n));
+        uint32_t* bounds = static_cast<uint32_t*>(tmp(sizeof(uint32_t) * 6));
+        const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+        CUDA_OK(cudaMemcpyAsync(bounds, init, sizeof init, cudaMemcpyHostToDevice, stream));
+        triangleBoxesKernel<<<blocks, kBlock, 0, stream>>>(vertices, indices, triangleCount, triLo, triHi, bounds);
+        uint64_t* keys = static_cast<uint64_t*>(tmp(sizeof(uint64_t) * n));
+        uint64_t* keysSorted = static_cast<uint64_t*>(tmp(sizeof(uint64_t) * n));
+        uint32_t* ids = static_cast<uint32_t*>(tmp(sizeof(uint32_t) * n));
+        uint32_t* idsSorted = static_cast<uint32_t*>(tmp(sizeof(uint32_t) * n));
+        mortonKernel<<<blocks, kBlock, 0, stream>>>(triLo, triHi, triangleCount, bounds, keys, ids);
+        size_t sortBytes = 0;
+        CUDA_OK(cub::DeviceRadixSort::SortPairs(nullptr, sortBytes, keys, keysSorted, ids, idsSorted, n, 0, 63, stream));
+        void* sortTemp = tmp(sortBytes);
+        CUDA_OK(cub::DeviceRadixSort::SortPairs(sortTemp, sortBytes, keys, keysSorted, ids, idsSorted, n, 0, 63, stream));
+
+        const int nodes = 2 * n - 1;
+        int* left = static_cast<int*>(tmp(sizeof(int) * std::max(n - 1, 1)));
+        int* right = static_cast<int*>(tmp(sizeof(int) * std::max(n - 1, 1)));
+        int* parent = static_cast<int*>(tmp(sizeof(int) * nodes));
+        CUDA_OK(cudaMemsetAsync(parent, 0xff, sizeof(int) * nodes, stream));
+        if (n > 1) karrasKernel<<<(n - 1 + kBlock - 1) / kBlock, kBlock, 0, stream>>>(keysSorted, n, left, right, parent);
+        float4* nodeLo = static_cast<float4*>(tmp(sizeof(float4) * nodes));
+        float4* nodeHi = static_cast<float4*>(tmp(sizeof(float4) * nodes));
+        uint32_t* visits = static_cast<uint32_t*>(tmp(sizeof(uint32_t) * std::max(n - 1, 1)));
+        CUDA_OK(cudaMemsetAsync(visits, 0, sizeof(uint32_t) * std::max(n - 1, 1), stream));
+        bottomUpKernel<<<blocks, kBlock, 0, stream>>>(n, idsSorted, triLo, triHi, left, right, parent, nodeLo, nodeHi, visits);
+
+        out.nodes = deviceAlloc<WideNode>(n);
+        out.triVerts = deviceAlloc<float4>(3 * static_cast<size_t>(n));
+        uint32_t* counters = static_cast<uint32_t*>(tmp(sizeof(uint32_t) * 4));
+        const uint32_t initCounters[4] = {1u, 0u, 0u, 0u};  // wide nodes (root allocated), triangles, error, next
+        CUDA_OK(cudaMemcpyAsync(counters, initCounters, sizeof initCounters, cudaMemcpyHostToDevice, stream));
+        CollapseItem* itemsA = static_cast<CollapseItem*>(tmp(sizeof(CollapseItem) * n));
+        CollapseItem* itemsB = static_cast<CollapseItem*>(tmp(sizeof(CollapseItem) * n));
+        const CollapseItem root{n > 1 ? 0 : 0 /* leaf id n-1 == 0 when n == 1 */, 0u, 0u, 0u};
+        CUDA_OK(cudaMemcpyAsync(itemsA, &root, sizeof root, cudaMemcpyHostToDevice, stream));
+        CollapseArgs args{n, left, right, nodeLo, nodeHi, idsSorted, vertices, indices, sceneScale,
+                          out.nodes, out.triVerts, counters + 0, counters + 1, counters + 2};
+        uint32_t itemCount = 1;
+        uint32_t depth = 0;
+        while (itemCount > 0) {
+            CUDA_OK(cudaMemsetAsync(counters + 3, 0, sizeof(uint32_t), stream));
+            collapseKernel<<<(itemCount + kBlock - 1) / kBlock, kBlock, 0, stream>>>(args, itemsA, itemCount, itemsB, counters + 3);
+            CUDA_OK(cudaGetLastError());
+            CUDA_OK(cudaMemcpyAsync(&itemCount, counters + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            CUDA_OK(cudaStreamSynchronize(stream));
+            std::swap(itemsA, itemsB);
+            ++depth;
+        }
+        uint32_t finalCounters[4];
+        CUDA_OK(cudaMemcpyAsync(finalCounters, counters, sizeof finalCounters, cudaMemcpyDeviceToHost, stream));
+        CUDA_OK(cudaStreamSynchronize(stream));
+        if (finalCounters[2] != 0u) throw std::runtime_error("BVH build: tree deeper than the traversal stack");
+        if (finalCounters[1] != triangleCount) throw std::runtime_error("BVH build: leaf triangle count mismatch");
+        out.nodeCount = finalCounters[0];
+        out.depth = depth;
+        out.triangleCount = triangleCount;
+    } catch (...) {
+        for (void* p : temps) cudaFree(p);
+        if (out.nodes) cudaFree(out.nodes);
+        if (out.triVerts) cudaFree(out.triVerts);
+        throw;
+    }
+    for (void* p : temps) cudaFree(p);
+    return out;
+}
+
+void freeWideBvh(WideBvh& bvh)
+{
+    if (bvh.nodes) cudaFree(bvh.nodes);
+    if (bvh.triVerts) cudaFree(bvh.triVerts);
+    bvh = WideBvh{};
+}
+
+}  // namespace hdcx

@@ -1,0 +1,235 @@
+// traverse.cuh - ray queries on the 8-wide compressed BVH.
+//
+// Replaces the reference's VK_KHR_ray_query loops (vulkan_path_tracer.cpp:
+// 1228-1243 closest hit with stochastic opacity, :855-912 shadow any-hit with
+// a 0.5 opacity threshold, :1130-1151 opaque boundary rays).
+//
+// * Triangle test: watertight test of Woop, Benthin and Wald (JCGT 2013) in
+//   binary32 with no fused multiply-add, degenerate edge functions recomputed
+//   in binary64, t = T / det, accepted when tmin <= t <= tmax. The CPU oracle
+//   states the same test, so hit/miss and (t, barycentrics) agree bit for bit.
+// * Closest hit: smallest t among confirmed candidates; equal t goes to the
+//   smaller flattened primitive index. The result does not depend on the
+//   order in which the traversal meets candidates.
+// * Traversal: one thread per ray over 80-byte nodes (Ylitie, Karras and
+//   Laine, HPG 2017): the eight quantised child boxes are tested per node
+//   with one fused multiply-add per plane; internal hits are visited nearest
+//   octant first, leaf triangles of the node are tested before descending,
+//   and pending node groups go on a per-thread stack. Child boxes are padded
+//   by one quantisation step on every side at build time, which keeps the
+//   binary32 slab test conservative.
+#pragma once
+
+#include "common.cuh"
+#include "shading.cuh"
+
+namespace hdcx {
+
+constexpr int kTraversalStack = 64;
+
+enum class Accept : int {
+    Opaque = 0,      // every candidate is confirmed
+    Stochastic = 1,  // confirmed iff anyHitThreshold(rayRng, prim) <= opacity
+    Threshold = 2,   // confirmed iff opacity >= 0.5
+};
+
+struct HitRecord {
+    float t;
+    uint32_t primitive;
+    float b1;
+    float b2;
+};
+
+struct RayPre {
+    float3 o;
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+HDCX_D float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+HDCX_D RayPre precomputeRay(float3 o, float3 d)
+{
+    RayPre r;
+    r.o = o;
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = 0;
+    float m = ax;
+    if (ay > m) { kz = 1; m = ay; }
+    if (az > m) kz = 2;
+    int kx = kz + 1;
+    if (kx == 3) kx = 0;
+    int ky = kx + 1;
+    if (ky == 3) ky = 0;
+    const float dz = comp(d, kz);
+    if (dz < 0.0f) {
+        const int tmp = kx;
+        kx = ky;
+        ky = tmp;
+    }
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
+    r.sx = __fdiv_rn(comp(d, kx), dz);
+    r.sy = __fdiv_rn(comp(d, ky), dz);
+    r.sz = __fdiv_rn(1.0f, dz);
+    return r;
+}
+
+HDCX_D bool intersectTriangle(const RayPre& r, float3 v0, float3 v1, float3 v2, float tmin, float tmax, float& tOut,
+                              float& b1, float& b2)
+{
+    const float3 a = v0 - r.o;
+    const float3 b = v1 - r.o;
+    const float3 c = v2 - r.o;
+    const float az = comp(a, r.kz), bz = comp(b, r.kz), cz = comp(c, r.kz);
+    const float ax = __fsub_rn(comp(a, r.kx), __fmul_rn(r.sx, az));
+    const float ay = __fsub_rn(comp(a, r.ky), __fmul_rn(r.sy, az));
+    const float bx = __fsub_rn(comp(b, r.kx), __fmul_rn(r.sx, bz));
+    const float by = __fsub_rn(comp(b, r.ky), __fmul_rn(r.sy, bz));
+    const float cx = __fsub_rn(comp(c, r.kx), __fmul_rn(r.sx, cz));
+    const float cy = __fsub_rn(comp(c, r.ky), __fmul_rn(r.sy, cz));
+    float u = __fsub_rn(__fmul_rn(cx, by), __fmul_rn(cy, bx));
+    float v = __fsub_rn(__fmul_rn(ax, cy), __fmul_rn(ay, cx));
+    float w = __fsub_rn(__fmul_rn(bx, ay), __fmul_rn(by, ax));
+    if (u == 0.0f || v == 0.0f || w == 0.0f) {
+        u = __double2float_rn(__dsub_rn(__dmul_rn(cx, by), __dmul_rn(cy, bx)));
+        v = __double2float_rn(__dsub_rn(__dmul_rn(ax, cy), __dmul_rn(ay, cx)));
+        w = __double2float_rn(__dsub_rn(__dmul_rn(bx, ay), __dmul_rn(by, ax)));
+    }
+    if ((u < 0.0f || v < 0.0f || w < 0.0f) && (u > 0.0f || v > 0.0f || w > 0.0f)) return false;
+    const float det = __fadd_rn(__fadd_rn(u, v), w);
+    if (det == 0.0f) return false;
+    const float saz = __fmul_rn(r.sz, az), sbz = __fmul_rn(r.sz, bz), scz = __fmul_rn(r.sz, cz);
+    const float tScaled = __fadd_rn(__fadd_rn(__fmul_rn(u, saz), __fmul_rn(v, sbz)), __fmul_rn(w, scz));
+    const float t = __fdiv_rn(tScaled, det);
+    if (!(t >= tmin && t <= tmax)) return false;
+    tOut = t;
+    b1 = __fdiv_rn(v, det);
+    b2 = __fdiv_rn(w, det);
+    return true;
+}
+
+HDCX_D float byteToFloat(uint32_t word, int index) { return __uint2float_rn((word >> (8 * index)) & 0xffu); }
+
+// Traverses the wide BVH. kAny: stop at the first confirmed candidate.
+// Returns true on a (confirmed) hit; for closest queries fills `hit`.
+// kCount adds the wide nodes loaded to work.x and the triangle tests to work.y.
+template <Accept kMode, bool kAny, bool kCount = false>
+HDCX_D bool traceRay(const DeviceScene& s, float3 o, float3 d, float tmin, float tmax, uint32_t rayRng, HitRecord& hit,
+                     uint2* work = nullptr)
+{
+    if (s.nodeCount == 0u) return false;
+    const RayPre pre = precomputeRay(o, d);
+    const float tiny = 8.271806e-25f;  // 2^-80: direction components below it are treated as 2^-80
+    const float idx = 1.0f / (fabsf(d.x) > tiny ? d.x : copysignf(tiny, d.x));
+    const float idy = 1.0f / (fabsf(d.y) > tiny ? d.y : copysignf(tiny, d.y));
+    const float idz = 1.0f / (fabsf(d.z) > tiny ? d.z : copysignf(tiny, d.z));
+    const uint32_t octInv = ((d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u)) ^ 7u;
+
+    float bestT = tmax;
+    uint32_t bestPrim = kInvalidPrimitive;
+    float bestB1 = 0.0f, bestB2 = 0.0f;
+
+    uint2 stack[kTraversalStack];
+    int sp = 0;
+    // A node group: x = base index of the internal children, y = hit bits in
+    // 24..31 (by visiting order) | parent imask in 0..7. The root is child
+    // slot 0 of a virtual parent whose children start at node 0.
+    uint2 nodeGroup = make_uint2(0u, (1u << (24u + (0u ^ octInv))) | 1u);
+    uint2 triGroup = make_uint2(0u, 0u);
+    // Every node is entered at most once in a tree; the cap only guards
+    // against a malformed node array.
+    uint32_t budget = s.nodeCount + 1u;
+
+    while (true) {
+        while (triGroup.y != 0u) {
+            const int bit = __ffs(triGroup.y) - 1;
+            triGroup.y &= triGroup.y - 1u;
+            const uint32_t slot = triGroup.x + static_cast<uint32_t>(bit);
+            const float4 w0 = __ldg(s.triVerts + slot * 3u + 0u);
+            const float4 w1 = __ldg(s.triVerts + slot * 3u + 1u);
+            const float4 w2 = __ldg(s.triVerts + slot * 3u + 2u);
+            if (kCount) work->y++;
+            float t, b1, b2;
+            if (!intersectTriangle(pre, xyz(w0), xyz(w1), xyz(w2), tmin, tmax, t, b1, b2)) continue;
+            const uint32_t prim = __float_as_uint(w0.w);
+            if (!kAny) {
+                if (t > bestT) continue;
+                if (t == bestT && prim > bestPrim) continue;
+            }
+            if (kMode == Accept::Stochastic) {
+                if (!(anyHitThreshold(rayRng, prim) <= surfaceOpacity(s, prim, b1, b2))) continue;
+            } else if (kMode == Accept::Threshold) {
+                if (!(surfaceOpacity(s, prim, b1, b2) >= 0.5f)) continue;
+            }
+            if (kAny) return true;
+            bestT = t;
+            bestPrim = prim;
+            bestB1 = b1;
+            bestB2 = b2;
+        }
+        if ((nodeGroup.y & 0xff000000u) == 0u) {
+            if (sp == 0) break;
+            nodeGroup = stack[--sp];
+        }
+        if (budget-- == 0u) break;
+        // Next child of the current group, nearest octant first.
+        const uint32_t hitBits = nodeGroup.y >> 24;
+        const uint32_t pos = 31u - __clz(hitBits);
+        nodeGroup.y &= ~(1u << (24u + pos));
+        const uint32_t childSlot = pos ^ octInv;
+        const uint32_t parentMask = nodeGroup.y & 0xffu;
+        const uint32_t nodeIndex = nodeGroup.x + __popc(parentMask & ((1u << childSlot) - 1u));
+        if ((nodeGroup.y & 0xff000000u) != 0u && sp < kTraversalStack) stack[sp++] = nodeGroup;
+
+        if (kCount) work->x++;
+        const uint4* np = reinterpret_cast<const uint4*>(s.nodes + nodeIndex);
+        const uint4 n0 = __ldg(np + 0), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+        const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+        const uint32_t e = n0.w;
+        const float scx = __uint_as_float((e & 0xffu) << 23);
+        const float scy = __uint_as_float(((e >> 8) & 0xffu) << 23);
+        const float scz = __uint_as_float(((e >> 16) & 0xffu) << 23);
+        const uint32_t imask = e >> 24;
+        // t = q * (scale * invd) + (p - o) * invd per plane.
+        const float ax = scx * idx, ay = scy * idy, az = scz * idz;
+        const float bx = (px - o.x) * idx, by = (py - o.y) * idy, bz = (pz - o.z) * idz;
+        // Near/far planes by direction sign: words of qlo (n2.x..n3.y) and qhi (n3.z..n4.w).
+        const uint32_t loX0 = n2.x, loX1 = n2.y, loY0 = n2.z, loY1 = n2.w, loZ0 = n3.x, loZ1 = n3.y;
+        const uint32_t hiX0 = n3.z, hiX1 = n3.w, hiY0 = n4.x, hiY1 = n4.y, hiZ0 = n4.z, hiZ1 = n4.w;
+        const bool sx = idx >= 0.0f, sy = idy >= 0.0f, sz = idz >= 0.0f;
+        const uint32_t nearX0 = sx ? loX0 : hiX0, nearX1 = sx ? loX1 : hiX1, farX0 = sx ? hiX0 : loX0, farX1 = sx ? hiX1 : loX1;
+        const uint32_t nearY0 = sy ? loY0 : hiY0, nearY1 = sy ? loY1 : hiY1, farY0 = sy ? hiY0 : loY0, farY1 = sy ? hiY1 : loY1;
+        const uint32_t nearZ0 = sz ? loZ0 : hiZ0, nearZ1 = sz ? loZ1 : hiZ1, farZ0 = sz ? hiZ0 : loZ0, farZ1 = sz ? hiZ1 : loZ1;
+        const uint32_t meta0 = n1.z, meta1 = n1.w;
+        uint32_t nodeHits = 0u, triHits = 0u;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int k = i & 3;
+            const uint32_t meta = ((i < 4 ? meta0 : meta1) >> (8 * k)) & 0xffu;
+            const float tnx = fmaf(byteToFloat(i < 4 ? nearX0 : nearX1, k), ax, bx);
+            const float tny = fmaf(byteToFloat(i < 4 ? nearY0 : nearY1, k), ay, by);
+            const float tnz = fmaf(byteToFloat(i < 4 ? nearZ0 : nearZ1, k), az, bz);
+            const float tfx = fmaf(byteToFloat(i < 4 ? farX0 : farX1, k), ax, bx);
+            const float tfy = fmaf(byteToFloat(i < 4 ? farY0 : farY1, k), ay, by);
+            const float tfz = fmaf(byteToFloat(i < 4 ? farZ0 : farZ1, k), az, bz);
+            const float tNear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+            const float tFar = fminf(fminf(tfx, tfy), fminf(tfz, bestT));
+            if (meta != 0u && tNear <= tFar) {
+                if ((imask >> i) & 1u) nodeHits |= 1u << (static_cast<uint32_t>(i) ^ octInv);
+                else triHits |= (meta >> 5) << (meta & 31u);
+            }
+        }
+        nodeGroup = make_uint2(n1.x, (nodeHits << 24) | imask);
+        triGroup = make_uint2(n1.y, triHits);
+    }
+    if (kAny || bestPrim == kInvalidPrimitive) return false;
+    hit.t = bestT;
+    hit.primitive = bestPrim;
+    hit.b1 = bestB1;
+    hit.b2 = bestB2;
+    return true;
+}
+
+}  // namespace hdcx

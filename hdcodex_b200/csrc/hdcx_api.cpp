@@ -1,0 +1,630 @@
+// hdcx_api.cpp - the C ABI of include/hdcx.h.
+//
+// One hdcx_tracer owns everything the reference's VulkanPathTracer::Impl owns
+// (vulkan_path_tracer.cpp:2082-3346): the device scene (flattened buffers,
+// textures, the BVH), the RGBA32F running-mean buffer of the last render size
+// and the fallback up axis fixed by its first render. Every entry point turns
+// exceptions and CUDA errors into a status code plus hdcx_last_error().
+#include "hdcx.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "bvh_build.h"
+#include "integrator.h"
+#include "scene_pack.h"
+
+namespace {
+
+using namespace hdcx;
+
+struct StatusError : std::runtime_error {
+    hdcx_status status;
+    StatusError(hdcx_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+void check(cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return;
+    const hdcx_status s = e == cudaErrorMemoryAllocation ? HDCX_ERROR_OUT_OF_MEMORY : HDCX_ERROR_CUDA;
+    throw StatusError(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Device allocation tracked by the tracer.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { reset(); }
+    void reset()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    void allocate(size_t n)
+    {
+        reset();
+        check(cudaMalloc(&ptr, std::max<size_t>(n, 16)), "cudaMalloc");
+        bytes = n;
+    }
+    template <typename T>
+    T* as() const
+    {
+        return static_cast<T*>(ptr);
+    }
+};
+
+}  // namespace
+
+struct hdcx_tracer {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string lastError;
+    int32_t shadingMode = HDCX_SHADING_FUSED;
+    bool geometryReady = false;
+    bool fallbackAxisInitialized = false;
+    bool fallbackZUp = false;
+    uint64_t wavePaths = 0;  // 0 = automatic
+    uint32_t profiling = 0;  // HDCX_PROFILE_* bits
+    // Scene.
+    std::vector<DeviceBuffer*> sceneBuffers;
+    DeviceBuffer texDescs;
+    DeviceScene scene{};
+    WideBvh bvh;
+    // Paths and frame.
+    std::vector<DeviceBuffer*> pathBuffers;
+    PathBuffers paths;
+    DeviceBuffer rgba, xyz, batch, batchXyz;
+    FrameBuffers fb;
+    uint64_t xyzSamples = 0;
+    hdcx_render_stats stats{};
+    cudaEvent_t start = nullptr, stop = nullptr;
+
+    ~hdcx_tracer()
+    {
+        if (stream) cudaStreamSynchronize(stream);
+        clearScene();
+        clearPaths();
+        if (start) cudaEventDestroy(start);
+        if (stop) cudaEventDestroy(stop);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void clearScene()
+    {
+        for (DeviceBuffer* b : sceneBuffers) delete b;
+        sceneBuffers.clear();
+        texDescs.reset();
+        freeWideBvh(bvh);
+        scene = DeviceScene{};
+        geometryReady = false;
+    }
+    void clearPaths()
+    {
+        for (DeviceBuffer* b : pathBuffers) delete b;
+        pathBuffers.clear();
+        paths = PathBuffers{};
+    }
+    template <typename T>
+    T* upload(const std::vector<T>& host)
+    {
+        auto* b = new DeviceBuffer();
+        sceneBuffers.push_back(b);
+        b->allocate(host.size() * sizeof(T));
+        if (!host.empty()) check(cudaMemcpyAsync(b->ptr, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
+        return b->as<T>();
+    }
+    template <typename T>
+    T* pathAlloc(size_t count)
+    {
+        auto* b = new DeviceBuffer();
+        pathBuffers.push_back(b);
+        b->allocate(count * sizeof(T));
+        return b->as<T>();
+    }
+};
+
+struct hdcx_packing {
+    PackedSceneData data;
+    std::vector<hdcx_packed_texture> textureViews;
+    hdcx_packed_scene view{};
+};
+
+namespace {
+
+hdcx_status fail(hdcx_tracer* t, hdcx_status s, const std::string& message)
+{
+    if (t) t->lastError = message;
+    return s;
+}
+
+template <typename F>
+hdcx_status guarded(hdcx_tracer* t, F&& body)
+{
+    try {
+        if (t) {
+            t->lastError.clear();
+            check(cudaSetDevice(t->device), "cudaSetDevice");
+        }
+        body();
+        return HDCX_OK;
+    } catch (const StatusError& e) {
+        return fail(t, e.status, e.what());
+    } catch (const std::invalid_argument& e) {
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(t, HDCX_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(t, HDCX_ERROR_CUDA, e.what());
+    }
+}
+
+void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
+{
+    check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+    t->clearScene();
+    if (!d.geometryReady) return;
+    DeviceScene s{};
+    s.vertices = reinterpret_cast<const float4*>(t->upload(d.vertices));
+    s.indices = t->upload(d.indices);
+    s.triangleMaterials = t->upload(d.triangleMaterials);
+    s.texcoords = reinterpret_cast<const float2*>(t->upload(d.texcoords));
+    s.normals = reinterpret_cast<const float4*>(t->upload(d.normals));
+    s.materials = reinterpret_cast<const GpuMaterial*>(t->upload(d.materials));
+    s.lights = reinterpret_cast<const GpuLight*>(t->upload(d.lights));
+    s.emissive = reinterpret_cast<const float4*>(t->upload(d.emissive));
+    std::vector<TexDesc> descs;
+    for (const PackedTexture& pt : d.textures) {
+        TexDesc td{};
+        td.width = pt.width;
+        td.height = pt.height;
+        td.format = pt.format;
+        td.texels = pt.format == HDCX_TEXEL_RGBA32F ? static_cast<const void*>(t->upload(pt.floats))
+                                                    : static_cast<const void*>(t->upload(pt.bytes));
+        descs.push_back(td);
+    }
+    t->texDescs.allocate(std::max<size_t>(1, descs.size()) * sizeof(TexDesc));
+    if (!descs.empty()) {
+        check(cudaMemcpyAsync(t->texDescs.ptr, descs.data(), descs.size() * sizeof(TexDesc), cudaMemcpyHostToDevice, t->stream),
+              "upload textures");
+    }
+    s.textures = t->texDescs.as<TexDesc>();
+    s.textureCount = static_cast<uint32_t>(descs.size());
+    s.primitiveCount = d.triangleCount();
+    s.lightCount = std::min(d.lightCount, static_cast<uint32_t>(HDCX_MAX_LIGHTS));
+    s.opaque = d.opaque ? 1u : 0u;
+    s.hasMeshLights = (d.triangleCount() > 0 && d.emissive[(size_t(d.triangleCount()) - 1) * 4u] > 0.0F) ? 1u : 0u;
+    // Padding floor of the BVH quantisation: the scene's coordinate scale.
+    float scale = 0.0F;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = 0; i < d.vertices.size(); i += 4) {
+        for (int k = 0; k < 3; ++k) {
+            const float v = d.vertices[i + k];
+            if (!std::isfinite(v)) continue;
+            lo[k] = std::min(lo[k], v);
+            hi[k] = std::max(hi[k], v);
+            scale = std::max(scale, std::fabs(v));
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (hi[k] >= lo[k]) scale = std::max(scale, hi[k] - lo[k]);
+    }
+    t->bvh = buildWideBvh(s.vertices, s.indices, s.primitiveCount, std::max(scale, 1e-20F), t->stream);
+    s.nodes = t->bvh.nodes;
+    s.triVerts = t->bvh.triVerts;
+    s.nodeCount = t->bvh.nodeCount;
+    check(cudaStreamSynchronize(t->stream), "scene upload");
+    t->scene = s;
+    t->geometryReady = true;
+}
+
+void ensureOutput(hdcx_tracer* t, uint32_t w, uint32_t h)
+{
+    if (t->fb.width == w && t->fb.height == h && t->fb.rgba) return;
+    // EnsureOutput (vulkan_path_tracer.cpp:3130-3160): a new size gets a
+    // zero-filled accumulation buffer.
+    check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+    const size_t pixels = size_t(w) * h;
+    t->rgba.allocate(pixels * sizeof(float4));
+    t->xyz.allocate(pixels * 3u * sizeof(double));
+    t->batch.allocate(pixels * sizeof(float4));
+    t->batchXyz.allocate(pixels * 3u * sizeof(double));
+    check(cudaMemsetAsync(t->rgba.ptr, 0, pixels * sizeof(float4), t->stream), "clear output");
+    check(cudaMemsetAsync(t->xyz.ptr, 0, pixels * 3u * sizeof(double), t->stream), "clear xyz");
+    t->fb.width = w;
+    t->fb.height = h;
+    t->fb.rgba = t->rgba.as<float4>();
+    t->fb.xyz = t->xyz.as<double>();
+    t->fb.batch = t->batch.as<float4>();
+    t->fb.batchXyz = t->batchXyz.as<double>();
+    t->xyzSamples = 0;
+}
+
+void ensurePaths(hdcx_tracer* t, uint64_t needed, uint32_t shadowPerPath)
+{
+    const uint64_t automatic = 12ull << 20;  // ~12.6M paths per wave
+    const uint64_t cap = t->wavePaths ? t->wavePaths : automatic;
+    const uint64_t capacity = std::max<uint64_t>(3, std::min(needed, cap));
+    if (t->paths.capacity >= capacity && t->paths.shadowPerPath >= shadowPerPath) return;
+    check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+    t->clearPaths();
+    PathBuffers& p = t->paths;
+    const uint64_t n = capacity;
+    const uint64_t ns = n * shadowPerPath;
+    p.capacity = n;
+    p.shadowPerPath = shadowPerPath;
+    p.rng = t->pathAlloc<uint32_t>(n);
+    p.wavelength = t->pathAlloc<float>(n);
+    p.spectrum = t->pathAlloc<float4>(n);
+    p.throughput = t->pathAlloc<float>(n);
+    p.radiance = t->pathAlloc<float>(n);
+    p.rayOrigin = t->pathAlloc<float4>(n);
+    p.rayDirection = t->pathAlloc<float4>(n);
+    p.flags = t->pathAlloc<uint32_t>(n);
+    p.previousPdf = t->pathAlloc<float2>(n);
+    p.medium = t->pathAlloc<float4>(n);
+    p.hit = t->pathAlloc<float4>(n);
+    p.contribution = t->pathAlloc<float>(3 * n);
+    p.contributionValid = t->pathAlloc<uint8_t>(3 * n);
+    p.queue[0] = t->pathAlloc<uint32_t>(n);
+    p.queue[1] = t->pathAlloc<uint32_t>(n);
+    p.shadowOrigin = t->pathAlloc<float4>(ns);
+    p.shadowDirection = t->pathAlloc<float4>(ns);
+    p.shadowFactors = t->pathAlloc<float4>(ns);
+    p.shadowSlot = t->pathAlloc<uint32_t>(ns);
+    p.shadowInfo = t->pathAlloc<uint32_t>(ns);
+    p.counters = t->pathAlloc<uint32_t>(4);
+    p.stats = t->pathAlloc<unsigned long long>(8);
+}
+
+FrameConst makeFrame(const hdcx_tracer* t, const hdcx_camera& c, uint32_t w, uint32_t h, uint32_t sampleIndex,
+                     uint32_t maxBounces, uint32_t sampleCount)
+{
+    FrameConst f{};
+    f.origin = make_float3(c.origin[0], c.origin[1], c.origin[2]);
+    f.lowerLeft = make_float3(c.lower_left[0], c.lower_left[1], c.lower_left[2]);
+    f.horizontal = make_float3(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
+    f.vertical = make_float3(c.vertical[0], c.vertical[1], c.vertical[2]);
+    f.width = w;
+    f.height = h;
+    f.sampleIndex = sampleIndex;
+    f.sampleCount = std::max(sampleCount, 1u);
+    f.maxBounces = std::clamp(maxBounces, 1u, HDCX_MAX_PATH_BOUNCES);
+    f.zUp = t->fallbackZUp ? 1u : 0u;
+    return f;
+}
+
+}  // namespace
+
+extern "C" {
+
+HDCX_API uint32_t hdcx_abi_version(void) { return HDCX_ABI_VERSION; }
+
+HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity)
+{
+    const uint64_t all[] = {sizeof(hdcx_camera),         sizeof(hdcx_mesh_desc),  sizeof(hdcx_material_desc),
+                            sizeof(hdcx_texture_desc),   sizeof(hdcx_light_desc), sizeof(hdcx_scene_desc),
+                            sizeof(hdcx_packed_texture), sizeof(hdcx_packed_scene), sizeof(hdcx_render_stats)};
+    const uint32_t n = static_cast<uint32_t>(sizeof(all) / sizeof(all[0]));
+    for (uint32_t i = 0; i < std::min(n, capacity); ++i) sizes[i] = all[i];
+    return n;
+}
+
+HDCX_API void hdcx_material_defaults(hdcx_material_desc* m)
+{
+    if (!m) return;
+    std::memset(m, 0, sizeof(*m));
+    auto set3 = [](float* d, float a, float b, float c) { d[0] = a; d[1] = b; d[2] = c; };
+    set3(m->base_color, 0.8F, 0.8F, 0.8F);
+    set3(m->base_color_texture_scale, 1.0F, 1.0F, 1.0F);
+    m->base_color_texture_channel = -1;
+    set3(m->transmission_color, 1.0F, 1.0F, 1.0F);
+    set3(m->specular_color, 1.0F, 1.0F, 1.0F);
+    set3(m->coat_color, 1.0F, 1.0F, 1.0F);
+    set3(m->sheen_color, 1.0F, 1.0F, 1.0F);
+    set3(m->translucent_color, 1.0F, 1.0F, 1.0F);
+    set3(m->subsurface_color, 0.8F, 0.8F, 0.8F);
+    set3(m->subsurface_radius, 1.0F, 0.2F, 0.1F);
+    m->diffuse_weight = 1.0F;
+    m->roughness = 0.5F;
+    m->roughness_v = 0.5F;
+    m->opacity = 1.0F;
+    m->transmission_dispersion_abbe_number = 20.0F;
+    m->index_of_refraction = 1.5F;
+    m->specular_weight = 1.0F;
+    m->coat_roughness = 0.1F;
+    m->coat_roughness_v = 0.1F;
+    m->coat_index_of_refraction = 1.5F;
+    m->sheen_roughness = 0.3F;
+    m->subsurface_scale = 1.0F;
+    m->normal_texture_scale = 1.0F;
+}
+
+HDCX_API void hdcx_light_defaults(hdcx_light_desc* l)
+{
+    if (!l) return;
+    std::memset(l, 0, sizeof(*l));
+    auto set3 = [](float* d, float a, float b, float c) { d[0] = a; d[1] = b; d[2] = c; };
+    l->visible = 1;
+    set3(l->color, 1.0F, 1.0F, 1.0F);
+    set3(l->temperature_color, 1.0F, 1.0F, 1.0F);
+    l->intensity = 1.0F;
+    l->diffuse = 1.0F;
+    l->specular = 1.0F;
+    set3(l->basis_x, 1.0F, 0.0F, 0.0F);
+    set3(l->basis_y, 0.0F, 1.0F, 0.0F);
+    set3(l->basis_z, 0.0F, 0.0F, 1.0F);
+    set3(l->axis_u, 1.0F, 0.0F, 0.0F);
+    set3(l->axis_v, 0.0F, 1.0F, 0.0F);
+    l->width = 1.0F;
+    l->height = 1.0F;
+    l->radius = 0.5F;
+    l->length = 1.0F;
+    l->angle = 0.53F;
+    l->area = 1.0F;
+    l->shaping_cone_angle = 180.0F;
+    l->shadow_enable = 1;
+    l->shadow_distance = -1.0F;
+    l->shadow_falloff = -1.0F;
+    l->shadow_falloff_gamma = 1.0F;
+}
+
+HDCX_API void hdcx_mesh_defaults(hdcx_mesh_desc* m)
+{
+    if (!m) return;
+    std::memset(m, 0, sizeof(*m));
+    m->display_color[0] = m->display_color[1] = m->display_color[2] = 0.5F;
+}
+
+HDCX_API hdcx_status hdcx_probe_devices(int32_t* supported, int32_t* deviceCount)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) count = 0;
+    int ok = 0;
+    for (int d = 0; d < count; ++d) {
+        cudaDeviceProp prop{};
+        if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10) ok = 1;
+    }
+    if (supported) *supported = ok;
+    if (deviceCount) *deviceCount = count;
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_create(int32_t device, hdcx_tracer** out)
+{
+    if (!out) return HDCX_ERROR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return HDCX_ERROR_NO_DEVICE;
+    if (device < 0 || device >= count) return HDCX_ERROR_INVALID_ARGUMENT;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return HDCX_ERROR_CUDA;
+    if (prop.major != 10) return HDCX_ERROR_UNSUPPORTED;  // kernels are built for sm_100a only
+    auto* t = new (std::nothrow) hdcx_tracer();
+    if (!t) return HDCX_ERROR_OUT_OF_MEMORY;
+    t->device = device;
+    const hdcx_status s = guarded(t, [&] {
+        check(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaEventCreate(&t->start), "cudaEventCreate");
+        check(cudaEventCreate(&t->stop), "cudaEventCreate");
+        float table[256];
+        srgbTable(table);
+        uploadSrgbTable(table, t->stream);
+        check(cudaStreamSynchronize(t->stream), "init");
+    });
+    if (s != HDCX_OK) {
+        delete t;
+        return s;
+    }
+    *out = t;
+    return HDCX_OK;
+}
+
+HDCX_API void hdcx_destroy(hdcx_tracer* t)
+{
+    if (!t) return;
+    cudaSetDevice(t->device);
+    delete t;
+}
+
+HDCX_API const char* hdcx_last_error(const hdcx_tracer* t) { return t ? t->lastError.c_str() : ""; }
+
+HDCX_API hdcx_status hdcx_set_scene(hdcx_tracer* t, const hdcx_scene_desc* desc)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    return guarded(t, [&] {
+        if (!desc) {
+            check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+            t->clearScene();
+            return;
+        }
+        const PackedSceneData d = packScene(*desc);
+        uploadScene(t, d);
+    });
+}
+
+HDCX_API hdcx_status hdcx_set_scene_packed(hdcx_tracer* t, const hdcx_packed_scene* view)
+{
+    if (!t || !view) return HDCX_ERROR_INVALID_ARGUMENT;
+    return guarded(t, [&] { uploadScene(t, copyPackedView(*view)); });
+}
+
+HDCX_API hdcx_status hdcx_pack_scene(const hdcx_scene_desc* desc, hdcx_packing** out)
+{
+    if (!desc || !out) return HDCX_ERROR_INVALID_ARGUMENT;
+    *out = nullptr;
+    try {
+        auto* p = new hdcx_packing();
+        p->data = packScene(*desc);
+        makePackedView(p->data, p->textureViews, &p->view);
+        *out = p;
+        return HDCX_OK;
+    } catch (const std::bad_alloc&) {
+        return HDCX_ERROR_OUT_OF_MEMORY;
+    } catch (const std::exception&) {
+        return HDCX_ERROR_INVALID_ARGUMENT;
+    }
+}
+
+HDCX_API const hdcx_packed_scene* hdcx_packing_view(const hdcx_packing* p) { return p ? &p->view : nullptr; }
+
+HDCX_API void hdcx_packing_destroy(hdcx_packing* p) { delete p; }
+
+HDCX_API int32_t hdcx_has_geometry(const hdcx_tracer* t) { return t && t->geometryReady ? 1 : 0; }
+
+HDCX_API hdcx_status hdcx_set_shading_mode(hdcx_tracer* t, int32_t mode)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (mode == HDCX_SHADING_RASTER_PREVIEW) {
+        return fail(t, HDCX_ERROR_UNSUPPORTED, "raster preview requires the MaterialX graphics backend");
+    }
+    if (mode != HDCX_SHADING_FUSED && mode != HDCX_SHADING_MODULAR) {
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "unknown shading mode");
+    }
+    t->shadingMode = mode;
+    t->lastError.clear();
+    return HDCX_OK;
+}
+
+HDCX_API int32_t hdcx_get_shading_mode(const hdcx_tracer* t) { return t ? t->shadingMode : HDCX_SHADING_FUSED; }
+
+HDCX_API hdcx_status hdcx_set_profiling(hdcx_tracer* t, uint32_t flags)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    t->profiling = flags;
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_set_wave_size(hdcx_tracer* t, uint64_t paths)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (paths != 0 && paths < 3) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "a wave holds at least 3 paths");
+    t->wavePaths = paths;
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint32_t width, uint32_t height,
+                                 uint32_t sampleIndex, uint32_t maxBounces, uint32_t sampleCount, float* rgbaOut,
+                                 int32_t* written)
+{
+    if (!t || !camera) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (written) *written = 0;
+    if (!t->geometryReady || width == 0 || height == 0) return HDCX_OK;
+    if (uint64_t(width) * height > (1ull << 28)) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels");
+    return guarded(t, [&] {
+        ensureOutput(t, width, height);
+        if (!t->fallbackAxisInitialized) {
+            t->fallbackZUp = std::fabs(camera->vertical[2]) > std::fabs(camera->vertical[1]);
+            t->fallbackAxisInitialized = true;
+        }
+        const FrameConst f = makeFrame(t, *camera, width, height, sampleIndex, maxBounces, sampleCount);
+        const uint64_t pathsNeeded = uint64_t(width) * height * 3u * f.sampleCount;
+        const uint32_t shadowPerPath = t->scene.lightCount > 0u ? (t->scene.hasMeshLights ? 2u : 1u)
+                                                                : (t->scene.hasMeshLights ? 2u : 3u);
+        ensurePaths(t, pathsNeeded, std::max(shadowPerPath, 3u));
+        check(cudaMemsetAsync(t->paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
+        StageTimes times;
+        const bool stageTiming = (t->profiling & HDCX_PROFILE_STAGE_TIMES) != 0u;
+        const bool counting = (t->profiling & HDCX_PROFILE_COUNT_TRAVERSAL) != 0u;
+        uint64_t launches = 0;
+        check(cudaEventRecord(t->start, t->stream), "cudaEventRecord");
+        renderFrame(t->scene, f, t->paths, t->fb, t->stream, stageTiming ? &times : nullptr, counting, &launches);
+        check(cudaEventRecord(t->stop, t->stream), "cudaEventRecord");
+        if (rgbaOut) {
+            check(cudaMemcpyAsync(rgbaOut, t->fb.rgba, size_t(width) * height * sizeof(float4), cudaMemcpyDeviceToHost, t->stream),
+                  "read back");
+        }
+        check(cudaStreamSynchronize(t->stream), "render");
+        t->xyzSamples = (sampleIndex == 0 ? 0 : t->xyzSamples) + f.sampleCount;
+        unsigned long long counters[8];
+        check(cudaMemcpy(counters, t->paths.stats, sizeof counters, cudaMemcpyDeviceToHost), "read stats");
+        float ms = 0.0F;
+        check(cudaEventElapsedTime(&ms, t->start, t->stop), "cudaEventElapsedTime");
+        t->stats = hdcx_render_stats{};
+        t->stats.spectral_paths = pathsNeeded;
+        t->stats.extension_rays = counters[0];
+        t->stats.shadow_rays = counters[1];
+        t->stats.subsurface_rays = counters[2];
+        t->stats.render_ms = ms;
+        t->stats.extend_ms = times.extendMs;
+        t->stats.shade_ms = times.shadeMs;
+        t->stats.shadow_ms = times.shadowMs;
+        t->stats.waves = times.waves;
+        t->stats.extend_launches = times.extendLaunches;
+        t->stats.kernel_launches = launches;
+        t->stats.extension_node_visits = counters[3];
+        t->stats.extension_triangle_tests = counters[4];
+        t->stats.shadow_node_visits = counters[5];
+        t->stats.shadow_triangle_tests = counters[6];
+        if (written) *written = 1;
+    });
+}
+
+HDCX_API hdcx_status hdcx_read_rgba(hdcx_tracer* t, float* out, uint64_t count)
+{
+    if (!t || !out) return HDCX_ERROR_INVALID_ARGUMENT;
+    return guarded(t, [&] {
+        const uint64_t n = uint64_t(t->fb.width) * t->fb.height * 4u;
+        if (count < n || !t->fb.rgba) throw std::invalid_argument("output buffer smaller than width*height*4");
+        check(cudaMemcpyAsync(out, t->fb.rgba, n * sizeof(float), cudaMemcpyDeviceToHost, t->stream), "read rgba");
+        check(cudaStreamSynchronize(t->stream), "read rgba");
+    });
+}
+
+HDCX_API hdcx_status hdcx_read_xyz(hdcx_tracer* t, double* out, uint64_t count, uint64_t* samples)
+{
+    if (!t || !out) return HDCX_ERROR_INVALID_ARGUMENT;
+    return guarded(t, [&] {
+        const uint64_t n = uint64_t(t->fb.width) * t->fb.height * 3u;
+        if (count < n || !t->fb.xyz) throw std::invalid_argument("output buffer smaller than width*height*3");
+        check(cudaMemcpyAsync(out, t->fb.xyz, n * sizeof(double), cudaMemcpyDeviceToHost, t->stream), "read xyz");
+        check(cudaStreamSynchronize(t->stream), "read xyz");
+        if (samples) *samples = t->xyzSamples;
+    });
+}
+
+HDCX_API hdcx_status hdcx_device_rgba(hdcx_tracer* t, const float** device)
+{
+    if (!t || !device) return HDCX_ERROR_INVALID_ARGUMENT;
+    *device = reinterpret_cast<const float*>(t->fb.rgba);
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_trace_primary(hdcx_tracer* t, const hdcx_camera* camera, uint32_t width, uint32_t height,
+                                        uint32_t sampleNumber, uint32_t* primitiveOut, float* distanceOut)
+{
+    if (!t || !camera || !primitiveOut) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (!t->geometryReady) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "no geometry");
+    if (width == 0 || height == 0) return HDCX_OK;
+    return guarded(t, [&] {
+        const size_t pixels = size_t(width) * height;
+        DeviceBuffer prims, dists;
+        prims.allocate(pixels * sizeof(uint32_t));
+        dists.allocate(pixels * sizeof(float));
+        const FrameConst f = makeFrame(t, *camera, width, height, 0u, 1u, 1u);
+        tracePrimary(t->scene, f, sampleNumber, prims.as<uint32_t>(), dists.as<float>(), t->stream);
+        check(cudaMemcpyAsync(primitiveOut, prims.ptr, pixels * sizeof(uint32_t), cudaMemcpyDeviceToHost, t->stream), "read ids");
+        if (distanceOut) {
+            check(cudaMemcpyAsync(distanceOut, dists.ptr, pixels * sizeof(float), cudaMemcpyDeviceToHost, t->stream), "read t");
+        }
+        check(cudaStreamSynchronize(t->stream), "trace primary");
+    });
+}
+
+HDCX_API hdcx_status hdcx_get_stats(const hdcx_tracer* t, hdcx_render_stats* stats)
+{
+    if (!t || !stats) return HDCX_ERROR_INVALID_ARGUMENT;
+    *stats = t->stats;
+    return HDCX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1080 @@
+// integrator.cu - wavefront form of the reference's spectral path tracer.
+//
+// The reference runs one megakernel invocation per pixel (GLSL main(),
+// src/gpu/vulkan_path_tracer.cpp:1189-1891): for every sample and each of the
+// three wavelength lanes it loops over bounces, tracing, shading, sampling
+// lights and the BSDF. Here every (pixel, sample, lane) is a path slot of a
+// wave, and each bounce of a wave is four queue-driven kernels:
+//   generate  - camera ray, RNG seed and wavelength of every slot (:1191-1213);
+//   extend    - closest-hit traversal of the extension queue (:1228-1243);
+//   shade     - miss/emission/medium/material/NEE/BSDF/roulette (:1245-1879),
+//               appending surviving paths to the next extension queue and
+//               light-sample rays to the shadow queue;
+//   shadow    - any-hit visibility of the shadow queue (:855-912);
+// and one accumulate kernel per wave adds the lane radiances through the
+// sensor (:1882-1884). A path's radiance gets its contributions in the
+// megakernel's order: light-sample contributions of bounce b are stored per
+// shadow slot and added, in slot order, before anything of bounce b+1.
+// Queues are compacted with warp-aggregated atomics; kernels loop over the
+// device-side queue length, so a frame needs no host round trip.
+#include "integrator.h"
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "device/shading.cuh"
+#include "device/traverse.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace hdcx {
+namespace {
+
+#define CUDA_OK(expr)                                                                                  \
+    do {                                                                                               \
+        cudaError_t err__ = (expr);                                                                    \
+        if (err__ != cudaSuccess) throw std::runtime_error(std::string("render: ") + #expr + ": " +     \
+                                                           cudaGetErrorString(err__));                 \
+    } while (0)
+
+constexpr uint32_t kFlagEnvironmentOnMiss = 1u;
+constexpr uint32_t kFlagPreviousWasDelta = 2u;
+constexpr uint32_t kFlagInsideMedium = 4u;
+
+enum ShadowKind : uint32_t {
+    kShadowAnalytic = 0,
+    kShadowSun = 1,
+    kShadowSky = 2,
+    kShadowMesh = 3,
+};
+
+struct WaveDesc {
+    uint32_t sampleBase;   // first sample offset of the wave (relative to the render)
+    uint32_t samples;      // samples per pixel in the wave
+    uint32_t pixelBase;    // first pixel
+    uint32_t pixels;       // pixels in the wave
+    uint32_t count;        // samples * pixels * 3
+};
+
+__device__ __forceinline__ uint32_t appendIndex(uint32_t* counter)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+    base = g.shfl(base, 0);
+    return base + g.thread_rank();
+}
+
+__device__ __forceinline__ void slotToPath(const WaveDesc& w, const FrameConst& f, uint32_t slot, uint32_t& pixel,
+                                           uint32_t& sampleNumber, uint32_t& lane)
+{
+    lane = slot % 3u;
+    const uint32_t q = slot / 3u;
+    pixel = w.pixelBase + q % w.pixels;
+    sampleNumber = f.sampleIndex + w.sampleBase + q / w.pixels;
+}
+
+// ---------------------------------------------------------------------------
+// generate: main() prologue (vulkan_path_tracer.cpp:1191-1223)
+// ---------------------------------------------------------------------------
+__global__ void generateKernel(FrameConst f, WaveDesc w, PathBuffers p)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot == 0) p.counters[0] = w.count;
+    if (slot >= w.count) return;
+    uint32_t pixel, sampleNumber, lane;
+    slotToPath(w, f, slot, pixel, sampleNumber, lane);
+    const uint32_t px = pixel % f.width, py = pixel / f.width;
+    const uint32_t index = pixel;
+    uint32_t rng = hashState(index ^ (sampleNumber * 0x9e3779b9u) ^ 0xa511e9b3u);
+    const float wavelengthShift = u2f(hashState(index ^ 0x68bc21ebu)) * (1.0f / 4294967296.0f);
+    const float wavelength =
+        380.0f + 400.0f * fract(wavelengthShift + (u2f(sampleNumber & 31u) + 0.5f) / 32.0f + u2f(lane) / 3.0f);
+    const float jx = randomFloat(rng);
+    const float jy = randomFloat(rng);
+    const float u = (u2f(px) + jx) / u2f(f.width);
+    const float v = (u2f(py) + jy) / u2f(f.height);
+    const float3 direction = normalize(f.lowerLeft + u * f.horizontal + v * f.vertical - f.origin);
+    const Spectrum s = makeSpectrum(wavelength);
+    p.rng[slot] = rng;
+    p.wavelength[slot] = wavelength;
+    p.spectrum[slot] = make_float4(s.br, s.bg, s.bb, s.planck);
+    p.throughput[slot] = 1.0f;
+    p.radiance[slot] = 0.0f;
+    p.rayOrigin[slot] = make_float4(f.origin.x, f.origin.y, f.origin.z, 0.0f);
+    p.rayDirection[slot] = make_float4(direction.x, direction.y, direction.z, 0.0f);
+    p.flags[slot] = kFlagEnvironmentOnMiss | kFlagPreviousWasDelta;
+    p.previousPdf[slot] = make_float2(0.0f, 0.0f);
+    p.medium[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    p.contributionValid[slot] = 0;
+    p.contributionValid[p.capacity + slot] = 0;
+    p.contributionValid[2 * p.capacity + slot] = 0;
+    p.queue[0][slot] = slot;
+}
+
+// ---------------------------------------------------------------------------
+// extend: closest hit of every queued ray (vulkan_path_tracer.cpp:1228-1243)
+// ---------------------------------------------------------------------------
+template <Accept kMode, bool kCount>
+__global__ void __launch_bounds__(128) extendKernel(DeviceScene s, PathBuffers p, const uint32_t* queue,
+                                                    const uint32_t* count)
+{
+    const uint32_t n = *count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(p.stats + 0, static_cast<unsigned long long>(n));
+    uint2 work = make_uint2(0u, 0u);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = queue[i];
+        const float4 o = p.rayOrigin[slot];
+        const float4 d = p.rayDirection[slot];
+        HitRecord h;
+        const bool found = traceRay<kMode, false, kCount>(s, xyz(o), xyz(d), 0.001f, 10000.0f, p.rng[slot], h, &work);
+        p.hit[slot] = found ? make_float4(h.t, __uint_as_float(h.primitive), h.b1, h.b2)
+                            : make_float4(0.0f, __uint_as_float(kInvalidPrimitive), 0.0f, 0.0f);
+    }
+    if (kCount) {
+        atomicAdd(p.stats + 3, static_cast<unsigned long long>(work.x));
+        atomicAdd(p.stats + 4, static_cast<unsigned long long>(work.y));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// shade
+// ---------------------------------------------------------------------------
+struct ShadeCtx {
+    const DeviceScene& s;
+    const FrameConst& f;
+    PathBuffers& p;
+    uint32_t slot;
+};
+
+__device__ __forceinline__ void setContribution(PathBuffers& p, uint32_t slot, uint32_t k, float value)
+{
+    p.contribution[k * p.capacity + slot] = value;
+    p.contributionValid[k * p.capacity + slot] = 1;
+}
+
+__device__ __forceinline__ void emitShadow(PathBuffers& p, uint32_t slot, uint32_t k, uint32_t kind, uint32_t light,
+                                           float3 origin, float3 direction, float tmax, float a, float g1, float g2,
+                                           float g3)
+{
+    const uint32_t j = appendIndex(p.counters + 2);
+    p.shadowOrigin[j] = make_float4(origin.x, origin.y, origin.z, tmax);
+    p.shadowDirection[j] = make_float4(direction.x, direction.y, direction.z, a);
+    p.shadowFactors[j] = make_float4(g1, g2, g3, 0.0f);
+    p.shadowSlot[j] = slot * 4u + k;
+    p.shadowInfo[j] = kind | (light << 8);
+    p.contributionValid[k * p.capacity + slot] = 1;
+}
+
+// Light-sample visibility that needs no ray: shadowVisibility's early returns
+// (vulkan_path_tracer.cpp:858-861) give vec3(1.0).
+__device__ __forceinline__ float analyticNeedsRay(const GpuLight& light, float maximumDistance, float& traceDistance)
+{
+    if (light.shadow.x < 0.5f) return 0.0f;
+    traceDistance = maximumDistance;
+    if (light.shadow.y >= 0.0f) traceDistance = gmin(traceDistance, light.shadow.y);
+    if (traceDistance <= 0.001f) return 0.0f;
+    return 1.0f;
+}
+
+// Analytic/sun/sky sample: value = contribution with visibility sv.
+__device__ __forceinline__ float combineShadow(uint32_t kind, float a, float sv, float g1, float g2, float g3)
+{
+    if (kind == kShadowAnalytic) return a * sv * g1 * g2 / g3;
+    if (kind == kShadowSun) return a * sv;
+    return a * sv * g1;  // sky
+}
+
+__device__ void traceSurfaceLightSample(PathBuffers& p, const DeviceScene& s, const Spectrum& spec, uint32_t slot,
+                                        uint32_t k, uint32_t kind, uint32_t lightIndex, const GpuLight& light,
+                                        float3 origin, float3 direction, float maximumDistance, float a, float g1,
+                                        float g2, float g3)
+{
+    float traceDistance = maximumDistance;
+    if (analyticNeedsRay(light, maximumDistance, traceDistance) != 0.0f) {
+        emitShadow(p, slot, k, kind, lightIndex, origin, direction, traceDistance, a, g1, g2, g3);
+    } else {
+        const float sv = reflectanceSpectrum(f3(1.0f), spec);
+        setContribution(p, slot, k, combineShadow(kind, a, sv, g1, g2, g3));
+    }
+}
+
+__device__ bool traceOpaqueBoundary(const DeviceScene& s, PathBuffers& p, float3 origin, float3 direction,
+                                    float3& boundary, float3& boundaryNormal, float& boundaryDistance)
+{
+    // :1130-1151
+    atomicAdd(p.stats + 2, 1ull);
+    HitRecord h;
+    if (!traceRay<Accept::Opaque, false>(s, origin, direction, 0.001f, 10000.0f, 0u, h)) return false;
+    const uint32_t primitive = h.primitive;
+    const float3 p0 = xyz(__ldg(s.vertices + __ldg(s.indices + primitive * 3u + 0u)));
+    const float3 p1 = xyz(__ldg(s.vertices + __ldg(s.indices + primitive * 3u + 1u)));
+    const float3 p2 = xyz(__ldg(s.vertices + __ldg(s.indices + primitive * 3u + 2u)));
+    boundaryDistance = h.t;
+    boundary = origin + direction * boundaryDistance;
+    boundaryNormal = normalize(cross(p1 - p0, p2 - p0));
+    if (dot(boundaryNormal, direction) > 0.0f) boundaryNormal = -boundaryNormal;
+    return true;
+}
+
+__device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float3 entry, float3 outwardNormal,
+                                     float meanFreePath, float albedo, float anisotropy, uint32_t& state,
+                                     float3& exitOrigin, float3& exitDirection, float& attenuation)
+{
+    // :1153-1186
+    const float radius = gmax(meanFreePath, 0.001f);
+    const float sigmaS = 1.0f / radius;
+    const float sigmaA = -glog(clampf(albedo, 0.001f, 0.9999f)) / radius;
+    float3 origin = entry - outwardNormal * 0.003f;
+    float3 direction = cosineHemisphere(-outwardNormal, state);
+    attenuation = 1.0f;
+    for (int step = 0; step < 8; ++step) {
+        float3 boundary, boundaryNormal;
+        float boundaryDistance;
+        if (!traceOpaqueBoundary(s, p, origin, direction, boundary, boundaryNormal, boundaryDistance)) return false;
+        const float scatterDistance = -glog(gmax(1.0f - randomFloat(state), 1e-6f)) / sigmaS;
+        const bool forceExit = step == 7;
+        const float travel = forceExit ? boundaryDistance : gmin(scatterDistance, boundaryDistance);
+        attenuation = attenuation * gexp(-sigmaA * travel);
+        if (forceExit || scatterDistance >= boundaryDistance) {
+            exitDirection = direction;
+            exitOrigin = boundary + direction * 0.003f;
+            return true;
+        }
+        origin = origin + direction * scatterDistance;
+        direction = sampleHenyeyGreenstein(direction, anisotropy, state);
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce,
+                                                   const uint32_t* queue, const uint32_t* count, uint32_t* nextQueue,
+                                                   uint32_t* nextCount)
+{
+    const uint32_t n = *count;
+    const bool lastBounce = bounce + 1u >= f.maxBounces;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = queue[i];
+        float radiance = p.radiance[slot];
+        // Light-sample contributions of the previous bounce, in slot order.
+        for (uint32_t k = 0; k < 3u; ++k) {
+            uint8_t& valid = p.contributionValid[k * p.capacity + slot];
+            if (valid) {
+                radiance += p.contribution[k * p.capacity + slot];
+                valid = 0;
+            }
+        }
+        const Spectrum spec = spectrumFromBasis(p.wavelength[slot], p.spectrum[slot]);
+        const float wavelength = spec.wavelength;
+        uint32_t rng = p.rng[slot];
+        float throughput = p.throughput[slot];
+        uint32_t flags = p.flags[slot];
+        bool environmentOnMiss = (flags & kFlagEnvironmentOnMiss) != 0u;
+        bool previousWasDelta = (flags & kFlagPreviousWasDelta) != 0u;
+        bool insideMedium = (flags & kFlagInsideMedium) != 0u;
+        float2 previousPdf = p.previousPdf[slot];
+        float previousBsdfPdf = previousPdf.x;
+        float previousEnvironmentLightPdf = previousPdf.y;
+        float4 medium = p.medium[slot];
+        float mediumAbsorption = medium.x, mediumScattering = medium.y, mediumAnisotropy = medium.z;
+        float3 rayOrigin = xyz(p.rayOrigin[slot]);
+        float3 rayDirection = xyz(p.rayDirection[slot]);
+        const float4 hitRec = p.hit[slot];
+        const uint32_t primitive = __float_as_uint(hitRec.y);
+        bool alive = true;
+
+        if (primitive == kInvalidPrimitive) {
+            // :1245-1255
+            if (environmentOnMiss) {
+                const float misWeight = previousWasDelta ? 1.0f : powerHeuristic(previousBsdfPdf, previousEnvironmentLightPdf);
+                radiance += throughput * misWeight * illuminantSpectrum(environment(s, f, rayDirection), spec);
+            }
+            p.radiance[slot] = radiance;
+            continue;
+        }
+
+        do {  // one bounce; `break` ends shading of this bounce
+            const uint32_t i0 = __ldg(s.indices + primitive * 3u + 0u);
+            const uint32_t i1 = __ldg(s.indices + primitive * 3u + 1u);
+            const uint32_t i2 = __ldg(s.indices + primitive * 3u + 2u);
+            const float3 p0 = xyz(__ldg(s.vertices + i0));
+            const float3 p1 = xyz(__ldg(s.vertices + i1));
+            const float3 p2 = xyz(__ldg(s.vertices + i2));
+            const float3 geometricNormal = normalize(cross(p1 - p0, p2 - p0));
+            const bool frontFace = dot(geometricNormal, rayDirection) < 0.0f;
+            const float3 orientedGeometricNormal = frontFace ? geometricNormal : -geometricNormal;
+            const float b1 = hitRec.z, b2 = hitRec.w;
+            const float3 authoredNormal = surfaceShadingNormal(s, primitive, b1, b2, geometricNormal);
+            float3 normal = frontFace ? authoredNormal : -authoredNormal;
+            const float2 uv0 = __ldg(s.texcoords + primitive * 3u + 0u);
+            const float2 uv1 = __ldg(s.texcoords + primitive * 3u + 1u);
+            const float2 uv2 = __ldg(s.texcoords + primitive * 3u + 2u);
+            const float2 surfaceUv = surfaceTextureCoordinates(s, primitive, b1, b2);
+            const float distance = hitRec.x;
+            const float3 hit = rayOrigin + rayDirection * distance;
+            if (insideMedium) {
+                // :1279-1295
+                if (mediumScattering > 0.0f) {
+                    const float scatterDistance = -glog(gmax(1.0f - randomFloat(rng), 1e-6f)) / mediumScattering;
+                    if (scatterDistance < distance) {
+                        throughput = throughput * gexp(-mediumAbsorption * scatterDistance);
+                        rayOrigin = rayOrigin + rayDirection * scatterDistance;
+                        rayDirection = sampleHenyeyGreenstein(rayDirection, mediumAnisotropy, rng);
+                        environmentOnMiss = true;
+                        previousWasDelta = true;
+                        previousBsdfPdf = 0.0f;
+                        break;
+                    }
+                }
+                throughput = throughput * gexp(-mediumAbsorption * distance);
+            }
+            const GpuMaterial* material = s.materials + __ldg(s.triangleMaterials + primitive);
+            float3 baseColorRgb = xyz(material->baseColorMetalness);
+            if (material->textureIndices0.x != kMissingTexture) {
+                const float4 sample = sampleMaterialTexture(s, material->textureIndices0.x, surfaceUv, f4(baseColorRgb, 1.0f));
+                const float scaleW = material->baseColorTextureScale.w;
+                const int channel = static_cast<int>(roundf(scaleW));
+                float3 sourceColor;
+                if (channel < 0) {
+                    sourceColor = f3(sample.x, sample.y, sample.z);
+                } else {
+                    const int c = min(channel, 3);
+                    sourceColor = f3(c == 0 ? sample.x : (c == 1 ? sample.y : (c == 2 ? sample.z : sample.w)));
+                }
+                baseColorRgb = xyz(material->baseColorTextureBias) + xyz(material->baseColorTextureScale) * sourceColor;
+            }
+            const float baseColor = reflectanceSpectrum(baseColorRgb, spec);
+            const float metalness = clampf(
+                sampleMaterialTexture(s, material->textureIndices0.y, surfaceUv, f4(material->baseColorMetalness.w)).x, 0.0f, 1.0f);
+            const float4 roughnessSample = sampleMaterialTexture(
+                s, material->textureIndices0.z, surfaceUv,
+                make_float4(material->emissionRoughness.w, material->subsurfaceColor.w, 0.0f, 1.0f));
+            const float2 roughness = make_float2(clampf(roughnessSample.x, 0.02f, 1.0f), clampf(roughnessSample.y, 0.02f, 1.0f));
+            const float diffuseRoughness = clampf(
+                sampleMaterialTexture(s, material->textureIndices4.z, surfaceUv, f4(material->diffuseProperties.x)).x, 0.0f, 1.0f);
+            const float diffuseWeight = clampf(
+                sampleMaterialTexture(s, material->textureIndices4.w, surfaceUv, f4(material->diffuseProperties.z)).x, 0.0f, 1.0f);
+            const uint32_t diffuseModel = static_cast<uint32_t>(material->diffuseProperties.y + 0.5f);
+            normal = applyNormalMap(s, material->textureIndices1.y, material->coatWeightRoughnessIor.w > 0.5f,
+                                    material->subsurfaceWeightScale.w, surfaceUv, normal, p0, p1, p2, uv0, uv1, uv2);
+            const float3 tangent = surfaceTangent(normal, p0, p1, p2, uv0, uv1, uv2);
+            const float3 emissionRgb = surfaceEmissionRgb(s, primitive, surfaceUv);
+            const float emission = illuminantSpectrum(emissionRgb, spec);
+            float emissionMisWeight = 1.0f;
+            if (!previousWasDelta && (emissionRgb.x > 0.0f || emissionRgb.y > 0.0f || emissionRgb.z > 0.0f)) {
+                const float emissionCosine = fabsf(dot(geometricNormal, -rayDirection));
+                const float lightPdf = emissionCosine <= 0.0f
+                                           ? 0.0f
+                                           : __ldg(&s.emissive[primitive].y) * (distance * distance) / emissionCosine;
+                emissionMisWeight = powerHeuristic(previousBsdfPdf, lightPdf);
+            }
+            radiance += throughput * emission * emissionMisWeight;
+
+            const float transmission = clampf(material->transmissionOpacityIor.x, 0.0f, 1.0f);
+            float3 transmissionColorRgb = xyz(material->transmissionColorThinWalled);
+            if (transmission > 0.0f) {
+                const float4 t = sampleMaterialTexture(s, material->textureIndices1.z, surfaceUv, f4(transmissionColorRgb, 1.0f));
+                transmissionColorRgb = f3(t.x, t.y, t.z);
+            }
+            const float transmissionColor = reflectanceSpectrum(transmissionColorRgb, spec);
+            float subsurface = 0.0f;
+            float diffuseColor = baseColor;
+            float3 subsurfaceColorRgb = xyz(material->subsurfaceColor);
+            float3 subsurfaceRadiusRgb = make_float3(gmax(material->subsurfaceRadius.x, 0.001f), gmax(material->subsurfaceRadius.y, 0.001f),
+                                                     gmax(material->subsurfaceRadius.z, 0.001f));
+            if (material->subsurfaceWeightScale.x > 0.0f || material->textureIndices2.x != kMissingTexture) {
+                subsurface = clampf(sampleMaterialTexture(s, material->textureIndices2.x, surfaceUv,
+                                                          f4(material->subsurfaceWeightScale.x)).x, 0.0f, 1.0f);
+                if (subsurface > 0.0f) {
+                    const float4 c = sampleMaterialTexture(s, material->textureIndices2.y, surfaceUv,
+                                                           f4(xyz(material->subsurfaceColor), 1.0f));
+                    subsurfaceColorRgb = f3(c.x, c.y, c.z);
+                    const float4 r = sampleMaterialTexture(s, material->textureIndices2.z, surfaceUv,
+                                                           f4(xyz(material->subsurfaceRadius), 1.0f));
+                    subsurfaceRadiusRgb = make_float3(gmax(r.x, 0.001f), gmax(r.y, 0.001f), gmax(r.z, 0.001f));
+                    const float subsurfaceColor = reflectanceSpectrum(subsurfaceColorRgb, spec);
+                    diffuseColor = mix(baseColor, subsurfaceColor, subsurface);
+                }
+            }
+            const float ior = dispersedIor(gmax(material->transmissionOpacityIor.z, 1.0001f), material->transmissionMedium.z,
+                                           material->transmissionMedium.w, wavelength);
+            const float specularWeight = clampf(
+                sampleMaterialTexture(s, material->textureIndices3.x, surfaceUv, f4(material->specularWeightColor.x)).x, 0.0f, 1.0f);
+            const float4 specularColorSample = sampleMaterialTexture(
+                s, material->textureIndices3.y, surfaceUv,
+                make_float4(material->specularWeightColor.y, material->specularWeightColor.z, material->specularWeightColor.w, 1.0f));
+            const float specularColor =
+                reflectanceSpectrum(f3(specularColorSample.x, specularColorSample.y, specularColorSample.z), spec);
+            float dielectricReflectance = (ior - 1.0f) / (ior + 1.0f);
+            dielectricReflectance = dielectricReflectance * dielectricReflectance;
+            const float f0 = mix(clampf(dielectricReflectance * specularWeight * specularColor, 0.0f, 1.0f), baseColor, metalness);
+            float coat = 0.0f;
+            float2 coatRoughness = make_float2(material->coatWeightRoughnessIor.y, material->subsurfaceRadius.w);
+            float coatF0 = 0.0f;
+            if (material->coatWeightRoughnessIor.x > 0.0f || material->textureIndices3.z != kMissingTexture) {
+                coat = clampf(sampleMaterialTexture(s, material->textureIndices3.z, surfaceUv,
+                                                    f4(material->coatWeightRoughnessIor.x)).x, 0.0f, 1.0f);
+                if (coat > 0.0f) {
+                    const float4 cc = sampleMaterialTexture(s, material->textureIndices3.w, surfaceUv, f4(xyz(material->coatColor), 1.0f));
+                    const float coatColor = reflectanceSpectrum(f3(cc.x, cc.y, cc.z), spec);
+                    const float4 cr = sampleMaterialTexture(s, material->textureIndices4.x, surfaceUv,
+                                                            make_float4(coatRoughness.x, coatRoughness.y, 0.0f, 1.0f));
+                    coatRoughness = make_float2(clampf(cr.x, 0.02f, 1.0f), clampf(cr.y, 0.02f, 1.0f));
+                    const float coatIor = gmax(material->coatWeightRoughnessIor.z, 1.0001f);
+                    float coatReflectance = (coatIor - 1.0f) / (coatIor + 1.0f);
+                    coatReflectance = coatReflectance * coatReflectance;
+                    coatF0 = clampf(coatReflectance * coatColor, 0.0f, 1.0f);
+                }
+            }
+            const float sheen = clampf(sampleMaterialTexture(s, material->textureIndices1.w, surfaceUv, f4(material->coatColor.w)).x, 0.0f, 1.0f);
+            const float4 sheenColorSample = sampleMaterialTexture(s, material->textureIndices2.w, surfaceUv,
+                                                                  f4(xyz(material->sheenColorMode), 1.0f));
+            const float sheenColor = reflectanceSpectrum(f3(sheenColorSample.x, sheenColorSample.y, sheenColorSample.z), spec);
+            const float sheenRoughness = clampf(
+                sampleMaterialTexture(s, material->textureIndices4.y, surfaceUv, f4(material->transmissionScatter.w)).x, 0.01f, 1.0f);
+            const bool sheenZeltner = material->sheenColorMode.w > 0.5f;
+            const float translucentWeight = clampf(
+                sampleMaterialTexture(s, material->textureIndices5.x, surfaceUv, f4(material->translucentColorWeight.w)).x, 0.0f, 1.0f);
+            const float4 translucentSample = sampleMaterialTexture(s, material->textureIndices5.y, surfaceUv,
+                                                                   f4(xyz(material->translucentColorWeight), 1.0f));
+            const float translucentColor = reflectanceSpectrum(f3(translucentSample.x, translucentSample.y, translucentSample.z), spec);
+
+            const float3 viewDirection = normalize(-rayDirection);
+            const float nDotView = gmax(dot(normal, viewDirection), 0.0f);
+            const float sheenAlbedo = sheenZeltner ? sheenZeltnerDirectionalAlbedo(nDotView, sheenRoughness)
+                                                   : sheenDirectionalAlbedo(nDotView, sheenRoughness);
+            const float sheenProbability = clampf(sheen * sheenAlbedo * luminance1(sheenColor), 0.0f, 0.95f);
+            const float coatContribution = coat > 0.0f ? coat * fresnelSchlick(nDotView, coatF0) : 0.0f;
+            const float coatProbability = clampf(luminance1(coatContribution), 0.0f, 0.95f);
+            const float baseFresnel = fresnelSchlick(nDotView, f0);
+            const float specularContribution = baseFresnel;
+            const float diffuseContribution =
+                (1.0f - baseFresnel) * diffuseWeight * (1.0f - translucentWeight) * (1.0f - metalness) * diffuseColor;
+            const float translucentContribution = (1.0f - baseFresnel) * translucentWeight * (1.0f - metalness) * translucentColor;
+            const float specularEnergy = luminance1(specularContribution);
+            const float diffuseEnergy = luminance1(diffuseContribution);
+            const float translucentEnergy = luminance1(translucentContribution);
+            const float baseEnergy = diffuseEnergy + translucentEnergy;
+            const float specularProbability = clampf(specularEnergy / gmax(specularEnergy + baseEnergy, 1e-5f), 0.05f, 0.95f);
+            const float translucentProbability = baseEnergy > 1e-5f ? translucentEnergy / baseEnergy : 0.0f;
+            const uint32_t lightCount = s.lightCount;
+            const bool hasMeshLights = s.hasMeshLights != 0u;
+
+            SurfaceParams sp;
+            sp.diffuseColor = diffuseColor;
+            sp.transmission = transmission;
+            sp.subsurface = subsurface;
+            sp.diffuseWeight = diffuseWeight;
+            sp.diffuseRoughness = diffuseRoughness;
+            sp.diffuseModel = diffuseModel;
+            sp.translucentWeight = translucentWeight;
+            sp.translucentColor = translucentColor;
+            sp.metalness = metalness;
+            sp.roughness = roughness;
+            sp.f0 = f0;
+            sp.coat = coat;
+            sp.coatRoughness = coatRoughness;
+            sp.coatF0 = coatF0;
+            sp.sheen = sheen;
+            sp.sheenColor = sheenColor;
+            sp.sheenRoughness = sheenRoughness;
+            sp.sheenZeltner = sheenZeltner;
+
+            if (lightCount > 0u) {
+                // :1469-1592 analytic light sample
+                const float directSpecularEnergy = specularEnergy + luminance1(coatContribution) + sheenProbability;
+                uint32_t lightIndex;
+                float lightSelectionPdf;
+                sampleAnalyticLight(s, hit, normal, diffuseEnergy, directSpecularEnergy, translucentEnergy, rng, lightIndex,
+                                    lightSelectionPdf);
+                const GpuLight& light = s.lights[lightIndex];
+                float3 lightDirection = f3(0.0f, 1.0f, 0.0f);
+                float3 lightRadiance = f3(0.0f);
+                float inversePdf = 0.0f;
+                float maximumShadowDistance = 10000.0f;
+                const uint32_t type = light.textureInfo.z;
+                if (type == 0u) {
+                    float lightPdf = 0.0f;
+                    sampleDomeLight(s, light, rng, lightDirection, lightPdf);
+                    lightRadiance = sampleDome(s, light, lightDirection);
+                    inversePdf = lightPdf > 0.0f ? 1.0f / lightPdf : 0.0f;
+                } else if (type == 5u) {
+                    const float halfAngle = 0.5f * radians(clampf(light.geometry.z, 0.0f, 359.999f));
+                    if (halfAngle <= 1e-6f) {
+                        lightDirection = normalize(xyz(light.basisZ));
+                        inversePdf = 1.0f;
+                    } else {
+                        const float cosineMaximum = gcos(halfAngle);
+                        const float cosineTheta = mix(cosineMaximum, 1.0f, randomFloat(rng));
+                        const float sineTheta = sqrtf(gmax(1.0f - cosineTheta * cosineTheta, 0.0f));
+                        const float phi = kTwoPi * randomFloat(rng);
+                        lightDirection = normalize(xyz(light.basisX) * (gcos(phi) * sineTheta) +
+                                                   xyz(light.basisY) * (gsin(phi) * sineTheta) + xyz(light.basisZ) * cosineTheta);
+                        inversePdf = 1.0f;
+                    }
+                    lightRadiance = xyz(light.colorIntensity) * light.colorIntensity.w;
+                } else {
+                    const float lu = randomFloat(rng);
+                    const float lv = randomFloat(rng);
+                    float3 lightPosition = xyz(light.position);
+                    float3 lightNormal = -normalize(xyz(light.basisZ));
+                    if (type == 1u) {
+                        lightPosition = lightPosition + ((lu - 0.5f) * xyz(light.axisU) + (lv - 0.5f) * xyz(light.axisV));
+                    } else if (type == 2u) {
+                        const float diskRadius = sqrtf(lu);
+                        const float diskPhi = kTwoPi * lv;
+                        lightPosition = lightPosition + diskRadius * (gcos(diskPhi) * xyz(light.axisU) + gsin(diskPhi) * xyz(light.axisV));
+                    } else if (type == 3u) {
+                        lightNormal = uniformSphere(rng);
+                        lightPosition = lightPosition + light.geometry.x * lightNormal;
+                    } else if (type == 4u) {
+                        const float cylinderPhi = kTwoPi * lv;
+                        lightNormal = normalize(gcos(cylinderPhi) * xyz(light.basisY) + gsin(cylinderPhi) * xyz(light.basisZ));
+                        lightPosition = lightPosition + ((lu - 0.5f) * xyz(light.axisU) + light.geometry.x * lightNormal);
+                    }
+                    const float3 toLight = lightPosition - hit;
+                    const float distanceSquared = dot(toLight, toLight);
+                    const float lightDistance = sqrtf(gmax(distanceSquared, 1e-8f));
+                    lightDirection = toLight / lightDistance;
+                    const float emissionCosine = gmax(dot(lightNormal, -lightDirection), 0.0f);
+                    if (emissionCosine > 0.0f && light.controls.w > 0.0f) {
+                        const float shapingCosine = gmax(dot(normalize(xyz(light.basisZ)), lightDirection), 0.0f);
+                        const float focus = gpow(shapingCosine, gmax(light.shaping.x, 0.0f));
+                        const float3 focusColor = mix(xyz(light.focusTint), f3(1.0f), focus);
+                        float3 textureValue = f3(1.0f);
+                        if (!(type != 1u || light.textureInfo.x == kMissingTexture)) {
+                            const float4 t = textureSample(s, light.textureInfo.x, make_float2(lu, lv));
+                            textureValue = f3(t.x, t.y, t.z);
+                        }
+                        lightRadiance = xyz(light.colorIntensity) * light.colorIntensity.w * textureValue * focusColor *
+                                        shapingConeFactor(light, shapingCosine);
+                        inversePdf = light.controls.w * emissionCosine / gmax(distanceSquared, 1e-8f);
+                        maximumShadowDistance = gmax(lightDistance - 0.003f, 0.001f);
+                    }
+                }
+                if (inversePdf > 0.0f) {
+                    const float direct = evaluateDirectSurface(normal, tangent, viewDirection, lightDirection, sp,
+                                                               light.controls.x, light.controls.y);
+                    if (direct > 0.0f) {
+                        const float spectralLight = illuminantSpectrum(lightRadiance, spec);
+                        const float misWeight =
+                            type == 0u ? powerHeuristic(environmentLightPdf(s, hit, normal, lightDirection, diffuseEnergy,
+                                                                            directSpecularEnergy, translucentEnergy),
+                                                        surfaceReflectionPdf(normal, tangent, viewDirection, lightDirection,
+                                                                             roughness, coatRoughness, sheenProbability,
+                                                                             coatProbability, specularProbability,
+                                                                             translucentProbability))
+                                       : 1.0f;
+                        const float a = throughput * direct * spectralLight;
+                        traceSurfaceLightSample(p, s, spec, slot, 0u, kShadowAnalytic, lightIndex, light,
+                                                offsetSurfaceOrigin(hit, orientedGeometricNormal, lightDirection), lightDirection,
+                                                maximumShadowDistance, a, inversePdf, misWeight, gmax(lightSelectionPdf, 1e-8f));
+                    }
+                }
+            } else if (!hasMeshLights) {
+                // :1593-1668 fallback sun and sky
+                const bool zUp = f.zUp != 0u;
+                const float3 up = zUp ? f3(0.0f, 0.0f, 1.0f) : f3(0.0f, 1.0f, 0.0f);
+                const float3 azimuth = zUp ? normalize(f3(1.0f, 1.0f, 0.0f)) : normalize(f3(1.0f, 0.0f, 1.0f));
+                const float3 sunDirection = normalize(up * 0.9659258f + azimuth * 0.2588190f);
+                const GpuLight& dummy = s.lights[0];
+                const float direct = evaluateDirectSurface(normal, tangent, viewDirection, sunDirection, sp, 1.0f, 1.0f);
+                if (direct > 0.0f) {
+                    const float spectralSun = illuminantSpectrum(f3(3.45575f, 3.14159f, 2.82743f), spec);
+                    traceSurfaceLightSample(p, s, spec, slot, 0u, kShadowSun, 0u, dummy,
+                                            offsetSurfaceOrigin(hit, orientedGeometricNormal, sunDirection), sunDirection,
+                                            10000.0f, throughput * direct * spectralSun, 0.0f, 0.0f, 0.0f);
+                }
+                const float3 skyDirection = cosineHemisphere(normal, rng);
+                const float skyDirect = evaluateDirectSurface(normal, tangent, viewDirection, skyDirection, sp, 1.0f, 0.0f);
+                if (skyDirect > 0.0f) {
+                    const float spectralSky = illuminantSpectrum(environment(s, f, skyDirection), spec);
+                    traceSurfaceLightSample(p, s, spec, slot, 1u, kShadowSky, 0u, dummy,
+                                            offsetSurfaceOrigin(hit, orientedGeometricNormal, skyDirection), skyDirection,
+                                            10000.0f, throughput * skyDirect * spectralSky,
+                                            kPi / gmax(dot(normal, skyDirection), 1e-4f), 0.0f, 0.0f);
+                }
+                if (translucentWeight > 0.0f) {
+                    const float3 backSkyDirection = cosineHemisphere(-normal, rng);
+                    const float backSkyDirect =
+                        evaluateDirectSurface(normal, tangent, viewDirection, backSkyDirection, sp, 1.0f, 0.0f);
+                    if (backSkyDirect > 0.0f) {
+                        const float spectralSky = illuminantSpectrum(environment(s, f, backSkyDirection), spec);
+                        traceSurfaceLightSample(p, s, spec, slot, 2u, kShadowSky, 0u, dummy,
+                                                offsetSurfaceOrigin(hit, orientedGeometricNormal, backSkyDirection),
+                                                backSkyDirection, 10000.0f, throughput * backSkyDirect * spectralSky,
+                                                kPi / gmax(dot(-normal, backSkyDirection), 1e-4f), 0.0f, 0.0f);
+                    }
+                }
+            }
+
+            if (hasMeshLights) {
+                // :1670-1731 emissive-triangle sample
+                const uint32_t primitiveCount = s.primitiveCount;
+                const float target = randomFloat(rng);
+                uint32_t low = 0u, high = primitiveCount - 1u;
+                while (low < high) {
+                    const uint32_t middle = low + (high - low) / 2u;
+                    if (target <= __ldg(&s.emissive[middle].x)) high = middle;
+                    else low = middle + 1u;
+                }
+                const uint32_t lightPrimitive = low;
+                if (lightPrimitive != primitive && __ldg(&s.emissive[lightPrimitive].y) > 0.0f) {
+                    const float root = sqrtf(randomFloat(rng));
+                    const float second = randomFloat(rng);
+                    const float w0 = 1.0f - root, w1 = root * (1.0f - second), w2 = root * second;
+                    const float3 lightP0 = xyz(__ldg(s.vertices + __ldg(s.indices + lightPrimitive * 3u + 0u)));
+                    const float3 lightP1 = xyz(__ldg(s.vertices + __ldg(s.indices + lightPrimitive * 3u + 1u)));
+                    const float3 lightP2 = xyz(__ldg(s.vertices + __ldg(s.indices + lightPrimitive * 3u + 2u)));
+                    const float3 lightPosition = lightP0 * w0 + lightP1 * w1 + lightP2 * w2;
+                    const float3 lightNormal = normalize(cross(lightP1 - lightP0, lightP2 - lightP0));
+                    const float3 toLight = lightPosition - hit;
+                    const float distanceSquared = dot(toLight, toLight);
+                    const float lightDistance = sqrtf(gmax(distanceSquared, 1e-8f));
+                    const float3 lightDirection = toLight / lightDistance;
+                    const float emissionCosine = fabsf(dot(lightNormal, -lightDirection));
+                    const float lightPdf =
+                        emissionCosine <= 0.0f ? 0.0f : __ldg(&s.emissive[lightPrimitive].y) * distanceSquared / emissionCosine;
+                    if (lightPdf > 0.0f) {
+                        const float direct = evaluateDirectSurface(normal, tangent, viewDirection, lightDirection, sp, 1.0f, 1.0f);
+                        if (direct > 0.0f) {
+                            const float2 lightUv = surfaceTextureCoordinates(s, lightPrimitive, w1, w2);
+                            float3 lightEmissionRgb = surfaceEmissionRgb(s, lightPrimitive, lightUv);
+                            lightEmissionRgb = lightEmissionRgb * surfaceOpacity(s, lightPrimitive, w1, w2);
+                            const float spectralLight = illuminantSpectrum(lightEmissionRgb, spec);
+                            const float bsdfPdf = surfaceReflectionPdf(normal, tangent, viewDirection, lightDirection, roughness,
+                                                                       coatRoughness, sheenProbability, coatProbability,
+                                                                       specularProbability, translucentProbability);
+                            const float misWeight = powerHeuristic(lightPdf, bsdfPdf);
+                            const float a = throughput * direct * spectralLight;
+                            const float maxDistance = gmax(lightDistance - 0.003f, 0.001f);
+                            const float f1 = misWeight / lightPdf;
+                            if (maxDistance <= 0.001f) {
+                                setContribution(p, slot, 1u, a * f1);
+                            } else {
+                                emitShadow(p, slot, 1u, kShadowMesh, 0u,
+                                           offsetSurfaceOrigin(hit, orientedGeometricNormal, lightDirection), lightDirection,
+                                           maxDistance, a, f1, 0.0f, 0.0f);
+                            }
+                        }
+                    }
+                }
+            }
+
+            if (randomFloat(rng) < transmission) {
+                // :1735-1777
+                const float eta = frontFace ? 1.0f / ior : ior;
+                const float cosTheta = gmin(dot(-rayDirection, normal), 1.0f);
+                float r0 = (1.0f - ior) / (1.0f + ior);
+                r0 = r0 * r0;
+                const float fresnel = r0 + (1.0f - r0) * gpow(1.0f - cosTheta, 5.0f);
+                const float3 refracted = refract(rayDirection, normal, eta);
+                const bool totalInternalReflection = dot(refracted, refracted) < 1e-8f;
+                const bool thinWalled = material->transmissionColorThinWalled.w > 0.5f;
+                bool refractedThroughBoundary = false;
+                if (totalInternalReflection || randomFloat(rng) < fresnel) {
+                    rayDirection = reflect(rayDirection, normal);
+                } else {
+                    rayDirection = thinWalled ? rayDirection : normalize(refracted);
+                    refractedThroughBoundary = !thinWalled;
+                }
+                const float transmissionDepth = gmax(material->transmissionMedium.x, 0.0f);
+                throughput = throughput * (transmissionDepth > 0.0f ? 1.0f : transmissionColor);
+                if (refractedThroughBoundary) {
+                    if (frontFace) {
+                        const float spectralTransmission = gmax(transmissionColor, 0.001f);
+                        mediumAbsorption = transmissionDepth > 0.0f ? -glog(spectralTransmission) / transmissionDepth : 0.0f;
+                        const float spectralScatter = gmax(reconstructRgb(xyz(material->transmissionScatter), spec), 0.0f);
+                        mediumScattering = transmissionDepth > 0.0f ? spectralScatter / transmissionDepth : spectralScatter;
+                        mediumAnisotropy = material->transmissionMedium.y;
+                        insideMedium = true;
+                    } else {
+                        insideMedium = false;
+                        mediumAbsorption = 0.0f;
+                        mediumScattering = 0.0f;
+                    }
+                }
+                rayOrigin = hit + rayDirection * 0.002f;
+                environmentOnMiss = true;
+                previousWasDelta = true;
+                previousBsdfPdf = 0.0f;
+                break;
+            }
+
+            // :1779-1858 BSDF sampling chain
+            environmentOnMiss = false;
+            rayOrigin = hit + orientedGeometricNormal * 0.002f;
+            if (sheenProbability > 0.0f && randomFloat(rng) < sheenProbability) {
+                rayDirection = cosineHemisphere(normal, rng);
+                const float sheenPdf = gmax(dot(normal, rayDirection), 0.0f) / kPi;
+                const float response = sheenResponse(normal, viewDirection, rayDirection, sheenRoughness, sheenZeltner);
+                throughput = throughput * (sheen * sheenColor * response / gmax(sheenProbability * sheenPdf, 1e-6f));
+                environmentOnMiss = true;
+            } else {
+                throughput = throughput * ((1.0f - sheen * sheenAlbedo) / gmax(1.0f - sheenProbability, 1e-4f));
+                if (coatProbability > 0.0f && randomFloat(rng) < coatProbability) {
+                    const float3 incident = rayDirection;
+                    rayDirection = sampleGGXReflectionAnisotropic(rayDirection, normal, tangent, coatRoughness, rng);
+                    throughput = throughput * (coat * ggxSampleWeightAnisotropic(incident, rayDirection, normal, tangent,
+                                                                                 coatRoughness, coatF0) / coatProbability);
+                    environmentOnMiss = gmax(coatRoughness.x, coatRoughness.y) < 0.2f;
+                } else {
+                    throughput = throughput * ((1.0f - coatContribution) / gmax(1.0f - coatProbability, 1e-4f));
+                    if (randomFloat(rng) < specularProbability) {
+                        const float3 incident = rayDirection;
+                        rayDirection = sampleGGXReflectionAnisotropic(rayDirection, normal, tangent, roughness, rng);
+                        throughput = throughput * (ggxSampleWeightAnisotropic(incident, rayDirection, normal, tangent,
+                                                                              roughness, f0) / specularProbability);
+                        environmentOnMiss = gmax(roughness.x, roughness.y) < 0.2f;
+                    } else {
+                        if (translucentProbability > 0.0f && randomFloat(rng) < translucentProbability) {
+                            throughput = throughput * (translucentContribution /
+                                                       gmax((1.0f - specularProbability) * translucentProbability, 1e-4f));
+                            rayDirection = cosineHemisphere(-normal, rng);
+                            rayOrigin = offsetSurfaceOrigin(hit, orientedGeometricNormal, rayDirection);
+                        } else {
+                            throughput = throughput * (diffuseContribution /
+                                                       gmax((1.0f - specularProbability) * (1.0f - translucentProbability), 1e-4f));
+                            bool walked = false;
+                            if (subsurface > 0.0f && randomFloat(rng) < subsurface) {
+                                const float radius = gmax(reconstructRgb(subsurfaceRadiusRgb, spec) *
+                                                              gmax(material->subsurfaceWeightScale.y, 0.0f),
+                                                          0.001f);
+                                const float albedo = reflectanceSpectrum(subsurfaceColorRgb, spec);
+                                float3 exitOrigin, exitDirection;
+                                float attenuation;
+                                if (randomWalkSubsurface(s, p, hit, orientedGeometricNormal, radius, albedo,
+                                                         material->subsurfaceWeightScale.z, rng, exitOrigin, exitDirection,
+                                                         attenuation)) {
+                                    throughput = throughput * attenuation;
+                                    rayOrigin = exitOrigin;
+                                    rayDirection = exitDirection;
+                                    environmentOnMiss = true;
+                                    previousWasDelta = true;
+                                    previousBsdfPdf = 0.0f;
+                                    walked = true;
+                                }
+                            }
+                            if (walked) break;
+                            rayDirection = cosineHemisphere(normal, rng);
+                            const float lambertResponse = gmax(dot(normal, rayDirection), 0.0f) / kPi;
+                            throughput = throughput * (evaluateDiffuseReflection(normal, viewDirection, rayDirection, diffuseColor,
+                                                                                 diffuseRoughness, diffuseModel) /
+                                                       gmax(lambertResponse, 1e-6f));
+                        }
+                    }
+                }
+            }
+            if (lightCount > 0u || hasMeshLights) {
+                // :1859-1874
+                previousBsdfPdf = surfaceReflectionPdf(normal, tangent, viewDirection, rayDirection, roughness, coatRoughness,
+                                                       sheenProbability, coatProbability, specularProbability,
+                                                       translucentProbability);
+                previousWasDelta = false;
+                environmentOnMiss = true;
+                previousEnvironmentLightPdf =
+                    lightCount > 0u ? environmentLightPdf(s, hit, normal, rayDirection, diffuseEnergy,
+                                                          specularEnergy + luminance1(coatContribution) + sheenProbability,
+                                                          translucentEnergy)
+                                    : 0.0f;
+            }
+            if (bounce >= 2u) {
+                // :1875-1879 Russian roulette
+                const float survival = clampf(throughput, 0.1f, 0.95f);
+                if (randomFloat(rng) > survival) {
+                    alive = false;
+                    break;
+                }
+                throughput = throughput / survival;
+            }
+        } while (false);
+
+        p.radiance[slot] = radiance;
+        if (!alive || lastBounce) continue;
+        p.rng[slot] = rng;
+        p.throughput[slot] = throughput;
+        p.flags[slot] = (environmentOnMiss ? kFlagEnvironmentOnMiss : 0u) | (previousWasDelta ? kFlagPreviousWasDelta : 0u) |
+                        (insideMedium ? kFlagInsideMedium : 0u);
+        p.previousPdf[slot] = make_float2(previousBsdfPdf, previousEnvironmentLightPdf);
+        p.medium[slot] = make_float4(mediumAbsorption, mediumScattering, mediumAnisotropy, 0.0f);
+        p.rayOrigin[slot] = make_float4(rayOrigin.x, rayOrigin.y, rayOrigin.z, 0.0f);
+        p.rayDirection[slot] = make_float4(rayDirection.x, rayDirection.y, rayDirection.z, 0.0f);
+        nextQueue[appendIndex(nextCount)] = slot;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// shadow: visibility of light samples (vulkan_path_tracer.cpp:855-912)
+// ---------------------------------------------------------------------------
+template <bool kOpaque, bool kCount>
+__global__ void __launch_bounds__(128) shadowKernel(DeviceScene s, PathBuffers p)
+{
+    const uint32_t n = p.counters[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(p.stats + 1, static_cast<unsigned long long>(n));
+    constexpr Accept kMode = kOpaque ? Accept::Opaque : Accept::Threshold;
+    uint2 work = make_uint2(0u, 0u);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const float4 o = p.shadowOrigin[j];
+        const float4 d = p.shadowDirection[j];
+        const float4 fct = p.shadowFactors[j];
+        const uint32_t slotK = p.shadowSlot[j];
+        const uint32_t info = p.shadowInfo[j];
+        const uint32_t slot = slotK >> 2, k = slotK & 3u;
+        const uint32_t kind = info & 0xffu, lightIndex = info >> 8;
+        const float3 origin = xyz(o), direction = xyz(d);
+        const float tmax = o.w;
+        HitRecord h;
+        if (kind == kShadowMesh) {
+            const bool occluded = traceRay<kMode, true, kCount>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+            if (occluded) p.contributionValid[k * p.capacity + slot] = 0;
+            else p.contribution[k * p.capacity + slot] = d.w * fct.x;
+            continue;
+        }
+        const GpuLight& light = s.lights[lightIndex];
+        const bool falloff = light.shadow.y >= 0.0f && light.shadow.z > 0.0f;
+        float3 visibility = f3(1.0f);
+        bool hitSomething;
+        float hitDistance = 0.0f;
+        if (falloff) {
+            hitSomething = traceRay<kMode, false, kCount>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+            hitDistance = h.t;
+        } else {
+            hitSomething = traceRay<kMode, true, kCount>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+        }
+        if (hitSomething) {
+            float strength = 1.0f;
+            if (falloff) {
+                const float falloffDistance = gmin(light.shadow.z, gmax(light.shadow.y, 0.0f));
+                strength = clampf((light.shadow.y - hitDistance) / gmax(falloffDistance, 1e-6f), 0.0f, 1.0f);
+                strength = gpow(strength, gmax(light.shadow.w, 0.0f));
+            }
+            visibility = mix(f3(1.0f), xyz(light.shadowColor), strength);
+        }
+        const Spectrum spec = spectrumFromBasis(p.wavelength[slot], p.spectrum[slot]);
+        const float sv = reflectanceSpectrum(visibility, spec);
+        p.contribution[k * p.capacity + slot] = combineShadow(kind, d.w, sv, fct.x, fct.y, fct.z);
+    }
+    if (kCount) {
+        atomicAdd(p.stats + 5, static_cast<unsigned long long>(work.x));
+        atomicAdd(p.stats + 6, static_cast<unsigned long long>(work.y));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// accumulate: sensor and per-pixel batch sums (vulkan_path_tracer.cpp:1882-1884)
+// ---------------------------------------------------------------------------
+__global__ void accumulateKernel(FrameConst f, WaveDesc w, PathBuffers p, float4* batch, double* batchXyz)
+{
+    const uint32_t local = blockIdx.x * blockDim.x + threadIdx.x;
+    if (local >= w.pixels) return;
+    const uint32_t pixel = w.pixelBase + local;
+    float4 b = batch[pixel];
+    double bx = batchXyz[3 * pixel + 0], by = batchXyz[3 * pixel + 1], bz = batchXyz[3 * pixel + 2];
+    for (uint32_t sOff = 0; sOff < w.samples; ++sOff) {
+        float3 spectral = f3(0.0f);
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (uint32_t lane = 0; lane < 3u; ++lane) {
+            const uint32_t slot = (sOff * w.pixels + local) * 3u + lane;
+            float radiance = p.radiance[slot];
+            for (uint32_t k = 0; k < 3u; ++k) {
+                if (p.contributionValid[k * p.capacity + slot]) radiance += p.contribution[k * p.capacity + slot];
+            }
+            const float wavelength = p.wavelength[slot];
+            spectral = spectral + spectralSensor(wavelength) * radiance;
+            const float3 x = sensorXyz(wavelength);
+            sx = __dadd_rn(sx, __dmul_rn(static_cast<double>(x.x), static_cast<double>(radiance)));
+            sy = __dadd_rn(sy, __dmul_rn(static_cast<double>(x.y), static_cast<double>(radiance)));
+            sz = __dadd_rn(sz, __dmul_rn(static_cast<double>(x.z), static_cast<double>(radiance)));
+        }
+        b = make_float4(b.x + spectral.x / 3.0f, b.y + spectral.y / 3.0f, b.z + spectral.z / 3.0f, 0.0f);
+        bx = __dadd_rn(bx, __ddiv_rn(sx, 3.0));
+        by = __dadd_rn(by, __ddiv_rn(sy, 3.0));
+        bz = __dadd_rn(bz, __ddiv_rn(sz, 3.0));
+    }
+    batch[pixel] = b;
+    batchXyz[3 * pixel + 0] = bx;
+    batchXyz[3 * pixel + 1] = by;
+    batchXyz[3 * pixel + 2] = bz;
+}
+
+// pixels[index] = vec4((previous * previousWeight + batchRadiance) / totalWeight, 1.0)
+// (vulkan_path_tracer.cpp:1886-1890); the FP64 XYZ sums add the batch.
+__global__ void finalizeKernel(FrameConst f, FrameBuffers fb)
+{
+    const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pixel >= f.width * f.height) return;
+    const float4 prev = fb.rgba[pixel];
+    const float4 b = fb.batch[pixel];
+    const float previousWeight = u2f(f.sampleIndex);
+    const float totalWeight = previousWeight + u2f(f.sampleCount);
+    fb.rgba[pixel] = make_float4((prev.x * previousWeight + b.x) / totalWeight, (prev.y * previousWeight + b.y) / totalWeight,
+                                 (prev.z * previousWeight + b.z) / totalWeight, 1.0f);
+    for (int k = 0; k < 3; ++k) {
+        const double base = f.sampleIndex == 0 ? 0.0 : fb.xyz[3 * pixel + k];
+        fb.xyz[3 * pixel + k] = __dadd_rn(base, fb.batchXyz[3 * pixel + k]);
+    }
+}
+
+__global__ void primaryKernel(DeviceScene s, FrameConst f, uint32_t sampleNumber, uint32_t* primitives, float* distances)
+{
+    const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pixel >= f.width * f.height) return;
+    const uint32_t px = pixel % f.width, py = pixel / f.width;
+    uint32_t rng = hashState(pixel ^ (sampleNumber * 0x9e3779b9u) ^ 0xa511e9b3u);
+    const float jx = randomFloat(rng);
+    const float jy = randomFloat(rng);
+    const float u = (u2f(px) + jx) / u2f(f.width);
+    const float v = (u2f(py) + jy) / u2f(f.height);
+    const float3 direction = normalize(f.lowerLeft + u * f.horizontal + v * f.vertical - f.origin);
+    HitRecord h;
+    const bool found = s.opaque ? traceRay<Accept::Opaque, false>(s, f.origin, direction, 0.001f, 10000.0f, rng, h)
+                                : traceRay<Accept::Stochastic, false>(s, f.origin, direction, 0.001f, 10000.0f, rng, h);
+    primitives[pixel] = found ? h.primitive : kInvalidPrimitive;
+    distances[pixel] = found ? h.t : 0.0f;
+}
+
+int gridFor(uint32_t maxItems, int perSm)
+{
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int blocks = static_cast<int>((static_cast<uint64_t>(maxItems) + 127u) / 128u);
+    return std::max(1, std::min(blocks, sms * perSm));
+}
+
+std::vector<WaveDesc> planWaves(uint32_t pixels, uint32_t samples, uint64_t capacity)
+{
+    std::vector<WaveDesc> waves;
+    const uint64_t perSample = static_cast<uint64_t>(pixels) * 3u;
+    if (perSample <= capacity) {
+        const uint32_t k = static_cast<uint32_t>(std::max<uint64_t>(1u, std::min<uint64_t>(samples, capacity / perSample)));
+        for (uint32_t s0 = 0; s0 < samples; s0 += k) {
+            const uint32_t ks = std::min(k, samples - s0);
+            waves.push_back({s0, ks, 0u, pixels, static_cast<uint32_t>(ks * perSample)});
+        }
+    } else {
+        const uint32_t chunk = static_cast<uint32_t>(capacity / 3u);
+        for (uint32_t s0 = 0; s0 < samples; ++s0) {
+            for (uint32_t p0 = 0; p0 < pixels; p0 += chunk) {
+                const uint32_t np = std::min(chunk, pixels - p0);
+                waves.push_back({s0, 1u, p0, np, np * 3u});
+            }
+        }
+    }
+    return waves;
+}
+
+struct EventPair {
+    cudaEvent_t start, stop;
+    int stage;
+};
+
+}  // namespace
+
+void uploadSrgbTable(const float* table256, cudaStream_t stream)
+{
+    CUDA_OK(cudaMemcpyToSymbolAsync(cSrgbToLinear, table256, 256 * sizeof(float), 0, cudaMemcpyHostToDevice, stream));
+}
+
+void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, FrameBuffers& fb,
+                 cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches)
+{
+    uint64_t launched = 0;
+    const uint32_t pixels = frame.width * frame.height;
+    CUDA_OK(cudaMemsetAsync(fb.batch, 0, sizeof(float4) * pixels, stream));
+    CUDA_OK(cudaMemsetAsync(fb.batchXyz, 0, sizeof(double) * 3u * pixels, stream));
+    const std::vector<WaveDesc> waves = planWaves(pixels, std::max(frame.sampleCount, 1u), paths.capacity);
+    const int traceGrid = gridFor(static_cast<uint32_t>(paths.capacity), 16);
+    const int shadeGrid = gridFor(static_cast<uint32_t>(paths.capacity), 8);
+    std::vector<EventPair> events;
+    auto timed = [&](int stage, auto&& launch) {
+        if (!timing) {
+            launch();
+            return;
+        }
+        EventPair e{};
+        e.stage = stage;
+        CUDA_OK(cudaEventCreate(&e.start));
+        CUDA_OK(cudaEventCreate(&e.stop));
+        CUDA_OK(cudaEventRecord(e.start, stream));
+        launch();
+        CUDA_OK(cudaEventRecord(e.stop, stream));
+        events.push_back(e);
+    };
+    for (const WaveDesc& w : waves) {
+        generateKernel<<<(w.count + 255u) / 256u, 256, 0, stream>>>(frame, w, paths);
+        CUDA_OK(cudaGetLastError());
+        for (uint32_t bounce = 0; bounce < frame.maxBounces; ++bounce) {
+            uint32_t* inQueue = paths.queue[bounce & 1u];
+            uint32_t* outQueue = paths.queue[(bounce + 1u) & 1u];
+            uint32_t* inCount = paths.counters + (bounce & 1u);
+            uint32_t* outCount = paths.counters + ((bounce + 1u) & 1u);
+            timed(0, [&] {
+                if (countTraversal) {
+                    if (scene.opaque) extendKernel<Accept::Opaque, true><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
+                    else extendKernel<Accept::Stochastic, true><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
+                } else {
+                    if (scene.opaque) extendKernel<Accept::Opaque, false><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
+                    else extendKernel<Accept::Stochastic, false><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
+                }
+            });
+            CUDA_OK(cudaGetLastError());
+            CUDA_OK(cudaMemsetAsync(outCount, 0, sizeof(uint32_t), stream));
+            CUDA_OK(cudaMemsetAsync(paths.counters + 2, 0, sizeof(uint32_t), stream));
+            timed(1, [&] {
+                shadeKernel<<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+            });
+            CUDA_OK(cudaGetLastError());
+            timed(2, [&] {
+                if (countTraversal) {
+                    if (scene.opaque) shadowKernel<true, true><<<traceGrid, 128, 0, stream>>>(scene, paths);
+                    else shadowKernel<false, true><<<traceGrid, 128, 0, stream>>>(scene, paths);
+                } else {
+                    if (scene.opaque) shadowKernel<true, false><<<traceGrid, 128, 0, stream>>>(scene, paths);
+                    else shadowKernel<false, false><<<traceGrid, 128, 0, stream>>>(scene, paths);
+                }
+            });
+            CUDA_OK(cudaGetLastError());
+            launched += 3;
+        }
+        launched += 2;
+        accumulateKernel<<<(w.pixels + 255u) / 256u, 256, 0, stream>>>(frame, w, paths, fb.batch, fb.batchXyz);
+        CUDA_OK(cudaGetLastError());
+    }
+    finalizeKernel<<<(pixels + 255u) / 256u, 256, 0, stream>>>(frame, fb);
+    CUDA_OK(cudaGetLastError());
+    launched += 1;
+    if (launches) *launches = launched;
+    if (timing) {
+        CUDA_OK(cudaStreamSynchronize(stream));
+        timing->waves = static_cast<uint32_t>(waves.size());
+        for (EventPair& e : events) {
+            float ms = 0.0f;
+            CUDA_OK(cudaEventElapsedTime(&ms, e.start, e.stop));
+            if (e.stage == 0) {
+                timing->extendMs += ms;
+                timing->extendLaunches++;
+            } else if (e.stage == 1) {
+                timing->shadeMs += ms;
+            } else {
+                timing->shadowMs += ms;
+            }
+            cudaEventDestroy(e.start);
+            cudaEventDestroy(e.stop);
+        }
+    }
+}
+
+void tracePrimary(const DeviceScene& scene, const FrameConst& frame, uint32_t sampleNumber, uint32_t* primitives,
+                  float* distances, cudaStream_t stream)
+{
+    const uint32_t pixels = frame.width * frame.height;
+    primaryKernel<<<(pixels + 127u) / 128u, 128, 0, stream>>>(scene, frame, sampleNumber, primitives, distances);
+    CUDA_OK(cudaGetLastError());
+}
+
+}  // namespace hdcx

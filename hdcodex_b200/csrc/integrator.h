@@ -1,0 +1,68 @@
+// integrator.h - host interface of the wavefront integrator.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device/common.cuh"
+
+namespace hdcx {
+
+// Device buffers of one wave of paths (structure of arrays, 16-byte records).
+struct PathBuffers {
+    uint64_t capacity = 0;          // paths per wave
+    uint32_t shadowPerPath = 0;     // shadow-ray slots per path per bounce
+    uint32_t* rng = nullptr;
+    float* wavelength = nullptr;
+    float4* spectrum = nullptr;     // basis r, g, b and Planck factor of the lane
+    float* throughput = nullptr;
+    float* radiance = nullptr;
+    float4* rayOrigin = nullptr;
+    float4* rayDirection = nullptr;
+    uint32_t* flags = nullptr;
+    float2* previousPdf = nullptr;  // previousBsdfPdf, previousEnvironmentLightPdf
+    float4* medium = nullptr;       // absorption, scattering, anisotropy
+    float4* hit = nullptr;          // t, primitive (bits), b1, b2
+    float* contribution = nullptr;  // 3 * capacity, slot-major per shadow slot k
+    uint8_t* contributionValid = nullptr;
+    uint32_t* queue[2] = {nullptr, nullptr};
+    float4* shadowOrigin = nullptr;     // xyz, tmax
+    float4* shadowDirection = nullptr;  // xyz, partial product
+    float4* shadowFactors = nullptr;    // f1, f2, f3
+    uint32_t* shadowSlot = nullptr;     // path slot * 4 + k
+    uint32_t* shadowInfo = nullptr;     // kind | light << 8
+    uint32_t* counters = nullptr;       // [0], [1] extension queues, [2] shadow queue
+    // extension, shadow, subsurface rays; extension node visits and triangle
+    // tests; shadow node visits and triangle tests (counting mode)
+    unsigned long long* stats = nullptr;
+};
+
+// Per-pixel accumulation buffers of the current output size.
+struct FrameBuffers {
+    uint32_t width = 0, height = 0;
+    float4* rgba = nullptr;        // running mean (the reference's output buffer)
+    double* xyz = nullptr;         // FP64 XYZ sums, 3 per pixel
+    float4* batch = nullptr;       // batchRadiance of the current render
+    double* batchXyz = nullptr;    // FP64 XYZ of the current render, 3 per pixel
+};
+
+struct StageTimes {
+    double extendMs = 0, shadeMs = 0, shadowMs = 0;
+    uint32_t waves = 0;
+    uint32_t extendLaunches = 0;
+};
+
+void uploadSrgbTable(const float* table256, cudaStream_t stream);
+
+// Renders sampleCount samples per pixel into fb (running mean update).
+// `timing` non-null records per-stage device times with CUDA events.
+// countTraversal selects the traversal kernels that count node visits and
+// triangle tests (into paths.stats[3..6]); *launches gets the kernel count.
+void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, FrameBuffers& fb,
+                 cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches);
+
+// Primary-hit ids and distances of sample `sampleNumber` (device outputs).
+void tracePrimary(const DeviceScene& scene, const FrameConst& frame, uint32_t sampleNumber, uint32_t* primitives,
+                  float* distances, cudaStream_t stream);
+
+}  // namespace hdcx

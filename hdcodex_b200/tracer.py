@@ -1,0 +1,243 @@
+"""Python binding of the hdcx C ABI (include/hdcx.h) over libhdcx.so.
+
+``PathTracer`` mirrors the reference's VulkanPathTracer
+(include/hdcodex/gpu/vulkan_path_tracer.h:26-52): ``set_scene``,
+``set_shading_mode`` / ``get_shading_mode``, ``render`` and ``has_geometry``,
+with the same argument meaning. ``render`` returns the cumulative running mean
+as a (height, width, 4) float32 array, or None where the reference returns an
+empty vector (no geometry or a zero size). A failed call raises
+``RuntimeError`` (``ValueError`` for the raster-preview mode), as the
+reference throws std::runtime_error / std::invalid_argument.
+
+There is no CPU path: without libhdcx.so or without an sm_100 GPU the
+constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from .scene import Scene
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhdcx.so")
+
+STATUS = {
+    0: "HDCX_OK", 1: "HDCX_ERROR_INVALID_ARGUMENT", 2: "HDCX_ERROR_CUDA", 3: "HDCX_ERROR_OUT_OF_MEMORY",
+    4: "HDCX_ERROR_NO_DEVICE", 5: "HDCX_ERROR_UNSUPPORTED", 6: "HDCX_ERROR_TIMEOUT", 7: "HDCX_ERROR_INTERNAL",
+}
+
+FUSED, MODULAR, RASTER_PREVIEW = 0, 1, 2
+
+# Every exported entry point of include/hdcx.h: name -> (restype, argtypes).
+_P = C.c_void_p
+SIGNATURES = {
+    "hdcx_abi_version": (C.c_uint32, []),
+    "hdcx_abi_struct_sizes": (C.c_uint32, [C.POINTER(C.c_uint64), C.c_uint32]),
+    "hdcx_material_defaults": (None, [C.POINTER(_abi.MaterialDesc)]),
+    "hdcx_light_defaults": (None, [C.POINTER(_abi.LightDesc)]),
+    "hdcx_mesh_defaults": (None, [C.POINTER(_abi.MeshDesc)]),
+    "hdcx_probe_devices": (C.c_int, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "hdcx_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "hdcx_destroy": (None, [_P]),
+    "hdcx_last_error": (C.c_char_p, [_P]),
+    "hdcx_set_scene": (C.c_int, [_P, _P]),
+    "hdcx_set_scene_packed": (C.c_int, [_P, C.POINTER(_abi.PackedScene)]),
+    "hdcx_pack_scene": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
+    "hdcx_packing_view": (C.POINTER(_abi.PackedScene), [_P]),
+    "hdcx_packing_destroy": (None, [_P]),
+    "hdcx_has_geometry": (C.c_int32, [_P]),
+    "hdcx_set_shading_mode": (C.c_int, [_P, C.c_int32]),
+    "hdcx_get_shading_mode": (C.c_int32, [_P]),
+    "hdcx_render": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                              C.c_uint32, _P, C.POINTER(C.c_int32)]),
+    "hdcx_read_rgba": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint64]),
+    "hdcx_read_xyz": (C.c_int, [_P, C.POINTER(C.c_double), C.c_uint64, C.POINTER(C.c_uint64)]),
+    "hdcx_device_rgba": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
+    "hdcx_trace_primary": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32,
+                                     C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
+    "hdcx_get_stats": (C.c_int, [_P, C.POINTER(_abi.RenderStats)]),
+    "hdcx_set_wave_size": (C.c_int, [_P, C.c_uint64]),
+    "hdcx_set_profiling": (C.c_int, [_P, C.c_uint32]),
+}
+
+PROFILE_STAGE_TIMES = 1
+PROFILE_COUNT_TRAVERSAL = 2
+
+_lib = None
+
+
+def lib():
+    """Loads libhdcx.so (building it first if it is missing and nvcc exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from .build import build
+            build()
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def probe_devices():
+    """(supported, device_count): HdCodexRendererPlugin::IsSupported's question."""
+    sup, cnt = C.c_int32(0), C.c_int32(0)
+    lib().hdcx_probe_devices(C.byref(sup), C.byref(cnt))
+    return bool(sup.value), int(cnt.value)
+
+
+class PathTracer:
+    """The CUDA path tracer behind the C ABI (see module docstring)."""
+
+    def __init__(self, device: int = 0):
+        handle = C.c_void_p()
+        status = lib().hdcx_create(device, C.byref(handle))
+        if status != 0:
+            raise RuntimeError(f"hdcx_create failed: {STATUS.get(status, status)} "
+                               "(the hdcx tracer needs an sm_100 GPU; it has no CPU path)")
+        self._h = handle
+        self.width = 0
+        self.height = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hdcx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, status: int, what: str):
+        if status != 0:
+            msg = lib().hdcx_last_error(self._h) or b""
+            raise RuntimeError(f"{what} failed: {STATUS.get(status, status)}: {msg.decode()}")
+
+    def set_scene(self, scene: Optional[Scene]):
+        if scene is None:
+            self._check(lib().hdcx_set_scene(self._h, None), "set_scene")
+            return
+        holder = scene.to_desc()
+        self._check(lib().hdcx_set_scene(self._h, C.cast(holder.pointer(), C.c_void_p)), "set_scene")
+
+    def set_shading_mode(self, mode: int):
+        if mode == RASTER_PREVIEW:
+            raise ValueError("raster preview requires the MaterialX graphics backend")
+        self._check(lib().hdcx_set_shading_mode(self._h, mode), "set_shading_mode")
+
+    def get_shading_mode(self) -> int:
+        return int(lib().hdcx_get_shading_mode(self._h))
+
+    def has_geometry(self) -> bool:
+        return bool(lib().hdcx_has_geometry(self._h))
+
+    def set_profiling(self, flags: int):
+        self._check(lib().hdcx_set_profiling(self._h, flags), "set_profiling")
+
+    def set_wave_size(self, paths: int):
+        self._check(lib().hdcx_set_wave_size(self._h, paths), "set_wave_size")
+
+    def render(self, camera, width, height, sample_index, max_bounces=8, sample_count=1, out=None):
+        """Render(camera, w, h, sampleIndex, maxBounces=8, sampleCount=1)."""
+        if out is None:
+            out = np.empty((height, width, 4), dtype=np.float32)
+        written = C.c_int32(0)
+        ptr = out.ctypes.data_as(C.c_void_p) if isinstance(out, np.ndarray) else C.c_void_p(out)
+        self._check(lib().hdcx_render(self._h, C.byref(camera), width, height, sample_index, max_bounces,
+                                      sample_count, ptr, C.byref(written)), "render")
+        if not written.value:
+            return None
+        self.width, self.height = width, height
+        return out
+
+    def render_device(self, camera, width, height, sample_index, max_bounces=8, sample_count=1) -> bool:
+        """Renders without a host copy; the image stays in device memory."""
+        written = C.c_int32(0)
+        self._check(lib().hdcx_render(self._h, C.byref(camera), width, height, sample_index, max_bounces,
+                                      sample_count, None, C.byref(written)), "render")
+        if written.value:
+            self.width, self.height = width, height
+        return bool(written.value)
+
+    def read_xyz(self):
+        """(xyz_sum (h, w, 3) float64, samples): FP64 CIE XYZ sums of the accumulation."""
+        xyz = np.zeros((self.height, self.width, 3), dtype=np.float64)
+        samples = C.c_uint64(0)
+        self._check(lib().hdcx_read_xyz(self._h, xyz.ctypes.data_as(C.POINTER(C.c_double)), xyz.size,
+                                        C.byref(samples)), "read_xyz")
+        return xyz, int(samples.value)
+
+    def trace_primary(self, camera, width, height, sample_number):
+        prims = np.zeros((height, width), dtype=np.uint32)
+        dist = np.zeros((height, width), dtype=np.float32)
+        self._check(lib().hdcx_trace_primary(self._h, C.byref(camera), width, height, sample_number,
+                                             prims.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                             dist.ctypes.data_as(C.POINTER(C.c_float))), "trace_primary")
+        return prims, dist
+
+    def stats(self) -> dict:
+        st = _abi.RenderStats()
+        self._check(lib().hdcx_get_stats(self._h, C.byref(st)), "get_stats")
+        return {name: getattr(st, name) for name, _ in _abi.RenderStats._fields_}
+
+
+def pack_scene(scene: Scene) -> dict:
+    """Host packing of a snapshot (no device needed), as numpy arrays."""
+    holder = scene.to_desc()
+    handle = C.c_void_p()
+    status = lib().hdcx_pack_scene(C.cast(holder.pointer(), C.c_void_p), C.byref(handle))
+    if status != 0:
+        raise RuntimeError(f"hdcx_pack_scene failed: {STATUS.get(status, status)}")
+    try:
+        view = lib().hdcx_packing_view(handle).contents
+        return _packed_to_dict(view)
+    finally:
+        lib().hdcx_packing_destroy(handle)
+
+
+def _packed_to_dict(view: _abi.PackedScene) -> dict:
+    def arr(ptr, count, dtype):
+        if count == 0 or not ptr:
+            return np.zeros(0, dtype=dtype)
+        addr = C.cast(ptr, C.c_void_p).value
+        raw = (C.c_uint8 * (count * np.dtype(dtype).itemsize)).from_address(addr)
+        return np.frombuffer(bytes(raw), dtype=dtype).copy()
+
+    n_lights = max(1, view.light_count)
+    out = {
+        "vertex_count": view.vertex_count, "triangle_count": view.triangle_count,
+        "material_count": view.material_count, "light_count": view.light_count,
+        "texture_count": view.texture_count, "opaque": view.opaque,
+        "vertices": arr(view.vertices, view.vertex_count * 4, np.float32),
+        "indices": arr(view.indices, view.triangle_count * 3, np.uint32),
+        "triangle_materials": arr(view.triangle_materials, view.triangle_count, np.uint32),
+        "texcoords": arr(view.texcoords, view.triangle_count * 6, np.float32),
+        "normals": arr(view.normals, view.triangle_count * 12, np.float32),
+        "materials": arr(view.materials, view.material_count * _abi.GPU_MATERIAL_BYTES, np.uint8),
+        "lights": arr(view.lights, n_lights * _abi.GPU_LIGHT_BYTES, np.uint8),
+        "emissive": arr(view.emissive, view.triangle_count * 4, np.float32),
+        "textures": [],
+    }
+    for i in range(view.texture_count):
+        t = view.textures[i]
+        n = t.width * t.height * 4
+        dtype = np.float32 if t.format == 2 else np.uint8
+        out["textures"].append((t.width, t.height, t.format, arr(t.texels, n, dtype)))
+    return out

@@ -1,0 +1,429 @@
+/*
+ * hdcx.h - C ABI of the B200 (sm_100a) spectral path-tracing backend for hdCodex.
+ *
+ * This is the drop-in boundary. Every entry point takes plain pointers, sizes and
+ * POD structs; no C++ or torch types cross it. The C++ class
+ * hdcodex::CudaPathTracer (include/hdcx/cuda_path_tracer.h) is a thin shim over
+ * these calls with the same methods as the reference's hdcodex::VulkanPathTracer
+ * (include/hdcodex/gpu/vulkan_path_tracer.h:26-52).
+ *
+ * Scene input mirrors the reference's scene ABI (include/hdcodex/core/
+ * versioned_scene.h:17-274): meshes with face-corner UVs/normals and per-triangle
+ * material ids, the compiled MaterialX closure fields of SceneMaterial, RGBA8 or
+ * RGBA32F textures with UDIM tiles, and UsdLux-derived lights. Field names follow
+ * the reference, in snake_case; defaults are given by hdcx_material_defaults() etc.
+ *
+ * Every function returns an hdcx_status. On a nonzero status the tracer's
+ * hdcx_last_error() holds a one-line message (the reference throws
+ * std::runtime_error on any Vulkan failure, vulkan_path_tracer.cpp:1894-1903).
+ */
+#ifndef HDCX_H
+#define HDCX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define HDCX_API __declspec(dllexport)
+#else
+#define HDCX_API __attribute__((visibility("default")))
+#endif
+
+#define HDCX_ABI_VERSION 1u
+
+/* Hard limits of the reference integrator (vulkan_path_tracer.cpp:22-29). */
+#define HDCX_MAX_TEXTURES 256u
+#define HDCX_MISSING_TEXTURE 0xffffffffu
+#define HDCX_UDIM_TEXTURE_FLAG 0x80000000u
+#define HDCX_UDIM_TILE_MASK 0x7fffffu
+#define HDCX_MAX_PATH_BOUNCES 12u
+#define HDCX_MAX_LIGHTS 64u
+
+typedef enum hdcx_status {
+    HDCX_OK = 0,
+    HDCX_ERROR_INVALID_ARGUMENT = 1,
+    HDCX_ERROR_CUDA = 2,
+    HDCX_ERROR_OUT_OF_MEMORY = 3,
+    HDCX_ERROR_NO_DEVICE = 4,
+    HDCX_ERROR_UNSUPPORTED = 5,
+    HDCX_ERROR_TIMEOUT = 6,
+    HDCX_ERROR_INTERNAL = 7
+} hdcx_status;
+
+/* ShadingMode (include/hdcodex/core/shading_mode.h:9-13). Fused and Modular
+ * select the same CUDA kernels; RasterPreview is rejected as the reference's
+ * CreatePipeline rejects it (vulkan_path_tracer.cpp:2495-2498). */
+typedef enum hdcx_shading_mode {
+    HDCX_SHADING_FUSED = 0,
+    HDCX_SHADING_MODULAR = 1,
+    HDCX_SHADING_RASTER_PREVIEW = 2
+} hdcx_shading_mode;
+
+/* PathTracerCamera (vulkan_path_tracer.h:16-23). Row 0 of the image is the
+ * lowerLeft edge; a pixel (x, y) looks along
+ * lowerLeft + u*horizontal + v*vertical - origin. */
+typedef struct hdcx_camera {
+    float origin[3];
+    float lower_left[3];
+    float horizontal[3];
+    float vertical[3];
+} hdcx_camera;
+
+/* SceneMesh (versioned_scene.h:17-34). Counts are element counts of the arrays. */
+typedef struct hdcx_mesh_desc {
+    const char* id;
+    const float* positions;          /* 3 floats per vertex */
+    uint64_t position_count;
+    const uint32_t* indices;         /* 3 per triangle */
+    uint64_t index_count;
+    const float* texcoords;          /* 2 floats per triangulated face corner */
+    uint64_t texcoord_count;
+    const float* normals;            /* 3 floats per face corner; zero = geometric */
+    uint64_t normal_count;
+    const char* material_id;         /* NULL or "" = display-color fallback */
+    const char* const* triangle_material_ids; /* optional, one per triangle */
+    uint64_t triangle_material_id_count;
+    float display_color[3];
+} hdcx_mesh_desc;
+
+/* Diffuse models of SceneMaterial::DiffuseModel (versioned_scene.h:37-42). */
+#define HDCX_DIFFUSE_LAMBERT 0u
+#define HDCX_DIFFUSE_OREN_NAYAR 1u
+#define HDCX_DIFFUSE_BURLEY 2u
+#define HDCX_DIFFUSE_OREN_NAYAR_ENERGY_COMPENSATED 3u
+
+/* The compact path-closure fields of SceneMaterial (versioned_scene.h:117-188),
+ * in the reference's declaration order. The MaterialX raster/SPIR-V members of
+ * SceneMaterial are never read by the integrator and are not part of this ABI. */
+typedef struct hdcx_material_desc {
+    const char* id;
+    float base_color[3];
+    float base_color_texture_scale[3];
+    float base_color_texture_bias[3];
+    int32_t base_color_texture_channel;
+    float emission[3];
+    float transmission_color[3];
+    float transmission_scatter[3];
+    float specular_color[3];
+    float coat_color[3];
+    float sheen_color[3];
+    float translucent_color[3];
+    float subsurface_color[3];
+    float subsurface_radius[3];
+    uint32_t diffuse_model;
+    float diffuse_weight;
+    float diffuse_roughness;
+    float metalness;
+    float roughness;
+    float roughness_v;
+    float opacity;
+    float emission_weight;
+    float transmission;
+    float transmission_depth;
+    float transmission_scatter_anisotropy;
+    float transmission_dispersion_scale;
+    float transmission_dispersion_abbe_number;
+    float index_of_refraction;
+    float specular_weight;
+    float coat;
+    float coat_roughness;
+    float coat_roughness_v;
+    float coat_index_of_refraction;
+    float sheen;
+    float sheen_roughness;
+    uint32_t sheen_mode;             /* 0 Conty-Kulla, 1 Zeltner */
+    float translucent_weight;
+    float subsurface;
+    float subsurface_scale;
+    float subsurface_scatter_anisotropy;
+    int32_t thin_walled;
+    int32_t normal_texture_flip_y;
+    float normal_texture_scale;
+    const char* base_color_texture;
+    const char* metalness_texture;
+    const char* roughness_texture;
+    const char* diffuse_weight_texture;
+    const char* diffuse_roughness_texture;
+    const char* emission_texture;
+    const char* opacity_texture;
+    const char* normal_texture;
+    const char* transmission_texture;
+    const char* specular_texture;
+    const char* specular_color_texture;
+    const char* coat_texture;
+    const char* coat_color_texture;
+    const char* coat_roughness_texture;
+    const char* sheen_texture;
+    const char* sheen_color_texture;
+    const char* sheen_roughness_texture;
+    const char* translucent_weight_texture;
+    const char* translucent_color_texture;
+    const char* subsurface_texture;
+    const char* subsurface_color_texture;
+    const char* subsurface_radius_texture;
+} hdcx_material_desc;
+
+/* SceneTexture (versioned_scene.h:191-206): RGBA8 (optionally sRGB) or RGBA32F. */
+typedef struct hdcx_texture_desc {
+    const char* id;
+    const char* udim_set_id;         /* non-empty for a UDIM tile */
+    uint32_t udim_tile;
+    uint32_t width;
+    uint32_t height;
+    int32_t srgb;
+    const uint8_t* rgba;             /* width*height*4 bytes, or NULL */
+    uint64_t rgba_count;
+    const float* rgba_float;         /* width*height*4 floats, or NULL */
+    uint64_t rgba_float_count;
+} hdcx_texture_desc;
+
+/* SceneLightType / DomeTextureFormat (versioned_scene.h:208-223). */
+#define HDCX_LIGHT_DOME 0u
+#define HDCX_LIGHT_RECT 1u
+#define HDCX_LIGHT_DISK 2u
+#define HDCX_LIGHT_SPHERE 3u
+#define HDCX_LIGHT_CYLINDER 4u
+#define HDCX_LIGHT_DISTANT 5u
+#define HDCX_DOME_AUTOMATIC 0u
+#define HDCX_DOME_LATLONG 1u
+#define HDCX_DOME_MIRRORED_BALL 2u
+#define HDCX_DOME_ANGULAR 3u
+#define HDCX_DOME_CUBEMAP_VERTICAL_CROSS 4u
+
+/* SceneLight (versioned_scene.h:225-266), in declaration order. */
+typedef struct hdcx_light_desc {
+    const char* id;
+    uint32_t type;
+    int32_t visible;
+    float color[3];
+    float temperature_color[3];
+    float intensity;
+    float exposure;
+    float diffuse;
+    float specular;
+    int32_t normalize;
+    const char* texture;
+    uint32_t texture_format;
+    float basis_x[3];
+    float basis_y[3];
+    float basis_z[3];
+    float position[3];
+    float axis_u[3];
+    float axis_v[3];
+    float width;
+    float height;
+    float radius;
+    float length;
+    float angle;
+    float area;
+    float shaping_focus;
+    float shaping_focus_tint[3];
+    float shaping_cone_angle;
+    float shaping_cone_softness;
+    int32_t shadow_enable;
+    float shadow_color[3];
+    float shadow_distance;
+    float shadow_falloff;
+    float shadow_falloff_gamma;
+} hdcx_light_desc;
+
+/* SceneSnapshot (versioned_scene.h:268-274). Arrays are taken in the given
+ * order, exactly as SetScene takes a published snapshot (whose containers the
+ * reference's VersionedScene fills in id order, versioned_scene.h:297-326). */
+typedef struct hdcx_scene_desc {
+    uint64_t revision;
+    const hdcx_mesh_desc* meshes;
+    uint64_t mesh_count;
+    const hdcx_material_desc* materials;
+    uint64_t material_count;
+    const hdcx_texture_desc* textures;
+    uint64_t texture_count;
+    const hdcx_light_desc* lights;
+    uint64_t light_count;
+} hdcx_scene_desc;
+
+/* Device records, byte-identical to the reference's GpuMaterial (23 x 16 B,
+ * vulkan_path_tracer.cpp:1907-1933) and GpuLight (14 x 16 B, :1935-1952). */
+#define HDCX_GPU_MATERIAL_BYTES 368u
+#define HDCX_GPU_LIGHT_BYTES 224u
+
+/* Texel formats of a packed texture (the reference's VkFormat choice,
+ * vulkan_path_tracer.cpp:2218-2221). */
+#define HDCX_TEXEL_RGBA8_UNORM 0u
+#define HDCX_TEXEL_RGBA8_SRGB 1u
+#define HDCX_TEXEL_RGBA32F 2u
+
+typedef struct hdcx_packed_texture {
+    uint32_t width;
+    uint32_t height;
+    uint32_t format;                 /* HDCX_TEXEL_* */
+    uint32_t reserved;
+    const void* texels;              /* width*height*4 bytes or floats */
+} hdcx_packed_texture;
+
+/* The flattened scene in the integrator's device layout (the reference's
+ * BuildScene output, vulkan_path_tracer.cpp:2604-2993). */
+typedef struct hdcx_packed_scene {
+    uint32_t vertex_count;
+    uint32_t triangle_count;
+    uint32_t material_count;
+    uint32_t light_count;            /* authored lights (<= 64); buffer holds max(1, n) */
+    uint32_t texture_count;
+    uint32_t opaque;                 /* all materials opaque (vulkan_path_tracer.cpp:2609-2612) */
+    const float* vertices;           /* 4 floats per vertex (xyz, w = 1) */
+    const uint32_t* indices;         /* 3 per triangle */
+    const uint32_t* triangle_materials;
+    const float* texcoords;          /* 6 floats per triangle (face corners) */
+    const float* normals;            /* 12 floats per triangle (corner xyz0) */
+    const void* materials;           /* material_count * 368 B */
+    const void* lights;              /* max(1, light_count) * 224 B */
+    const float* emissive;           /* 4 floats per triangle: cdf, prob/area, area, 0 */
+    const hdcx_packed_texture* textures;
+} hdcx_packed_scene;
+
+typedef struct hdcx_tracer hdcx_tracer;
+typedef struct hdcx_packing hdcx_packing;
+
+/* Per-render counters, filled by hdcx_get_stats after a render. */
+typedef struct hdcx_render_stats {
+    uint64_t spectral_paths;         /* pixels * spp * 3 */
+    uint64_t extension_rays;         /* closest-hit rays (camera + bounces) */
+    uint64_t shadow_rays;            /* any-hit visibility rays */
+    uint64_t subsurface_rays;        /* opaque boundary rays of the SSS walk */
+    double render_ms;                /* device time of the last render call */
+    double extend_ms;                /* device time in closest-hit traversal */
+    double shade_ms;                 /* device time in shading */
+    double shadow_ms;                /* device time in shadow traversal */
+    uint32_t waves;                  /* path waves the render was split into */
+    uint32_t extend_launches;        /* closest-hit traversal launches */
+    uint64_t kernel_launches;        /* kernels the render launched */
+    uint64_t extension_node_visits;  /* wide nodes loaded by closest-hit rays (counting mode) */
+    uint64_t extension_triangle_tests; /* triangle tests of closest-hit rays (counting mode) */
+    uint64_t shadow_node_visits;     /* wide nodes loaded by shadow rays (counting mode) */
+    uint64_t shadow_triangle_tests;  /* triangle tests of shadow rays (counting mode) */
+} hdcx_render_stats;
+
+/* Profiling switches for hdcx_set_profiling. */
+#define HDCX_PROFILE_STAGE_TIMES 1u      /* CUDA events around every extend/shade/shadow launch */
+#define HDCX_PROFILE_COUNT_TRAVERSAL 2u  /* traversal kernels count node visits and triangle tests */
+
+/* ---------------------------------------------------------------------------
+ * Library and device probing
+ * ------------------------------------------------------------------------- */
+
+/* Returns HDCX_ABI_VERSION. */
+HDCX_API uint32_t hdcx_abi_version(void);
+
+/* Byte size of each ABI struct, indexed 0..7: camera, mesh, material, texture,
+ * light, scene, packed_texture, packed_scene; 8: render_stats. Lets bindings
+ * check their struct mirrors. Returns the number of entries written. */
+HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity);
+
+/* Fills the reference defaults of SceneMaterial / SceneLight / SceneMesh
+ * (versioned_scene.h:121-188, :225-266, :33). String members are set to NULL. */
+HDCX_API void hdcx_material_defaults(hdcx_material_desc* material);
+HDCX_API void hdcx_light_defaults(hdcx_light_desc* light);
+HDCX_API void hdcx_mesh_defaults(hdcx_mesh_desc* mesh);
+
+/* Replaces HdCodexRendererPlugin::IsSupported / ProbeVulkanDevices
+ * (renderer_plugin.cpp:34-60, vulkan_context.h:10-60): *supported = 1 when a
+ * CUDA device of compute capability 10.x is present. */
+HDCX_API hdcx_status hdcx_probe_devices(int32_t* supported, int32_t* device_count);
+
+/* ---------------------------------------------------------------------------
+ * Tracer lifetime (VulkanPathTracer constructor/destructor,
+ * vulkan_path_tracer.cpp:3348-3350; render_delegate.cpp:113-132 constructs it)
+ * ------------------------------------------------------------------------- */
+HDCX_API hdcx_status hdcx_create(int32_t device, hdcx_tracer** tracer);
+HDCX_API void hdcx_destroy(hdcx_tracer* tracer);
+
+/* Message of the last failed call on this tracer ("" when none). */
+HDCX_API const char* hdcx_last_error(const hdcx_tracer* tracer);
+
+/* ---------------------------------------------------------------------------
+ * Scene (VulkanPathTracer::SetScene, vulkan_path_tracer.cpp:3351-3354 ->
+ * Impl::BuildScene :2604-3128)
+ * ------------------------------------------------------------------------- */
+
+/* Flattens, packs and uploads a snapshot and builds the BVH on the GPU.
+ * scene == NULL clears the scene (HasGeometry becomes false). Synchronous. */
+HDCX_API hdcx_status hdcx_set_scene(hdcx_tracer* tracer, const hdcx_scene_desc* scene);
+
+/* Uploads an already packed scene (a caller that packs on its own side). */
+HDCX_API hdcx_status hdcx_set_scene_packed(hdcx_tracer* tracer, const hdcx_packed_scene* scene);
+
+/* Packs a snapshot on the host without a device; the view stays valid until
+ * hdcx_packing_destroy. Used to check the packing against the reference rules. */
+HDCX_API hdcx_status hdcx_pack_scene(const hdcx_scene_desc* scene, hdcx_packing** packing);
+HDCX_API const hdcx_packed_scene* hdcx_packing_view(const hdcx_packing* packing);
+HDCX_API void hdcx_packing_destroy(hdcx_packing* packing);
+
+/* VulkanPathTracer::HasGeometry (vulkan_path_tracer.cpp:3371). */
+HDCX_API int32_t hdcx_has_geometry(const hdcx_tracer* tracer);
+
+/* SetShadingMode / GetShadingMode (vulkan_path_tracer.cpp:3355-3362).
+ * RasterPreview returns HDCX_ERROR_UNSUPPORTED and keeps the current mode. */
+HDCX_API hdcx_status hdcx_set_shading_mode(hdcx_tracer* tracer, int32_t mode);
+HDCX_API int32_t hdcx_get_shading_mode(const hdcx_tracer* tracer);
+
+/* ---------------------------------------------------------------------------
+ * Rendering (VulkanPathTracer::Render, vulkan_path_tracer.cpp:3363-3370 ->
+ * Impl::Trace :3230-3306)
+ * ------------------------------------------------------------------------- */
+
+/* Traces sample_count samples per pixel starting at sample_index and updates
+ * the device running mean exactly like the reference's accumulation
+ * (vulkan_path_tracer.cpp:1886-1890): pixel = (prev*sample_index + batch) /
+ * (sample_index + sample_count), alpha = 1. sample_index == 0 restarts.
+ * max_bounces is clamped to [1, 12]. When rgba_out is not NULL the whole
+ * RGBA32F image (width*height*4 floats, row 0 = bottom) is copied into it.
+ * With no geometry or a zero size nothing is traced and *written = 0
+ * (the reference returns an empty vector, :3235); otherwise *written = 1. */
+HDCX_API hdcx_status hdcx_render(hdcx_tracer* tracer, const hdcx_camera* camera,
+                                 uint32_t width, uint32_t height,
+                                 uint32_t sample_index, uint32_t max_bounces,
+                                 uint32_t sample_count, float* rgba_out,
+                                 int32_t* written);
+
+/* Copies the current device RGBA32F accumulation (width*height*4 floats). */
+HDCX_API hdcx_status hdcx_read_rgba(hdcx_tracer* tracer, float* rgba_out, uint64_t float_count);
+
+/* Copies the FP64 per-pixel CIE XYZ sums (width*height*3 doubles) and the
+ * number of samples they hold. The mean XYZ is sum / samples. For every sample
+ * the three lanes add (cie(lambda) * 400/106.856895 * radiance) / 3, the XYZ
+ * the reference's sensor (vulkan_path_tracer.cpp:172-179) feeds its sRGB matrix. */
+HDCX_API hdcx_status hdcx_read_xyz(hdcx_tracer* tracer, double* xyz_out,
+                                   uint64_t double_count, uint64_t* samples);
+
+/* Device pointer of the RGBA32F accumulation buffer (valid until the next
+ * render with another size, set_scene or destroy). */
+HDCX_API hdcx_status hdcx_device_rgba(hdcx_tracer* tracer, const float** device_rgba);
+
+/* Primary-ray hit test for sample `sample_number`: writes for every pixel the
+ * flattened primitive index of the closest accepted hit (0xffffffff = miss)
+ * and its distance. All three wavelength lanes of a sample share the camera
+ * ray (same seed and jitter, vulkan_path_tracer.cpp:1202-1213). */
+HDCX_API hdcx_status hdcx_trace_primary(hdcx_tracer* tracer, const hdcx_camera* camera,
+                                        uint32_t width, uint32_t height,
+                                        uint32_t sample_number, uint32_t* primitive_out,
+                                        float* distance_out);
+
+/* Counters of the last render. */
+HDCX_API hdcx_status hdcx_get_stats(const hdcx_tracer* tracer, hdcx_render_stats* stats);
+
+/* Turns profiling on or off (HDCX_PROFILE_* bits); results are unchanged. */
+HDCX_API hdcx_status hdcx_set_profiling(hdcx_tracer* tracer, uint32_t flags);
+
+/* Number of paths resident per wave (0 = automatic). Larger waves use more
+ * device memory for path state; results do not depend on it. */
+HDCX_API hdcx_status hdcx_set_wave_size(hdcx_tracer* tracer, uint64_t paths_per_wave);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HDCX_H */

@@ -1,0 +1,176 @@
+"""Scenes of the reference's GPU integration test, restated as Scene objects.
+
+The base scene, camera and every variant follow tests/path_tracer_tests.cpp of
+hdCodex (line numbers cited per variant): a triangle at z = -3 seen by a 64x64
+camera, a green sRGB base-color texture, a blue dome and a textured rect light.
+"""
+from __future__ import annotations
+
+from hdcodex_b200.scene import (CYLINDER, DISK, DISTANT, DOME, RECT, SPHERE, Light, Material,
+                                Mesh, Scene, Texture, camera)
+
+WIDTH = 64
+HEIGHT = 64
+CENTER = (HEIGHT // 2, WIDTH // 2)
+CORNER = (0, 0)
+
+
+def base_camera():
+    # path_tracer_tests.cpp:132-137
+    return camera((0.0, 0.0, 0.0), (-1.0, -1.0, -1.0), (2.0, 0.0, 0.0), (0.0, 2.0, 0.0))
+
+
+def z_up_camera():
+    # path_tracer_tests.cpp:478-483
+    return camera((0.0, 0.0, 0.0), (-1.0, -1.0, -1.0), (2.0, 0.0, 0.0), (0.0, 0.0, 2.0))
+
+
+def base_scene() -> Scene:
+    # path_tracer_tests.cpp:36-129
+    s = Scene(revision=1)
+    s.meshes.append(Mesh(
+        id="/triangle",
+        positions=[-1.25, -1.0, -3.0, 1.25, -1.0, -3.0, 0.0, 1.2, -3.0],
+        indices=[0, 1, 2],
+        texcoords=[0.0, 0.0, 1.0, 0.0, 0.5, 1.0],
+        material_id="/red",
+    ))
+    s.materials.append(Material(id="/red", base_color=[1.0, 1.0, 1.0], metalness=0.15,
+                                roughness=0.3, base_color_texture="green#srgb"))
+    s.textures += [
+        Texture(id="green#srgb", source_path="synthetic", width=1, height=1, srgb=True,
+                rgba=[16, 220, 32, 255]),
+        Texture(id="scatter#raw", source_path="synthetic", width=1, height=1, srgb=False,
+                rgba=[255, 255, 255, 255]),
+        Texture(id="synthetic-udim#srgb#udim=1001", source_path="synthetic.1001",
+                udim_set_id="synthetic-udim#srgb", udim_tile=1001, width=1, height=1, srgb=True,
+                rgba=[230, 16, 16, 255]),
+        Texture(id="synthetic-udim#srgb#udim=1002", source_path="synthetic.1002",
+                udim_set_id="synthetic-udim#srgb", udim_tile=1002, width=1, height=1, srgb=True,
+                rgba=[16, 24, 230, 255]),
+        Texture(id="rect#hdr", source_path="synthetic", width=1, height=1, srgb=False,
+                rgba_float=[2.0, 2.0, 2.0, 1.0]),
+        Texture(id="spectral-gradient#hdr", source_path="synthetic", width=4, height=1, srgb=False,
+                rgba_float=[3.0, 0.02, 0.02, 1.0, 0.02, 3.0, 0.02, 1.0,
+                            0.02, 0.02, 3.0, 1.0, 3.0, 3.0, 3.0, 1.0]),
+    ]
+    s.lights += [
+        Light(id="/dome", type=DOME, color=[0.08, 0.16, 0.8], intensity=0.35),
+        Light(id="/rect", type=RECT, color=[1.0, 0.92, 0.82], intensity=50.0, texture="rect#hdr",
+              basis_x=[0.817, -0.576, 0.0], basis_y=[0.184, 0.261, -0.947],
+              basis_z=[0.547, 0.775, 0.319], position=[3.282, 4.650, -1.086],
+              axis_u=[1.634, -1.152, 0.0], axis_v=[0.368, 0.522, -1.894], width=2.0, height=2.0,
+              area=4.0),
+    ]
+    return s
+
+
+def analytic_lights():
+    # path_tracer_tests.cpp:169-203
+    return [
+        Light(id="/disk", type=DISK, intensity=20.0, position=[0.0, 0.0, -1.5],
+              axis_u=[0.75, 0.0, 0.0], axis_v=[0.0, 0.75, 0.0], area=1.7671459),
+        Light(id="/sphere", type=SPHERE, intensity=20.0, position=[0.0, 0.0, -1.5], radius=0.35,
+              area=1.5393804),
+        Light(id="/cylinder", type=CYLINDER, intensity=20.0, position=[0.0, 0.0, -1.5],
+              axis_u=[1.0, 0.0, 0.0], radius=0.25, length=1.0, area=1.5707963),
+        Light(id="/distant", type=DISTANT, intensity=1.0, angle=0.53),
+    ]
+
+
+def selection_scene() -> Scene:
+    # path_tracer_tests.cpp:217-226: 63 black domes and the rect light.
+    s = base_scene()
+    rect = s.lights[1]
+    s.lights = [Light(id=f"/black{i}", type=DOME, intensity=0.0) for i in range(63)] + [rect]
+    return s
+
+
+def mesh_light_scene(emission_weight=1.0) -> Scene:
+    # path_tracer_tests.cpp:237-283
+    s = Scene(revision=2)
+    s.meshes = [
+        Mesh(id="/receiver", positions=[-1.25, -1.0, -3.0, 1.25, -1.0, -3.0, 0.0, 1.2, -3.0],
+             indices=[0, 1, 2], material_id="/receiverMaterial"),
+        Mesh(id="/emitter", positions=[0.35, 0.35, -1.8, 1.10, 0.35, -1.8, 0.70, 1.00, -1.8],
+             indices=[0, 1, 2], material_id="/emitterMaterial"),
+    ]
+    s.materials = [
+        Material(id="/receiverMaterial", base_color=[0.8, 0.8, 0.8], roughness=0.6),
+        Material(id="/emitterMaterial", base_color=[0.0, 0.0, 0.0], emission=[16.0, 12.0, 8.0],
+                 emission_weight=emission_weight),
+    ]
+    s.lights = [Light(id="/blackDome", type=DOME, intensity=0.0)]
+    return s
+
+
+def variant(name: str) -> Scene:
+    """Named variants of the base scene from path_tracer_tests.cpp."""
+    s = base_scene()
+    m = s.materials[0]
+    if name == "base":
+        pass
+    elif name == "oren_nayar":  # :294-298
+        m.diffuse_model = 1
+        m.diffuse_roughness = 0.85
+    elif name == "udim":  # :313-318
+        s.meshes[0].texcoords = [1.1, 0.1, 1.9, 0.1, 1.5, 0.9]
+        m.base_color_texture = "synthetic-udim#srgb"
+    elif name == "authored_normals":  # :334-341
+        s.meshes[0].normals = [0.6, 0.85, 0.35] * 3
+    elif name in ("glossy", "matte_black", "coated"):  # :345-371
+        s.meshes[0].normals = [0.3446, 0.4881, 0.8027] * 3
+        m.base_color = [0.0, 0.0, 0.0]
+        m.base_color_texture = ""
+        m.roughness = 0.08
+        m.specular_weight = 1.0 if name != "matte_black" else 0.0
+        if name == "coated":
+            m.specular_weight = 0.0
+            m.coat = 1.0
+            m.coat_roughness = 0.08
+    elif name == "subsurface":  # :380-384
+        m.subsurface_color = [0.02, 0.05, 1.0]
+        m.subsurface_scale = 0.0
+        m.subsurface_texture = "scatter#raw"
+    elif name == "cutout":  # :391-393
+        m.opacity = 0.0
+    elif name in ("opaque_black", "translucent"):  # :398-414
+        m.base_color = [0.0, 0.0, 0.0]
+        m.base_color_texture = ""
+        m.diffuse_weight = 0.0
+        m.specular_weight = 0.0
+        m.coat = 0.0
+        if name == "translucent":
+            m.translucent_weight = 1.0
+            m.translucent_color = [1.0, 0.02, 0.01]
+    elif name in ("thin_walled", "nondispersive", "dispersive"):  # :416-449
+        m.base_color = [0.0, 0.0, 0.0]
+        m.base_color_texture = ""
+        m.diffuse_weight = 1.0
+        m.specular_weight = 0.0
+        m.transmission = 1.0
+        m.metalness = 0.0
+        if name == "thin_walled":
+            m.transmission_color = [1.0, 0.05, 0.02]
+            m.thin_walled = True
+        else:
+            m.transmission_color = [1.0, 1.0, 1.0]
+            s.lights = s.lights[:1]
+            s.lights[0].color = [1.0, 1.0, 1.0]
+            s.lights[0].intensity = 1.0
+            s.lights[0].texture = "spectral-gradient#hdr"
+            if name == "dispersive":
+                m.transmission_dispersion_scale = 1.0
+                m.transmission_dispersion_abbe_number = 9.0
+    elif name in ("fallback", "fallback_zup"):  # :451-490
+        s.lights = []
+        s.meshes[0].material_id = ""
+        s.meshes[0].display_color = [0.05, 0.8, 0.1]
+        m.base_color = [0.8, 0.8, 0.8]
+        m.base_color_texture = ""
+        m.roughness = 1.0
+        if name == "fallback_zup":
+            s.meshes[0].positions = [-1.25, -3.0, -1.0, 0.0, -3.0, 1.2, 1.25, -3.0, -1.0]
+    else:
+        raise KeyError(name)
+    return s
