@@ -51,14 +51,26 @@ def parse():
     ap.add_argument("--workload", default="heavy", choices=["heavy", "box"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="render exactly one frame and exit (for ncu launch lists and captures)")
+    ap.add_argument("--width", type=int, default=0, help="override the workload width (profiling only)")
+    ap.add_argument("--height", type=int, default=0, help="override the workload height (profiling only)")
+    ap.add_argument("--spp", type=int, default=0, help="override the workload spp (profiling only)")
     return ap.parse_args()
 
 
-def make_workload(name):
+def make_workload(name, args=None):
     from hdcodex_b200 import workloads
-    if name == "box":
-        return workloads.closed_box()
-    return workloads.heavy_geometry()
+    wl = workloads.closed_box() if name == "box" else workloads.heavy_geometry()
+    if args is not None and (args.width or args.height or args.spp):
+        from hdcodex_b200.workloads import look_at_camera
+        w = args.width or wl.width
+        h = args.height or wl.height
+        if name != "box":
+            wl.camera = look_at_camera((0.0, 7.5, 17.0), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), 45.0, w / h)
+        wl.width, wl.height = w, h
+        wl.spp = args.spp or wl.spp
+    return wl
 
 
 def measured_peaks():
@@ -237,9 +249,15 @@ def run_hdcx(args):
     from hdcodex_b200 import PathTracer, workloads
     from hdcodex_b200.tracer import PROFILE_COUNT_TRAVERSAL, PROFILE_STAGE_TIMES
 
-    wl = make_workload(args.workload)
+    wl = make_workload(args.workload, args)
     tracer = PathTracer(local)
     tracer.set_scene(wl.scene)
+    if args.profile:
+        tracer.render_device(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp)
+        print(json.dumps({"profile_frame": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
+                          "stats": tracer.stats()}), flush=True)
+        tracer.close()
+        return
     tri_count = workloads.triangle_count(wl.scene)
     paths_per_step = wl.spectral_paths
 
@@ -260,11 +278,14 @@ def run_hdcx(args):
     sampler.start()
     wall0 = time.perf_counter()
     render_ms, extend_ms, extend_launches, ext_rays, sh_rays, ss_rays, launches = 0.0, 0.0, 0, 0, 0, 0, 0
+    shade_ms, shadow_ms = 0.0, 0.0
     for i in range(args.steps):
         tracer.render_device(wl.camera, wl.width, wl.height, sample_index(args.warmup + i), wl.max_bounces, wl.spp)
         st = tracer.stats()
         render_ms += st["render_ms"]
         extend_ms += st["extend_ms"]
+        shade_ms += st["shade_ms"]
+        shadow_ms += st["shadow_ms"]
         extend_launches += st["extend_launches"]
         ext_rays += st["extension_rays"]
         sh_rays += st["shadow_rays"]
@@ -336,6 +357,9 @@ def run_hdcx(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48,
                     "d2h_bytes_per_step": wl.width * wl.height * 16, "image_finite": finite},
             "gpu_launches": launches,
+            "stage_ms_per_step": {"extend": extend_ms / args.steps, "shade": shade_ms / args.steps,
+                                  "shadow": shadow_ms / args.steps,
+                                  "other": (render_ms - extend_ms - shade_ms - shadow_ms) / args.steps},
             "roofline": roofline,
             "cpu_baseline": baseline,
             "clocks": clocks,
