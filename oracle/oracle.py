@@ -146,3 +146,57 @@ def packed_view_to_dict(view: _abi.PackedScene) -> dict:
         dtype = np.float32 if t.format == 2 else np.uint8
         out["textures"].append((t.width, t.height, t.format, arr(t.texels, n, dtype)))
     return out
+
+
+# ---------------------------------------------------------------------------
+# The reference integrator's own GLSL, compiled as C++ by oracle/ref_build.py
+# into oracle/_ref/libhdcx_ref.so (built only where the reference checkout is
+# present; the library then travels with the repository snapshot).
+# ---------------------------------------------------------------------------
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libhdcx_ref.so")
+_ref_lib = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB_PATH)
+
+
+def ref_lib():
+    global _ref_lib
+    if _ref_lib is None:
+        L = C.CDLL(REF_LIB_PATH)
+        L.ref_create.restype = C.c_void_p
+        L.ref_destroy.argtypes = [C.c_void_p]
+        L.ref_set_scene.argtypes = [C.c_void_p, C.c_void_p]
+        L.ref_render.argtypes = [
+            C.c_void_p, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+            C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, C.POINTER(C.c_float)]
+        _ref_lib = L
+    return _ref_lib
+
+
+class ReferenceTracer:
+    """VulkanPathTracer's shader run on the CPU (same methods as OracleTracer)."""
+
+    def __init__(self):
+        self._h = ref_lib().ref_create()
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            ref_lib().ref_destroy(self._h)
+            self._h = None
+
+    def set_scene(self, scene: Scene | None):
+        if scene is None:
+            ref_lib().ref_set_scene(self._h, None)
+            return
+        holder = scene.to_desc()
+        ref_lib().ref_set_scene(self._h, C.cast(holder.pointer(), C.c_void_p))
+
+    def render(self, camera, width, height, sample_index, max_bounces=8, sample_count=1, crop=None, threads=0):
+        rgba = np.zeros((height, width, 4), dtype=np.float32)
+        x0, y0, x1, y1 = crop if crop else (0, 0, 0, 0)
+        ok = ref_lib().ref_render(self._h, C.byref(camera), width, height, sample_index, max_bounces,
+                                  sample_count, x0, y0, x1, y1, threads,
+                                  rgba.ctypes.data_as(C.POINTER(C.c_float)))
+        return rgba if ok else None

@@ -137,6 +137,10 @@ enum class AcceptMode {
 // primitive index. Returns false on a miss.
 bool TraceClosest(const PackedScene& scene, const Bvh& bvh, vec3 origin, vec3 direction,
                   float tmin, float tmax, AcceptMode mode, uint32_t rayRng, Hit* hit);
+// Every triangle the watertight test hits with t in [tmin, tmax], in no
+// particular order (the candidates a ray query reports).
+void TraceAll(const PackedScene& scene, const Bvh& bvh, vec3 origin, vec3 direction, float tmin, float tmax,
+              std::vector<Hit>* hits);
 // Any confirmed hit with t in [tmin, tmax].
 bool TraceAny(const PackedScene& scene, const Bvh& bvh, vec3 origin, vec3 direction,
               float tmin, float tmax, AcceptMode mode);

@@ -345,6 +345,41 @@ bool TraceClosest(const PackedScene& scene, const Bvh& bvh, vec3 origin, vec3 di
     return Traverse<false>(scene, bvh, origin, direction, tmin, tmax, mode, rayRng, hit);
 }
 
+void TraceAll(const PackedScene& scene, const Bvh& bvh, vec3 origin, vec3 direction, float tmin, float tmax,
+              std::vector<Hit>* hits)
+{
+    hits->clear();
+    if (bvh.nodes.empty()) return;
+    const RayPre pre = Precompute(origin, direction);
+    const double o[3] = {origin.x, origin.y, origin.z};
+    const double inv[3] = {1.0 / static_cast<double>(direction.x), 1.0 / static_cast<double>(direction.y),
+                           1.0 / static_cast<double>(direction.z)};
+    const double limit = static_cast<double>(tmax) * (1.0 + 1e-5) + 1e-6;
+    uint32_t stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const BvhNode& node = bvh.nodes[stack[--sp]];
+        double tNear;
+        if (!BoxHit(node, o, inv, static_cast<double>(tmin) * (1.0 - 1e-5) - 1e-6, limit, &tNear)) continue;
+        if (node.count == 0) {
+            if (sp + 2 > 128) continue;
+            stack[sp++] = node.right;
+            stack[sp++] = node.left;
+            continue;
+        }
+        for (uint32_t i = 0; i < node.count; ++i) {
+            const uint32_t prim = bvh.primitives[node.left + i];
+            float t;
+            vec2 bary;
+            if (IntersectTriangle(pre, Vertex(scene, prim, 0), Vertex(scene, prim, 1), Vertex(scene, prim, 2), tmin,
+                                  tmax, &t, &bary)) {
+                hits->push_back(Hit{prim, t, bary});
+            }
+        }
+    }
+}
+
 bool TraceAny(const PackedScene& scene, const Bvh& bvh, vec3 origin, vec3 direction, float tmin,
               float tmax, AcceptMode mode)
 {
