@@ -207,6 +207,21 @@ HDCX_D float gatan2(float y, float x) { return static_cast<float>(atan2(static_c
 
 #endif  // __CUDACC__
 
+#if defined(__CUDACC__)
+// pow(x, 2.0): x * x in binary32 is the correctly rounded square, the value a
+// binary64 pow rounded once to binary32 returns.
+HDCX_D float gpow2(float x) { return x * x; }
+// pow(x, 5.0): x^5 in binary64 products (x^2 exact), rounded once to binary32;
+// differs from a correctly rounded x^5 only when x^5 lies within ~1.5
+// binary64 ulps of a binary32 rounding boundary.
+HDCX_D float gpow5(float x)
+{
+    const double d = static_cast<double>(x);
+    const double d2 = __dmul_rn(d, d);
+    return __double2float_rn(__dmul_rn(__dmul_rn(d2, d2), d));
+}
+#endif
+
 // lowbias32 integer hash and randomFloat (vulkan_path_tracer.cpp:100-113).
 HDCX_HD uint32_t hashState(uint32_t value)
 {

@@ -27,14 +27,14 @@ HDCX_D Spectrum makeSpectrum(float wavelength)
 {
     Spectrum s;
     s.wavelength = wavelength;
-    s.br = gexp(-0.5f * gpow((wavelength - 620.0f) / 30.0f, 2.0f));
-    s.bg = gexp(-0.5f * gpow((wavelength - 535.0f) / 25.0f, 2.0f));
-    s.bb = gexp(-0.5f * gpow((wavelength - 450.0f) / 20.0f, 2.0f));
+    s.br = gexp(-0.5f * gpow2((wavelength - 620.0f) / 30.0f));
+    s.bg = gexp(-0.5f * gpow2((wavelength - 535.0f) / 25.0f));
+    s.bb = gexp(-0.5f * gpow2((wavelength - 450.0f) / 20.0f));
     s.denominator = gmax(s.br + s.bg + s.bb, 1e-5f);
     const float temperature = 6504.0f;
     const float c2 = 1.4387769e7f;
     const float referenceWavelength = 560.0f;
-    s.planck = gpow(referenceWavelength / wavelength, 5.0f) *
+    s.planck = gpow5(referenceWavelength / wavelength) *
                (gexp(c2 / (referenceWavelength * temperature)) - 1.0f) /
                gmax(gexp(c2 / (wavelength * temperature)) - 1.0f, 1e-5f);
     return s;
@@ -221,7 +221,7 @@ HDCX_D float3 cosineHemisphere(float3 normal, uint32_t& state)
 HDCX_D float fresnelSchlick(float cosTheta, float f0)
 {
     // :202-205
-    return f0 + (1.0f - f0) * gpow(1.0f - clampf(cosTheta, 0.0f, 1.0f), 5.0f);
+    return f0 + (1.0f - f0) * gpow5(1.0f - clampf(cosTheta, 0.0f, 1.0f));
 }
 
 HDCX_D float3 orthogonalTangent(float3 normal, float3 tangent)
@@ -258,7 +258,7 @@ HDCX_D float geometryGGXAnisotropic(float3 direction, float3 normal, float3 tang
     const float3 axisX = orthogonalTangent(normal, tangent);
     const float3 axisY = cross(normal, axisX);
     const float2 alpha = clampRoughness(roughness);
-    const float projected = gpow(alpha.x * dot(direction, axisX), 2.0f) + gpow(alpha.y * dot(direction, axisY), 2.0f);
+    const float projected = gpow2(alpha.x * dot(direction, axisX)) + gpow2(alpha.y * dot(direction, axisY));
     const float lambda = (-1.0f + sqrtf(1.0f + projected / gmax(nDotDirection * nDotDirection, 1e-8f))) * 0.5f;
     return 1.0f / (1.0f + lambda);
 }
@@ -363,7 +363,7 @@ HDCX_D float sheenZeltnerDirectionalAlbedo(float nDotV, float roughness)
     const float s = y * (0.0206607f + 1.58491f * y) / (0.0379424f + y * (1.32227f + y));
     const float m = y * (-0.193854f + y * (-1.14885f + y * (1.7932f - 0.95943f * y * y))) / (0.046391f + y);
     const float o = y * (0.000654023f + (-0.0207818f + 0.119681f * y) * y) / (1.26264f + y * (-1.92021f + y));
-    return clampf(gexp(-0.5f * gpow((x - m) / gmax(s, 1e-6f), 2.0f)) / (gmax(s, 1e-6f) * sqrtf(2.0f * kPi)) + o,
+    return clampf(gexp(-0.5f * gpow2((x - m) / gmax(s, 1e-6f))) / (gmax(s, 1e-6f) * sqrtf(2.0f * kPi)) + o,
                   0.0f, 1.0f);
 }
 
@@ -417,8 +417,8 @@ HDCX_D float evaluateDiffuseReflection(float3 normal, float3 viewDirection, floa
         const float3 halfway = normalize(viewDirection + lightDirection);
         const float lDotH = gmax(dot(lightDirection, halfway), 0.0f);
         const float grazing = 0.5f + 2.0f * clampf(roughness, 0.0f, 1.0f) * lDotH * lDotH;
-        const float lightScatter = 1.0f + (grazing - 1.0f) * gpow(1.0f - nDotL, 5.0f);
-        const float viewScatter = 1.0f + (grazing - 1.0f) * gpow(1.0f - nDotV, 5.0f);
+        const float lightScatter = 1.0f + (grazing - 1.0f) * gpow5(1.0f - nDotL);
+        const float viewScatter = 1.0f + (grazing - 1.0f) * gpow5(1.0f - nDotV);
         return nDotL * lightScatter * viewScatter / kPi;
     }
     if (model == 3u) {
@@ -459,6 +459,8 @@ struct SurfaceParams {
     bool sheenZeltner;
 };
 
+HDCX_D float diffuseLayerSum(float diffuse, float translucent, float specular) { return diffuse + translucent + specular; }
+
 HDCX_D float evaluateDirectSurface(float3 normal, float3 tangent, float3 viewDirection, float3 lightDirection,
                                    const SurfaceParams& p, float diffuseScale, float specularScale)
 {
@@ -487,7 +489,10 @@ HDCX_D float evaluateDirectSurface(float3 normal, float3 tangent, float3 viewDir
         coatSpecular = specularScale * p.coat * nDotL *
                        evaluateGGXAnisotropic(normal, tangent, viewDirection, lightDirection, p.coatRoughness, p.coatF0);
     }
-    const float baseLayer = (1.0f - p.coat * coatFresnel) * (diffuse + translucent + specular) + coatSpecular;
+    const float baseLayer = (1.0f - p.coat * coatFresnel) * (diffuseLayerSum(diffuse, translucent, specular)) + coatSpecular;
+    // With sheen == 0 the sheen terms are exact zeros (the albedo and the
+    // response are finite), leaving baseLayer * 1 + 0.
+    if (p.sheen == 0.0f) return baseLayer;
     const float sheenAlbedo = p.sheenZeltner ? sheenZeltnerDirectionalAlbedo(gmax(dot(normal, viewDirection), 0.0f), p.sheenRoughness)
                                              : sheenDirectionalAlbedo(gmax(dot(normal, viewDirection), 0.0f), p.sheenRoughness);
     const float sheenLayer = specularScale * p.sheen * p.sheenColor *
@@ -556,7 +561,7 @@ HDCX_D float3 sampleHenyeyGreenstein(float3 forward, float anisotropy, uint32_t&
     const float g = clampf(anisotropy, -0.95f, 0.95f);
     const float u = randomFloat(state);
     const float cosine = fabsf(g) < 1e-3f ? 1.0f - 2.0f * u
-                                          : (1.0f + g * g - gpow((1.0f - g * g) / (1.0f - g + 2.0f * g * u), 2.0f)) / (2.0f * g);
+                                          : (1.0f + g * g - gpow2((1.0f - g * g) / (1.0f - g + 2.0f * g * u))) / (2.0f * g);
     const float sine = sqrtf(gmax(1.0f - cosine * cosine, 0.0f));
     const float phi = kTwoPi * randomFloat(state);
     const float3 w = normalize(forward);

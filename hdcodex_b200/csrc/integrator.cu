@@ -445,8 +445,11 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
 
             const float3 viewDirection = normalize(-rayDirection);
             const float nDotView = gmax(dot(normal, viewDirection), 0.0f);
-            const float sheenAlbedo = sheenZeltner ? sheenZeltnerDirectionalAlbedo(nDotView, sheenRoughness)
-                                                   : sheenDirectionalAlbedo(nDotView, sheenRoughness);
+            // sheenAlbedo only ever appears multiplied by sheen; with sheen == 0
+            // those products are exact zeros for any finite albedo.
+            const float sheenAlbedo = sheen == 0.0f ? 0.0f
+                                      : (sheenZeltner ? sheenZeltnerDirectionalAlbedo(nDotView, sheenRoughness)
+                                                      : sheenDirectionalAlbedo(nDotView, sheenRoughness));
             const float sheenProbability = clampf(sheen * sheenAlbedo * luminance1(sheenColor), 0.0f, 0.95f);
             const float coatContribution = coat > 0.0f ? coat * fresnelSchlick(nDotView, coatF0) : 0.0f;
             const float coatProbability = clampf(luminance1(coatContribution), 0.0f, 0.95f);
@@ -671,7 +674,7 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
                 const float cosTheta = gmin(dot(-rayDirection, normal), 1.0f);
                 float r0 = (1.0f - ior) / (1.0f + ior);
                 r0 = r0 * r0;
-                const float fresnel = r0 + (1.0f - r0) * gpow(1.0f - cosTheta, 5.0f);
+                const float fresnel = r0 + (1.0f - r0) * gpow5(1.0f - cosTheta);
                 const float3 refracted = refract(rayDirection, normal, eta);
                 const bool totalInternalReflection = dot(refracted, refracted) < 1e-8f;
                 const bool thinWalled = material->transmissionColorThinWalled.w > 0.5f;
