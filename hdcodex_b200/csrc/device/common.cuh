@@ -121,6 +121,7 @@ struct DeviceScene {
     uint32_t opaque;
     uint32_t hasMeshLights;
     uint32_t nodeCount;
+    uint32_t fullShading;    // 0: no material uses textures or layered lobes (see shadeKernel)
 };
 
 // Per-render constants: the reference's CameraBlock (vulkan_path_tracer.cpp:91-98)

@@ -168,6 +168,31 @@ hdcx_status guarded(hdcx_tracer* t, F&& body)
     }
 }
 
+// Whether any material uses a texture, a layered lobe (coat, sheen,
+// transmission, subsurface, diffuse transmission) or a non-Lambert diffuse
+// model; scenes without these run the specialised shade kernel.
+bool needsFullShading(const PackedSceneData& d)
+{
+    const size_t n = d.materials.size() / HDCX_GPU_MATERIAL_BYTES;
+    for (size_t i = 0; i < n; ++i) {
+        GpuMaterial m;
+        std::memcpy(&m, d.materials.data() + i * HDCX_GPU_MATERIAL_BYTES, sizeof m);
+        const uint32_t* tex = &m.textureIndices0.x;
+        for (int k = 0; k < 24; ++k) {
+            if (tex[k] != HDCX_MISSING_TEXTURE) return true;
+        }
+        if (m.transmissionOpacityIor.x > 0.0F || m.subsurfaceWeightScale.x > 0.0F || m.coatWeightRoughnessIor.x > 0.0F ||
+            m.coatColor.w > 0.0F || m.translucentColorWeight.w > 0.0F ||
+            static_cast<uint32_t>(m.diffuseProperties.y + 0.5F) != 0u) {
+            return true;
+        }
+        if (!(m.transmissionOpacityIor.x <= 0.0F) || !(m.coatColor.w <= 0.0F) || !(m.translucentColorWeight.w <= 0.0F)) {
+            return true;  // NaN weights take the general kernel
+        }
+    }
+    return false;
+}
+
 void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
 {
     check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
@@ -202,6 +227,7 @@ void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
     s.primitiveCount = d.triangleCount();
     s.lightCount = std::min(d.lightCount, static_cast<uint32_t>(HDCX_MAX_LIGHTS));
     s.opaque = d.opaque ? 1u : 0u;
+    s.fullShading = needsFullShading(d) ? 1u : 0u;
     s.hasMeshLights = (d.triangleCount() > 0 && d.emissive[(size_t(d.triangleCount()) - 1) * 4u] > 0.0F) ? 1u : 0u;
     // Padding floor of the BVH quantisation: the scene's coordinate scale.
     float scale = 0.0F;

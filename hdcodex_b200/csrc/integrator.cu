@@ -143,7 +143,21 @@ __global__ void __launch_bounds__(128) extendKernel(DeviceScene s, PathBuffers p
 
 // ---------------------------------------------------------------------------
 // shade
+//
+// shadeKernel<true> evaluates the whole closure. shadeKernel<false> serves
+// scenes whose materials bind no textures and have no coat, sheen,
+// transmission, subsurface or diffuse-transmission weight and use the Lambert
+// diffuse model (DeviceScene::fullShading == 0): there those quantities are
+// the constants the general kernel computes for them (fallback values, zero
+// weights), so both kernels return the same bits and the specialised one
+// carries far less code and state.
 // ---------------------------------------------------------------------------
+template <bool kFull>
+HDCX_D float4 materialTexture(const DeviceScene& s, uint32_t index, float2 uv, float4 fallback)
+{
+    if (!kFull) return fallback;
+    return sampleMaterialTexture(s, index, uv, fallback);
+}
 struct ShadeCtx {
     const DeviceScene& s;
     const FrameConst& f;
@@ -251,6 +265,7 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
     return false;
 }
 
+template <bool kFull>
 __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce,
                                                    const uint32_t* queue, const uint32_t* count, uint32_t* nextQueue,
                                                    uint32_t* nextCount)
@@ -334,8 +349,8 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
             }
             const GpuMaterial* material = s.materials + __ldg(s.triangleMaterials + primitive);
             float3 baseColorRgb = xyz(material->baseColorMetalness);
-            if (material->textureIndices0.x != kMissingTexture) {
-                const float4 sample = sampleMaterialTexture(s, material->textureIndices0.x, surfaceUv, f4(baseColorRgb, 1.0f));
+            if (kFull && material->textureIndices0.x != kMissingTexture) {
+                const float4 sample = materialTexture<kFull>(s, material->textureIndices0.x, surfaceUv, f4(baseColorRgb, 1.0f));
                 const float scaleW = material->baseColorTextureScale.w;
                 const int channel = static_cast<int>(roundf(scaleW));
                 float3 sourceColor;
@@ -349,17 +364,17 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
             }
             const float baseColor = reflectanceSpectrum(baseColorRgb, spec);
             const float metalness = clampf(
-                sampleMaterialTexture(s, material->textureIndices0.y, surfaceUv, f4(material->baseColorMetalness.w)).x, 0.0f, 1.0f);
-            const float4 roughnessSample = sampleMaterialTexture(
+                materialTexture<kFull>(s, material->textureIndices0.y, surfaceUv, f4(material->baseColorMetalness.w)).x, 0.0f, 1.0f);
+            const float4 roughnessSample = materialTexture<kFull>(
                 s, material->textureIndices0.z, surfaceUv,
                 make_float4(material->emissionRoughness.w, material->subsurfaceColor.w, 0.0f, 1.0f));
             const float2 roughness = make_float2(clampf(roughnessSample.x, 0.02f, 1.0f), clampf(roughnessSample.y, 0.02f, 1.0f));
             const float diffuseRoughness = clampf(
-                sampleMaterialTexture(s, material->textureIndices4.z, surfaceUv, f4(material->diffuseProperties.x)).x, 0.0f, 1.0f);
+                materialTexture<kFull>(s, material->textureIndices4.z, surfaceUv, f4(material->diffuseProperties.x)).x, 0.0f, 1.0f);
             const float diffuseWeight = clampf(
-                sampleMaterialTexture(s, material->textureIndices4.w, surfaceUv, f4(material->diffuseProperties.z)).x, 0.0f, 1.0f);
-            const uint32_t diffuseModel = static_cast<uint32_t>(material->diffuseProperties.y + 0.5f);
-            normal = applyNormalMap(s, material->textureIndices1.y, material->coatWeightRoughnessIor.w > 0.5f,
+                materialTexture<kFull>(s, material->textureIndices4.w, surfaceUv, f4(material->diffuseProperties.z)).x, 0.0f, 1.0f);
+            const uint32_t diffuseModel = kFull ? static_cast<uint32_t>(material->diffuseProperties.y + 0.5f) : 0u;
+            if (kFull) normal = applyNormalMap(s, material->textureIndices1.y, material->coatWeightRoughnessIor.w > 0.5f,
                                     material->subsurfaceWeightScale.w, surfaceUv, normal, p0, p1, p2, uv0, uv1, uv2);
             const float3 tangent = surfaceTangent(normal, p0, p1, p2, uv0, uv1, uv2);
             const float3 emissionRgb = surfaceEmissionRgb(s, primitive, surfaceUv);
@@ -374,10 +389,10 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
             }
             radiance += throughput * emission * emissionMisWeight;
 
-            const float transmission = clampf(material->transmissionOpacityIor.x, 0.0f, 1.0f);
+            const float transmission = kFull ? clampf(material->transmissionOpacityIor.x, 0.0f, 1.0f) : 0.0f;
             float3 transmissionColorRgb = xyz(material->transmissionColorThinWalled);
             if (transmission > 0.0f) {
-                const float4 t = sampleMaterialTexture(s, material->textureIndices1.z, surfaceUv, f4(transmissionColorRgb, 1.0f));
+                const float4 t = materialTexture<kFull>(s, material->textureIndices1.z, surfaceUv, f4(transmissionColorRgb, 1.0f));
                 transmissionColorRgb = f3(t.x, t.y, t.z);
             }
             const float transmissionColor = reflectanceSpectrum(transmissionColorRgb, spec);
@@ -386,14 +401,14 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
             float3 subsurfaceColorRgb = xyz(material->subsurfaceColor);
             float3 subsurfaceRadiusRgb = make_float3(gmax(material->subsurfaceRadius.x, 0.001f), gmax(material->subsurfaceRadius.y, 0.001f),
                                                      gmax(material->subsurfaceRadius.z, 0.001f));
-            if (material->subsurfaceWeightScale.x > 0.0f || material->textureIndices2.x != kMissingTexture) {
-                subsurface = clampf(sampleMaterialTexture(s, material->textureIndices2.x, surfaceUv,
+            if (kFull && (material->subsurfaceWeightScale.x > 0.0f || material->textureIndices2.x != kMissingTexture)) {
+                subsurface = clampf(materialTexture<kFull>(s, material->textureIndices2.x, surfaceUv,
                                                           f4(material->subsurfaceWeightScale.x)).x, 0.0f, 1.0f);
                 if (subsurface > 0.0f) {
-                    const float4 c = sampleMaterialTexture(s, material->textureIndices2.y, surfaceUv,
+                    const float4 c = materialTexture<kFull>(s, material->textureIndices2.y, surfaceUv,
                                                            f4(xyz(material->subsurfaceColor), 1.0f));
                     subsurfaceColorRgb = f3(c.x, c.y, c.z);
-                    const float4 r = sampleMaterialTexture(s, material->textureIndices2.z, surfaceUv,
+                    const float4 r = materialTexture<kFull>(s, material->textureIndices2.z, surfaceUv,
                                                            f4(xyz(material->subsurfaceRadius), 1.0f));
                     subsurfaceRadiusRgb = make_float3(gmax(r.x, 0.001f), gmax(r.y, 0.001f), gmax(r.z, 0.001f));
                     const float subsurfaceColor = reflectanceSpectrum(subsurfaceColorRgb, spec);
@@ -403,8 +418,8 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
             const float ior = dispersedIor(gmax(material->transmissionOpacityIor.z, 1.0001f), material->transmissionMedium.z,
                                            material->transmissionMedium.w, wavelength);
             const float specularWeight = clampf(
-                sampleMaterialTexture(s, material->textureIndices3.x, surfaceUv, f4(material->specularWeightColor.x)).x, 0.0f, 1.0f);
-            const float4 specularColorSample = sampleMaterialTexture(
+                materialTexture<kFull>(s, material->textureIndices3.x, surfaceUv, f4(material->specularWeightColor.x)).x, 0.0f, 1.0f);
+            const float4 specularColorSample = materialTexture<kFull>(
                 s, material->textureIndices3.y, surfaceUv,
                 make_float4(material->specularWeightColor.y, material->specularWeightColor.z, material->specularWeightColor.w, 1.0f));
             const float specularColor =
@@ -415,13 +430,13 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
             float coat = 0.0f;
             float2 coatRoughness = make_float2(material->coatWeightRoughnessIor.y, material->subsurfaceRadius.w);
             float coatF0 = 0.0f;
-            if (material->coatWeightRoughnessIor.x > 0.0f || material->textureIndices3.z != kMissingTexture) {
-                coat = clampf(sampleMaterialTexture(s, material->textureIndices3.z, surfaceUv,
+            if (kFull && (material->coatWeightRoughnessIor.x > 0.0f || material->textureIndices3.z != kMissingTexture)) {
+                coat = clampf(materialTexture<kFull>(s, material->textureIndices3.z, surfaceUv,
                                                     f4(material->coatWeightRoughnessIor.x)).x, 0.0f, 1.0f);
                 if (coat > 0.0f) {
-                    const float4 cc = sampleMaterialTexture(s, material->textureIndices3.w, surfaceUv, f4(xyz(material->coatColor), 1.0f));
+                    const float4 cc = materialTexture<kFull>(s, material->textureIndices3.w, surfaceUv, f4(xyz(material->coatColor), 1.0f));
                     const float coatColor = reflectanceSpectrum(f3(cc.x, cc.y, cc.z), spec);
-                    const float4 cr = sampleMaterialTexture(s, material->textureIndices4.x, surfaceUv,
+                    const float4 cr = materialTexture<kFull>(s, material->textureIndices4.x, surfaceUv,
                                                             make_float4(coatRoughness.x, coatRoughness.y, 0.0f, 1.0f));
                     coatRoughness = make_float2(clampf(cr.x, 0.02f, 1.0f), clampf(cr.y, 0.02f, 1.0f));
                     const float coatIor = gmax(material->coatWeightRoughnessIor.z, 1.0001f);
@@ -430,16 +445,18 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
                     coatF0 = clampf(coatReflectance * coatColor, 0.0f, 1.0f);
                 }
             }
-            const float sheen = clampf(sampleMaterialTexture(s, material->textureIndices1.w, surfaceUv, f4(material->coatColor.w)).x, 0.0f, 1.0f);
-            const float4 sheenColorSample = sampleMaterialTexture(s, material->textureIndices2.w, surfaceUv,
+            const float sheen =
+                kFull ? clampf(materialTexture<kFull>(s, material->textureIndices1.w, surfaceUv, f4(material->coatColor.w)).x, 0.0f, 1.0f)
+                      : 0.0f;
+            const float4 sheenColorSample = materialTexture<kFull>(s, material->textureIndices2.w, surfaceUv,
                                                                   f4(xyz(material->sheenColorMode), 1.0f));
             const float sheenColor = reflectanceSpectrum(f3(sheenColorSample.x, sheenColorSample.y, sheenColorSample.z), spec);
             const float sheenRoughness = clampf(
-                sampleMaterialTexture(s, material->textureIndices4.y, surfaceUv, f4(material->transmissionScatter.w)).x, 0.01f, 1.0f);
+                materialTexture<kFull>(s, material->textureIndices4.y, surfaceUv, f4(material->transmissionScatter.w)).x, 0.01f, 1.0f);
             const bool sheenZeltner = material->sheenColorMode.w > 0.5f;
-            const float translucentWeight = clampf(
-                sampleMaterialTexture(s, material->textureIndices5.x, surfaceUv, f4(material->translucentColorWeight.w)).x, 0.0f, 1.0f);
-            const float4 translucentSample = sampleMaterialTexture(s, material->textureIndices5.y, surfaceUv,
+            const float translucentWeight = !kFull ? 0.0f : clampf(
+                materialTexture<kFull>(s, material->textureIndices5.x, surfaceUv, f4(material->translucentColorWeight.w)).x, 0.0f, 1.0f);
+            const float4 translucentSample = materialTexture<kFull>(s, material->textureIndices5.y, surfaceUv,
                                                                    f4(xyz(material->translucentColorWeight), 1.0f));
             const float translucentColor = reflectanceSpectrum(f3(translucentSample.x, translucentSample.y, translucentSample.z), spec);
 
@@ -1029,7 +1046,11 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
             CUDA_OK(cudaMemsetAsync(outCount, 0, sizeof(uint32_t), stream));
             CUDA_OK(cudaMemsetAsync(paths.counters + 2, 0, sizeof(uint32_t), stream));
             timed(1, [&] {
-                shadeKernel<<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+                if (scene.fullShading) {
+                    shadeKernel<true><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+                } else {
+                    shadeKernel<false><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+                }
             });
             CUDA_OK(cudaGetLastError());
             timed(2, [&] {
