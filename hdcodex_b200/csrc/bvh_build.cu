@@ -5,11 +5,9 @@
 // triangles, one identity TLAS). Steps, all on the device:
 //   1. triangle boxes and the scene box;
 //   2. 63-bit Morton codes of the box centres, sorted with their triangle ids;
-//   3. the binary radix tree of Karras, "Maximizing Parallelism in the
-//      Construction of BVHs, Octrees, and k-d Trees", HPG 2012 (equal codes are
-//      split by index);
-//   4. bottom-up boxes, triangle counts and surface areas;
-//   5. a top-down collapse into 8-wide nodes: each wide node repeatedly opens
+//   3. a binary tree by PLOC agglomerative clustering in Morton order, with
+//      node boxes and triangle counts;
+//   4. a top-down collapse into 8-wide nodes: each wide node repeatedly opens
 //      its largest child that is too big for a leaf, then opens small subtrees
 //      while slots remain; children take the octant slot their centre points
 //      to, so traversal visits them nearest first; child boxes are quantised to
@@ -115,72 +113,88 @@ __global__ void mortonKernel(const float4* boxLo, const float4* boxHi, uint32_t 
     ids[i] = i;
 }
 
-__device__ __forceinline__ int delta(const uint64_t* keys, int n, int i, int j)
-{
-    if (j < 0 || j >= n) return -1;
-    const uint64_t a = keys[i], b = keys[j];
-    if (a == b) return 64 + __clz(static_cast<uint32_t>(i ^ j));
-    return __clzll(static_cast<long long>(a ^ b));
-}
+// ---------------------------------------------------------------------------
+// Binary tree: PLOC (Meister and Bittner, "Parallel Locally-Ordered Clustering
+// for Bounding Volume Hierarchy Construction", IEEE TVCG 2018). Clusters stay
+// in Morton order; each pass every cluster finds the neighbour within
+// +-kSearchRadius positions whose merged box has the smallest surface area,
+// mutual nearest neighbours merge into a new internal node, and the cluster
+// list is compacted, until one cluster (the root) is left. Candidates of equal
+// area are ordered by their index pair, so the globally best pair is always
+// mutual and every pass makes progress.
+// Binary node ids: internal 0..n-2 (in merge order), leaf k -> (n-1)+k.
+// nodeLo.w holds the subtree's triangle count.
+// ---------------------------------------------------------------------------
+constexpr int kSearchRadius = 16;
 
-// Binary node ids: internal 0..n-2, leaf k -> (n-1)+k.
-__global__ void karrasKernel(const uint64_t* keys, int n, int* left, int* right, int* parent)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1) return;
-    const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
-    const int deltaMin = delta(keys, n, i, i - d);
-    int lmax = 2;
-    while (delta(keys, n, i, i + lmax * d) > deltaMin) lmax *= 2;
-    int l = 0;
-    for (int t = lmax / 2; t >= 1; t /= 2) {
-        if (delta(keys, n, i, i + (l + t) * d) > deltaMin) l += t;
-    }
-    const int j = i + l * d;
-    const int deltaNode = delta(keys, n, i, j);
-    int s = 0;
-    for (int div = 2;; div *= 2) {
-        const int t = (l + div - 1) / div;
-        if (delta(keys, n, i, i + (s + t) * d) > deltaNode) s += t;
-        if (t <= 1) break;
-    }
-    const int gamma = i + s * d + min(d, 0);
-    const int lo = min(i, j), hi = max(i, j);
-    const int leftNode = (lo == gamma) ? (n - 1) + gamma : gamma;
-    const int rightNode = (hi == gamma + 1) ? (n - 1) + gamma + 1 : gamma + 1;
-    left[i] = leftNode;
-    right[i] = rightNode;
-    parent[leftNode] = i;
-    parent[rightNode] = i;
-}
-
-__global__ void bottomUpKernel(int n, const uint32_t* sortedIds, const float4* triLo, const float4* triHi, const int* left,
-                               const int* right, const int* parent, float4* nodeLo, float4* nodeHi, uint32_t* visits)
+__global__ void initLeavesKernel(int n, const uint32_t* sortedIds, const float4* triLo, const float4* triHi,
+                                 float4* nodeLo, float4* nodeHi, int* clusters)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    int node = (n - 1) + k;
     const uint32_t prim = sortedIds[k];
-    float4 lo = triLo[prim], hi = triHi[prim];
-    lo.w = 1.0f;  // triangle count in .w of lo
-    nodeLo[node] = lo;
-    nodeHi[node] = hi;
-    __threadfence();
-    while (true) {
-        const int p = parent[node];
-        if (p < 0) break;
-        if (atomicAdd(&visits[p], 1u) == 0u) break;  // the sibling finishes the parent
-        __threadfence();
-        const int a = left[p], b = right[p];
-        const float4 la = __ldcg(nodeLo + a), lb = __ldcg(nodeLo + b);
-        const float4 ha = __ldcg(nodeHi + a), hb = __ldcg(nodeHi + b);
-        const float4 l2 = make_float4(fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z), la.w + lb.w);
-        const float4 h2 = make_float4(fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z), 0.0f);
-        nodeLo[p] = l2;
-        nodeHi[p] = h2;
-        __threadfence();
-        node = p;
+    float4 lo = triLo[prim];
+    lo.w = 1.0f;
+    nodeLo[(n - 1) + k] = lo;
+    nodeHi[(n - 1) + k] = triHi[prim];
+    clusters[k] = (n - 1) + k;
+}
+
+__device__ __forceinline__ float mergedArea(float4 la, float4 ha, float4 lb, float4 hb)
+{
+    const float dx = fmaxf(ha.x, hb.x) - fminf(la.x, lb.x);
+    const float dy = fmaxf(ha.y, hb.y) - fminf(la.y, lb.y);
+    const float dz = fmaxf(ha.z, hb.z) - fminf(la.z, lb.z);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void nearestNeighbourKernel(const int* clusters, int m, const float4* nodeLo, const float4* nodeHi, int* nn)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int ci = clusters[i];
+    const float4 li = nodeLo[ci], hi = nodeHi[ci];
+    float best = 3.4e38f;
+    int bestJ = -1;
+    const int j0 = max(0, i - kSearchRadius), j1 = min(m - 1, i + kSearchRadius);
+    for (int j = j0; j <= j1; ++j) {
+        if (j == i) continue;
+        const int cj = clusters[j];
+        const float a = mergedArea(li, hi, nodeLo[cj], nodeHi[cj]);
+        // Candidates are visited in increasing j, so the first of equal areas
+        // is the one with the smallest (min(i,j), max(i,j)) pair.
+        if (a < best || bestJ < 0) {
+            best = a;
+            bestJ = j;
+        }
     }
+    nn[i] = bestJ;
+}
+
+__global__ void mergeKernel(const int* clusters, int m, const int* nn, int* left, int* right, float4* nodeLo,
+                            float4* nodeHi, uint32_t* nodeCounter, int* merged, int* keep)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int j = nn[i];
+    const bool mutual = j >= 0 && nn[j] == i;
+    if (mutual && i > j) {
+        keep[i] = 0;  // merged by its partner
+        return;
+    }
+    keep[i] = 1;
+    if (!mutual) {
+        merged[i] = clusters[i];
+        return;
+    }
+    const int a = clusters[i], b = clusters[j];
+    const int k = static_cast<int>(atomicAdd(nodeCounter, 1u));
+    const float4 la = nodeLo[a], lb = nodeLo[b], ha = nodeHi[a], hb = nodeHi[b];
+    left[k] = a;
+    right[k] = b;
+    nodeLo[k] = make_float4(fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z), la.w + lb.w);
+    nodeHi[k] = make_float4(fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z), 0.0f);
+    merged[i] = k;
 }
 
 struct CollapseItem {
@@ -445,14 +459,35 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
         const int nodes = 2 * n - 1;
         int* left = static_cast<int*>(tmp(sizeof(int) * std::max(n - 1, 1)));
         int* right = static_cast<int*>(tmp(sizeof(int) * std::max(n - 1, 1)));
-        int* parent = static_cast<int*>(tmp(sizeof(int) * nodes));
-        CUDA_OK(cudaMemsetAsync(parent, 0xff, sizeof(int) * nodes, stream));
-        if (n > 1) karrasKernel<<<(n - 1 + kBlock - 1) / kBlock, kBlock, 0, stream>>>(keysSorted, n, left, right, parent);
         float4* nodeLo = static_cast<float4*>(tmp(sizeof(float4) * nodes));
         float4* nodeHi = static_cast<float4*>(tmp(sizeof(float4) * nodes));
-        uint32_t* visits = static_cast<uint32_t*>(tmp(sizeof(uint32_t) * std::max(n - 1, 1)));
-        CUDA_OK(cudaMemsetAsync(visits, 0, sizeof(uint32_t) * std::max(n - 1, 1), stream));
-        bottomUpKernel<<<blocks, kBlock, 0, stream>>>(n, idsSorted, triLo, triHi, left, right, parent, nodeLo, nodeHi, visits);
+        int* clustersA = static_cast<int*>(tmp(sizeof(int) * n));
+        int* clustersB = static_cast<int*>(tmp(sizeof(int) * n));
+        int* nn = static_cast<int*>(tmp(sizeof(int) * n));
+        int* keep = static_cast<int*>(tmp(sizeof(int) * n));
+        uint32_t* plocCounters = static_cast<uint32_t*>(tmp(sizeof(uint32_t) * 2));  // internal nodes, clusters
+        CUDA_OK(cudaMemsetAsync(plocCounters, 0, sizeof(uint32_t) * 2, stream));
+        initLeavesKernel<<<blocks, kBlock, 0, stream>>>(n, idsSorted, triLo, triHi, nodeLo, nodeHi, clustersA);
+        size_t selectBytes = 0;
+        CUDA_OK(cub::DeviceSelect::Flagged(nullptr, selectBytes, clustersB, keep, clustersA, plocCounters + 1, n, stream));
+        void* selectTemp = tmp(selectBytes);
+        int m = n;
+        while (m > 1) {
+            const int mb = (m + kBlock - 1) / kBlock;
+            nearestNeighbourKernel<<<mb, kBlock, 0, stream>>>(clustersA, m, nodeLo, nodeHi, nn);
+            mergeKernel<<<mb, kBlock, 0, stream>>>(clustersA, m, nn, left, right, nodeLo, nodeHi, plocCounters, clustersB,
+                                                   keep);
+            CUDA_OK(cub::DeviceSelect::Flagged(selectTemp, selectBytes, clustersB, keep, clustersA, plocCounters + 1, m,
+                                               stream));
+            uint32_t next = 0;
+            CUDA_OK(cudaMemcpyAsync(&next, plocCounters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            CUDA_OK(cudaStreamSynchronize(stream));
+            if (static_cast<int>(next) >= m) throw std::runtime_error("BVH build: clustering made no progress");
+            m = static_cast<int>(next);
+        }
+        int rootNode = 0;
+        CUDA_OK(cudaMemcpyAsync(&rootNode, clustersA, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_OK(cudaStreamSynchronize(stream));
 
         out.nodes = deviceAlloc<WideNode>(n);
         out.triVerts = deviceAlloc<float4>(3 * static_cast<size_t>(n));
@@ -461,7 +496,7 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
         CUDA_OK(cudaMemcpyAsync(counters, initCounters, sizeof initCounters, cudaMemcpyHostToDevice, stream));
         CollapseItem* itemsA = static_cast<CollapseItem*>(tmp(sizeof(CollapseItem) * n));
         CollapseItem* itemsB = static_cast<CollapseItem*>(tmp(sizeof(CollapseItem) * n));
-        const CollapseItem root{n > 1 ? 0 : 0 /* leaf id n-1 == 0 when n == 1 */, 0u, 0u, 0u};
+        const CollapseItem root{rootNode, 0u, 0u, 0u};
         CUDA_OK(cudaMemcpyAsync(itemsA, &root, sizeof root, cudaMemcpyHostToDevice, stream));
         CollapseArgs args{n, left, right, nodeLo, nodeHi, idsSorted, vertices, indices, sceneScale,
                           out.nodes, out.triVerts, counters + 0, counters + 1, counters + 2};
