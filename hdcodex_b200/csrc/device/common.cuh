@@ -8,8 +8,9 @@
 //   * dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z; normalize(v) = v * (1/sqrt(dot(v, v)));
 //   * GLSL min/max/clamp/mix/smoothstep/reflect/refract/fract follow the GLSL
 //     4.60 formulas;
-//   * exp, log, pow, sin, cos, acos and atan2 are evaluated in binary64 and
-//     rounded once to binary32; pow follows C99 pow (pow(x, 0) = 1).
+//   * exp, log, pow, sin, cos, acos and atan2 are the binary32 functions of
+//     hdcx/fpmath.h (fixed sequences of binary32 operations and fused
+//     multiply-adds, so host and device evaluations agree bit for bit).
 // Every vec3 the GLSL integrator carries per wavelength lane (throughput,
 // radiance, colours after reflectanceSpectrum) holds one value in all three
 // components, so the device code carries it as one float; luminance() of such
@@ -18,6 +19,8 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+
+#include "hdcx/fpmath.h"
 
 namespace hdcx {
 
@@ -197,30 +200,23 @@ HDCX_D float3 refract(float3 i, float3 n, float eta)
 }
 HDCX_D float radians(float degrees) { return degrees * 0.017453292519943295f; }
 
-// Transcendentals: binary64 evaluation, one rounding to binary32.
-HDCX_D float gexp(float x) { return static_cast<float>(exp(static_cast<double>(x))); }
-HDCX_D float glog(float x) { return static_cast<float>(log(static_cast<double>(x))); }
-HDCX_D float gpow(float x, float y) { return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y))); }
-HDCX_D float gsin(float x) { return static_cast<float>(sin(static_cast<double>(x))); }
-HDCX_D float gcos(float x) { return static_cast<float>(cos(static_cast<double>(x))); }
-HDCX_D float gacos(float x) { return static_cast<float>(acos(static_cast<double>(x))); }
-HDCX_D float gatan2(float y, float x) { return static_cast<float>(atan2(static_cast<double>(y), static_cast<double>(x))); }
+// Transcendentals: the binary32 functions of hdcx/fpmath.h, bit-identical to
+// the CPU evaluations of the integrator.
+HDCX_D float gexp(float x) { return hdcx_fp_exp(x); }
+HDCX_D float glog(float x) { return hdcx_fp_log(x); }
+HDCX_D float gpow(float x, float y) { return hdcx_fp_pow(x, y); }
+HDCX_D float gsin(float x) { return hdcx_fp_sin(x); }
+HDCX_D float gcos(float x) { return hdcx_fp_cos(x); }
+HDCX_D float gacos(float x) { return hdcx_fp_acos(x); }
+HDCX_D float gatan2(float y, float x) { return hdcx_fp_atan2(y, x); }
 
 #endif  // __CUDACC__
 
 #if defined(__CUDACC__)
-// pow(x, 2.0): x * x in binary32 is the correctly rounded square, the value a
-// binary64 pow rounded once to binary32 returns.
+// pow(x, 2.0) and pow(x, 5.0) at call sites whose exponent is a constant:
+// the same values hdcx_fp_pow returns for those exponents.
 HDCX_D float gpow2(float x) { return x * x; }
-// pow(x, 5.0): x^5 in binary64 products (x^2 exact), rounded once to binary32;
-// differs from a correctly rounded x^5 only when x^5 lies within ~1.5
-// binary64 ulps of a binary32 rounding boundary.
-HDCX_D float gpow5(float x)
-{
-    const double d = static_cast<double>(x);
-    const double d2 = __dmul_rn(d, d);
-    return __double2float_rn(__dmul_rn(__dmul_rn(d2, d2), d));
-}
+HDCX_D float gpow5(float x) { return hdcx_fp_pow5(x); }
 #endif
 
 // lowbias32 integer hash and randomFloat (vulkan_path_tracer.cpp:100-113).

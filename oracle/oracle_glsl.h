@@ -16,14 +16,16 @@
 //     normalize(v) = v * (1 / sqrt(dot(v, v)));
 //   * mix, clamp, smoothstep, reflect, refract and fract follow the GLSL 4.60
 //     specification formulas;
-//   * transcendentals (exp, log, pow, sin, cos, acos, atan) are evaluated in
-//     binary64 and rounded once to binary32, so they are correctly rounded
-//     except in vanishingly rare double-rounding cases; pow follows C99 pow
-//     (pow(x, 0) = 1, exact for integral exponents of negative bases).
+//   * transcendentals (exp, log, pow, sin, cos, acos, atan) are the binary32
+//     functions of hdcx/fpmath.h: fixed sequences of binary32 operations and
+//     fused multiply-adds (fmaf), bit-identical on host and device; pow(x, 2)
+//     is x * x and pow(x, 5) is x^5 in exact binary64 products.
 #pragma once
 
 #include <cmath>
 #include <cstdint>
+
+#include "hdcx/fpmath.h"
 
 namespace oracle {
 
@@ -127,20 +129,15 @@ inline vec3 refract(vec3 i, vec3 n, float eta)
 inline bool anyGreaterThanZero(vec3 v) { return v.x > 0.0f || v.y > 0.0f || v.z > 0.0f; }
 inline float radians(float degrees) { return degrees * 0.017453292519943295f; }
 
-// Transcendentals: binary64 evaluation, one rounding to binary32.
-inline float gexp(float x) { return static_cast<float>(std::exp(static_cast<double>(x))); }
-inline float glog(float x) { return static_cast<float>(std::log(static_cast<double>(x))); }
-inline float gpow(float x, float y)
-{
-    return static_cast<float>(std::pow(static_cast<double>(x), static_cast<double>(y)));
-}
-inline float gsin(float x) { return static_cast<float>(std::sin(static_cast<double>(x))); }
-inline float gcos(float x) { return static_cast<float>(std::cos(static_cast<double>(x))); }
-inline float gacos(float x) { return static_cast<float>(std::acos(static_cast<double>(x))); }
-inline float gatan2(float y, float x)
-{
-    return static_cast<float>(std::atan2(static_cast<double>(y), static_cast<double>(x)));
-}
+// Transcendentals: the binary32 functions of hdcx/fpmath.h (the device
+// integrator calls the same functions, so both produce the same bits).
+inline float gexp(float x) { return hdcx_fp_exp(x); }
+inline float glog(float x) { return hdcx_fp_log(x); }
+inline float gpow(float x, float y) { return hdcx_fp_pow(x, y); }
+inline float gsin(float x) { return hdcx_fp_sin(x); }
+inline float gcos(float x) { return hdcx_fp_cos(x); }
+inline float gacos(float x) { return hdcx_fp_acos(x); }
+inline float gatan2(float y, float x) { return hdcx_fp_atan2(y, x); }
 
 inline float uintToFloat(uint32_t v) { return static_cast<float>(v); }
 

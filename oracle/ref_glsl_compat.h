@@ -9,8 +9,8 @@
 // oracle/_ref/. Nothing of the reference's source is kept in this repository.
 //
 // Semantics: binary32 vector arithmetic component by component, in source
-// order (compiled with -ffp-contract=off); transcendentals evaluated in
-// binary64 and rounded once to binary32 (the same rule as the oracle);
+// order (compiled with -ffp-contract=off); transcendentals are the binary32
+// functions of hdcx/fpmath.h (the same rule as the oracle);
 // GLSL builtin formulas from the GLSL 4.60 specification.
 #pragma once
 
@@ -18,6 +18,8 @@
 #include <cstring>
 #include <algorithm>
 #include <cmath>
+
+#include "hdcx/fpmath.h"
 
 namespace glsl {
 
@@ -188,16 +190,15 @@ inline vec3 refract(const vec3& i, const vec3& n, float eta)
     return eta * i - (eta * d + std::sqrt(k)) * n;
 }
 inline float radians(float d) { return d * 0.017453292519943295f; }
-inline float exp(float x) { return static_cast<float>(std::exp(static_cast<double>(x))); }
-inline float log(float x) { return static_cast<float>(std::log(static_cast<double>(x))); }
-inline float pow(float x, float y) { return static_cast<float>(std::pow(static_cast<double>(x), static_cast<double>(y))); }
-inline float sin(float x) { return static_cast<float>(std::sin(static_cast<double>(x))); }
-inline float cos(float x) { return static_cast<float>(std::cos(static_cast<double>(x))); }
-inline float acos(float x) { return static_cast<float>(std::acos(static_cast<double>(x))); }
-inline float atan(float y, float x)
-{
-    return static_cast<float>(std::atan2(static_cast<double>(y), static_cast<double>(x)));
-}
+// GLSL leaves the precision of these builtins to the implementation; this
+// harness evaluates them with the binary32 functions of hdcx/fpmath.h.
+inline float exp(float x) { return hdcx_fp_exp(x); }
+inline float log(float x) { return hdcx_fp_log(x); }
+inline float pow(float x, float y) { return hdcx_fp_pow(x, y); }
+inline float sin(float x) { return hdcx_fp_sin(x); }
+inline float cos(float x) { return hdcx_fp_cos(x); }
+inline float acos(float x) { return hdcx_fp_acos(x); }
+inline float atan(float y, float x) { return hdcx_fp_atan2(y, x); }
 inline int bitCount(uint v) { return __builtin_popcount(v); }
 inline bvec3 greaterThan(const vec3& a, const vec3& b) { return bvec3{a.x > b.x, a.y > b.y, a.z > b.z}; }
 inline bool any(const bvec3& v) { return v.x || v.y || v.z; }
