@@ -19,6 +19,7 @@
 
 #include "bvh_build.h"
 #include "integrator.h"
+#include "render_static.h"
 #include "scene_pack.h"
 
 namespace {
@@ -591,6 +592,31 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint
         t->stats.extension_triangle_tests = counters[4];
         t->stats.shadow_node_visits = counters[5];
         t->stats.shadow_triangle_tests = counters[6];
+        if (written) *written = 1;
+    });
+}
+
+HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* t, const hdcx_camera* camera, uint32_t width, uint32_t height,
+                                        uint32_t sampleIndex, uint32_t maxBounces, uint32_t sampleCount,
+                                        float* rgbaDevice, int32_t* written)
+{
+    if (!t || !camera || !rgbaDevice) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (written) *written = 0;
+    if (!t->geometryReady || width == 0 || height == 0) return HDCX_OK;
+    if (uint64_t(width) * height > kStaticMaxPixels) {
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT,
+                    "hdcx_render_static: width*height = " + std::to_string(uint64_t(width) * height) +
+                        " exceeds its maximum of " + std::to_string(kStaticMaxPixels) + " pixels");
+    }
+    if (reinterpret_cast<uintptr_t>(rgbaDevice) % 16u != 0u)
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_render_static: rgba_device must be 16-byte aligned");
+    return guarded(t, [&] {
+        if (!t->fallbackAxisInitialized) {
+            t->fallbackZUp = std::fabs(camera->vertical[2]) > std::fabs(camera->vertical[1]);
+            t->fallbackAxisInitialized = true;
+        }
+        const FrameConst f = makeFrame(t, *camera, width, height, sampleIndex, maxBounces, sampleCount);
+        renderStatic(t->scene, f, reinterpret_cast<float4*>(rgbaDevice), t->stream);
         if (written) *written = 1;
     });
 }

@@ -55,6 +55,8 @@ SIGNATURES = {
     "hdcx_get_shading_mode": (C.c_int32, [_P]),
     "hdcx_render": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                               C.c_uint32, _P, C.POINTER(C.c_int32)]),
+    "hdcx_render_static": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                     C.c_uint32, _P, C.POINTER(C.c_int32)]),
     "hdcx_read_rgba": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint64]),
     "hdcx_read_xyz": (C.c_int, [_P, C.POINTER(C.c_double), C.c_uint64, C.POINTER(C.c_uint64)]),
     "hdcx_device_rgba": (C.c_int, [_P, C.POINTER(C.c_void_p)]),

@@ -389,6 +389,42 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* tracer, const hdcx_camera* camera,
                                  uint32_t sample_count, float* rgba_out,
                                  int32_t* written);
 
+/* hdcx_render for callers that cannot allocate device memory. No counterpart
+ * in the reference: VulkanPathTracer has no entry point of this kind.
+ *
+ * Who needs it: a plugin running inside a host application that reserves the
+ * GPU's memory for itself and gives plugins no allocator, and interactive
+ * loops that cannot afford the device-wide synchronisation cudaFree (and often
+ * cudaMalloc) implies. hdcx_render allocates path state and per-pixel sums on
+ * its first call and whenever the image size grows; this entry point calls no
+ * allocator (no cudaMalloc, no cudaFree, no allocating library routine).
+ *
+ * Same integrator and results as hdcx_render, except where the image lives:
+ * the running mean is the caller's device buffer `rgba_device`
+ * (width*height*4 floats, 16-byte aligned), read when sample_index > 0 and
+ * written on every call, in place of the tracer's own accumulation buffer
+ * (which this call neither reads nor writes; hdcx_read_rgba, hdcx_read_xyz and
+ * hdcx_get_stats are not updated). The caller's earlier work on rgba_device
+ * must have finished before the call; the call returns once the image is
+ * written.
+ *
+ * The scratch (the path state of one wave of 65,536 paths and the per-pixel
+ * sums of one frame) is one static device array of 61,538,816 bytes inside
+ * the library, which every GPU that loads the library keeps until the process
+ * exits. Images above 1,048,576 pixels (width*height) are rejected with
+ * HDCX_ERROR_INVALID_ARGUMENT and a message. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture. All calls on a
+ * device share the array, which keeps the last call's contents, so calls whose
+ * GPU work overlapped would race: the library holds a per-device lock for the
+ * whole call, GPU work included. With no geometry or a zero size nothing is
+ * traced and *written = 0; otherwise *written = 1. */
+HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* tracer, const hdcx_camera* camera,
+                                        uint32_t width, uint32_t height,
+                                        uint32_t sample_index, uint32_t max_bounces,
+                                        uint32_t sample_count, float* rgba_device,
+                                        int32_t* written);
+
 /* Copies the current device RGBA32F accumulation (width*height*4 floats). */
 HDCX_API hdcx_status hdcx_read_rgba(hdcx_tracer* tracer, float* rgba_out, uint64_t float_count);
 
