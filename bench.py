@@ -18,8 +18,10 @@ Printed JSON line:
                 triangle tested, visits counted by a counting pass) over its
                 CUDA-event time, against the measured HBM copy bandwidth;
   cpu_baseline- the CPU oracle on the host cores on a centre crop.
-`--impl reference` times the CPU restatement of the reference integrator (the
-oracle) on the same workload and metric, on rank 0 only.
+`--impl reference` times the reference's own integrator on the host cores, on
+rank 0 only: its GLSL compiled as C++ (oracle/_ref, built from the reference's
+sources by oracle/ref_build.py) when that library is present, else the
+oracle's restatement; same workload and metric, a centre crop per step.
 """
 from __future__ import annotations
 
@@ -84,7 +86,8 @@ def measured_peaks():
 
 
 def traffic_from_profile():
-    """dram bytes per closest-hit launch from the committed ncu summary, if any."""
+    """DRAM bytes per extension ray of the closest-hit kernel from the committed
+    ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "extend_kernel_traffic.json")
     try:
         with open(path) as f:
@@ -206,16 +209,28 @@ def cpu_baseline(wl, target_seconds, rank0=True):
             "rays_per_s": (ext + sh + ss) / secs}
 
 
+def workload_config(wl, world):
+    from hdcodex_b200 import workloads
+    return {"workload": wl.name, "triangles": workloads.triangle_count(wl.scene), "width": wl.width,
+            "height": wl.height, "spp": wl.spp, "max_bounces": wl.max_bounces, "spectral_lanes": 3,
+            "spectral_paths_per_step_per_gpu": wl.spectral_paths,
+            "l2": "inputs larger than L2 (scene + BVH + dome + per-wave path state)",
+            "parallelism": f"replicas x{world}, disjoint sample ranges"}
+
+
 def run_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return  # rank 0 alone times the CPU reference
     wl = make_workload(args.workload)
     import oracle as O
-    O.build()
-    t = O.OracleTracer()
+    if O.ref_available():
+        t, kind = O.ReferenceTracer(), "reference"
+    else:
+        O.build()
+        t, kind = O.OracleTracer(), "port"
     t.set_scene(wl.scene)
     threads = os.cpu_count() or 1
-    side = 32
+    side = 64
     cx, cy = wl.width // 2, wl.height // 2
     crop = (cx - side // 2, cy - side // 2, cx + side // 2, cy + side // 2)
     for i in range(args.warmup):
@@ -229,13 +244,14 @@ def run_reference(args):
     paths = side * side * wl.spp * 3 * args.steps
     value = paths / sum(times)
     sample = f"{side}x{side} centre crop of the {wl.width}x{wl.height} frame at {wl.spp} spp per step"
+    if kind == "reference":
+        sample += " (the reference's GLSL integrator compiled as C++, ray queries on a CPU BVH)"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
-                   "max_bounces": wl.max_bounces},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "config": workload_config(wl, args.gpus),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -258,7 +274,6 @@ def run_hdcx(args):
                           "stats": tracer.stats()}), flush=True)
         tracer.close()
         return
-    tri_count = workloads.triangle_count(wl.scene)
     paths_per_step = wl.spectral_paths
 
     def sample_index(step):
@@ -327,7 +342,10 @@ def run_hdcx(args):
         "kernel": "extendKernel (closest-hit traversal)",
         "bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
         "frac": (achieved_gbs / peak) if achieved_gbs else None, "peak_source": peak_kind,
-        "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+        # ncu DRAM bytes per extension ray (profiles/extend_kernel_traffic.json,
+        # captured on a smaller frame) times this run's rays per launch.
+        "traffic": (traffic["dram_bytes_per_ray"] * ext_rays / extend_launches
+                    if traffic and extend_launches else None),
         "algorithmic_bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray,
         "triangles_per_ray": tris_per_ray, "extend_ms_per_step": extend_ms / args.steps,
         "extend_launches_per_step": extend_launches / args.steps,
@@ -347,11 +365,7 @@ def run_hdcx(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl.name, "triangles": tri_count, "width": wl.width, "height": wl.height,
-                       "spp": wl.spp, "max_bounces": wl.max_bounces, "spectral_lanes": 3,
-                       "spectral_paths_per_step_per_gpu": paths_per_step,
-                       "l2": "inputs larger than L2 (scene + BVH + dome + per-wave path state)",
-                       "parallelism": f"replicas x{world}, disjoint sample ranges"},
+            "config": workload_config(wl, world),
             "rays_per_s": (ext_rays + sh_rays + ss_rays) * world / (total_ms / 1000.0),
             "extension_rays_per_step": ext_rays / args.steps, "shadow_rays_per_step": sh_rays / args.steps,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48,
