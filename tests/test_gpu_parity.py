@@ -4,12 +4,12 @@
   candidate, ties to the smaller flattened primitive index).
 * Per-pixel RGBA32F and FP64 XYZ at fixed spp: both sides evaluate the same
   binary32 operation sequence (see the arithmetic contract in
-  hdcodex_b200/csrc/device/common.cuh and oracle/oracle_glsl.h), so almost
-  every pixel is bit-identical. The only admitted source of difference is a
-  binary64 transcendental whose CUDA and glibc results straddle a binary32
-  rounding boundary, which changes one value by one ulp and can send that one
-  path elsewhere. Tolerance: at least 99% of pixels bit-identical and the
-  image-level relative L1 difference below 1e-3.
+  hdcodex_b200/csrc/device/common.cuh and oracle/oracle_glsl.h), with the same
+  transcendental functions (include/hdcx/fpmath.h), so the images are
+  bit-identical (measured: every pixel of every scene here). The tolerance
+  still admits a rare one-ulp difference that sends one path elsewhere: at
+  least 99% of pixels bit-identical and the image-level relative L1
+  difference below 1e-3.
 """
 import numpy as np
 import pytest
