@@ -50,7 +50,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hdcx", choices=["hdcx", "reference"])
-    ap.add_argument("--workload", default="heavy", choices=["heavy", "box"])
+    ap.add_argument("--workload", default="heavy", choices=["heavy", "box", "stress"],
+                    help="heavy: 1.0M triangles, 1920x1080, 64 spp (the headline); box: 34-triangle closed box, "
+                         "256x256, 16 spp; stress: 200k-triangle spectral stress scene, 1280x720, 256 spp")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -61,18 +63,19 @@ def parse():
     return ap.parse_args()
 
 
+WORKLOADS = {"heavy": "heavy_geometry", "box": "closed_box", "stress": "spectral_stress"}
+
+
 def make_workload(name, args=None):
+    """The named workload; --width/--height/--spp (profiling only) resize it."""
     from hdcodex_b200 import workloads
-    wl = workloads.closed_box() if name == "box" else workloads.heavy_geometry()
-    if args is not None and (args.width or args.height or args.spp):
-        from hdcodex_b200.workloads import look_at_camera
-        w = args.width or wl.width
-        h = args.height or wl.height
-        if name != "box":
-            wl.camera = look_at_camera((0.0, 7.5, 17.0), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), 45.0, w / h)
-        wl.width, wl.height = w, h
-        wl.spp = args.spp or wl.spp
-    return wl
+    make = getattr(workloads, WORKLOADS[name])
+    overrides = {}
+    if args is not None:
+        for key in ("width", "height", "spp"):
+            if getattr(args, key):
+                overrides[key] = getattr(args, key)
+    return make(**overrides)
 
 
 def measured_peaks():

@@ -251,5 +251,133 @@ def heavy_geometry(width=1920, height=1080, spp=64, max_bounces=8, seed=0, spher
     return Workload("heavy-geometry-1.0M-tri-dome", s, cam, width, height, spp, max_bounces)
 
 
+def _torus(major: float, minor: float, segments: int, rings: int):
+    u = np.arange(segments) * (2 * math.pi / segments)
+    v = np.arange(rings) * (2 * math.pi / rings)
+    U, V = np.meshgrid(u, v, indexing="ij")
+    x = (major + minor * np.cos(V)) * np.cos(U)
+    z = (major + minor * np.cos(V)) * np.sin(U)
+    y = minor * np.sin(V)
+    verts = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    i, j = np.meshgrid(np.arange(segments), np.arange(rings), indexing="ij")
+    a = (i * rings + j).ravel()
+    b = (((i + 1) % segments) * rings + j).ravel()
+    c = (i * rings + (j + 1) % rings).ravel()
+    d = (((i + 1) % segments) * rings + (j + 1) % rings).ravel()
+    faces = np.stack([np.stack([a, c, b], 1), np.stack([b, c, d], 1)], 1).reshape(-1, 3)
+    return verts, faces.astype(np.uint32)
+
+
+def _grid_top(x0, x1, z0, z1, y, nx, nz):
+    xs = np.linspace(x0, x1, nx + 1)
+    zs = np.linspace(z0, z1, nz + 1)
+    X, Z = np.meshgrid(xs, zs, indexing="ij")
+    verts = np.stack([X.ravel(), np.full(X.size, y), Z.ravel()], 1)
+    i, j = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    a = (i * (nz + 1) + j).ravel()
+    b = a + (nz + 1)
+    c = a + 1
+    d = b + 1
+    faces = np.stack([np.stack([a, c, b], 1), np.stack([b, c, d], 1)], 1).reshape(-1, 3)
+    return verts, faces.astype(np.uint32)
+
+
+def spectral_stress(width=1280, height=720, spp=256, max_bounces=8, seed=0, sphere_level=6,
+                    torus_segments=(256, 192), leaf_count=2048, mask_size=64,
+                    dome_size=(1024, 512)) -> Workload:
+    """~200k triangles: a dispersive, absorbing, scattering glass sphere (g = 0.7),
+    two small glass spheres (g = -0.3 and 0), a subsurface torus (radius
+    (1, 0.2, 0.1)) and opacity-cutout leaves (seeded fp32 mask, 25% of texels
+    cut) on a plinth, under a lat-long dome and a rect light. Every dielectric
+    has transmission 1, dispersion scale 1, an Abbe number drawn from
+    U{20..60} and transmission depth 0.5; the leaves make the scene
+    non-opaque, so every ray takes the opacity any-hit path."""
+    rng = np.random.default_rng(seed)
+    s = Scene(revision=1)
+    mats = [Material(id="/plinth", base_color=[0.55, 0.52, 0.48], roughness=0.45, specular_weight=0.5)]
+    for name, g, color in (("/glass_forward", 0.7, [0.85, 0.6, 0.4]), ("/glass_back", -0.3, [0.5, 0.7, 0.9]),
+                           ("/glass_iso", 0.0, [0.7, 0.9, 0.6])):
+        m = Material(id=name, base_color=[1.0, 1.0, 1.0], transmission=1.0, transmission_color=color,
+                     transmission_depth=0.5, transmission_scatter=[0.6, 0.6, 0.6],
+                     transmission_scatter_anisotropy=g, transmission_dispersion_scale=1.0,
+                     transmission_dispersion_abbe_number=float(rng.integers(20, 61)), index_of_refraction=1.5,
+                     roughness=0.0, specular_weight=1.0)
+        m.roughness_v = 0.0
+        mats.append(m)
+    mats.append(Material(id="/subsurface", base_color=[0.9, 0.62, 0.5], subsurface=1.0,
+                         subsurface_color=[0.9, 0.62, 0.5], subsurface_radius=[1.0, 0.2, 0.1],
+                         subsurface_scale=0.25, roughness=0.35, specular_weight=0.5))
+    mats.append(Material(id="/leaf", base_color=[0.2, 0.55, 0.12], specular_weight=0.25, roughness=0.6,
+                         opacity_texture="leafmask#raw"))
+    s.materials = mats
+
+    # Plinth: subdivided top (64 x 48) and four sides.
+    tv, tf = _grid_top(-4.0, 4.0, -3.0, 3.0, 0.0, 64, 48)
+    side_v, side_f = [], []
+    for quad in (((-4, -0.5, 3), (4, -0.5, 3), (4, 0, 3), (-4, 0, 3)),
+                 ((4, -0.5, -3), (-4, -0.5, -3), (-4, 0, -3), (4, 0, -3)),
+                 ((4, -0.5, 3), (4, -0.5, -3), (4, 0, -3), (4, 0, 3)),
+                 ((-4, -0.5, -3), (-4, -0.5, 3), (-4, 0, 3), (-4, 0, -3))):
+        base = len(tv) + len(side_v)
+        side_v += [list(map(float, p)) for p in quad]
+        side_f += [[base, base + 1, base + 2], [base, base + 2, base + 3]]
+    pv = np.concatenate([tv, np.asarray(side_v)])
+    pf = np.concatenate([tf, np.asarray(side_f, np.uint32)])
+    s.meshes.append(Mesh(id="/plinth", positions=pv.astype(np.float32).ravel(), indices=pf.ravel(),
+                         material_id="/plinth"))
+
+    # Glass spheres.
+    sv, sf = _icosphere(sphere_level)
+    s.meshes.append(Mesh(id="/sphere", positions=(sv * 1.0 + np.array([-1.7, 1.0, 0.2])).astype(np.float32).ravel(),
+                         indices=sf.ravel(), material_id="/glass_forward"))
+    small_v, small_f = _icosphere(max(sphere_level - 2, 1))
+    for k, (mat, centre) in enumerate((("/glass_back", (0.2, 0.45, 1.6)), ("/glass_iso", (-0.4, 0.45, -1.7)))):
+        s.meshes.append(Mesh(id=f"/small{k}",
+                             positions=(small_v * 0.45 + np.array(centre)).astype(np.float32).ravel(),
+                             indices=small_f.ravel(), material_id=mat))
+
+    # Subsurface torus, tilted.
+    ov, of = _torus(1.0, 0.38, *torus_segments)
+    tilt = math.radians(25.0)
+    rot = np.array([[1, 0, 0], [0, math.cos(tilt), -math.sin(tilt)], [0, math.sin(tilt), math.cos(tilt)]])
+    ov = ov @ rot.T + np.array([1.7, 0.85, 0.0])
+    s.meshes.append(Mesh(id="/torus", positions=ov.astype(np.float32).ravel(), indices=of.ravel(),
+                         material_id="/subsurface"))
+
+    # Leaves: random quads in a bush behind the objects, UV 0..1 per quad.
+    lv, lf, luv = [], [], []
+    for k in range(leaf_count):
+        c = np.array([rng.uniform(-3.5, 3.5), rng.uniform(0.4, 3.2), rng.uniform(-2.9, -1.6)])
+        n = rng.normal(size=3)
+        n /= np.linalg.norm(n)
+        t = np.cross(n, [0.0, 1.0, 0.0] if abs(n[1]) < 0.9 else [1.0, 0.0, 0.0])
+        t /= np.linalg.norm(t)
+        b = np.cross(n, t)
+        size = rng.uniform(0.12, 0.3)
+        corners = [c - size * t - size * b, c + size * t - size * b, c + size * t + size * b, c - size * t + size * b]
+        base = 4 * k
+        lv += corners
+        lf += [[base, base + 1, base + 2], [base, base + 2, base + 3]]
+        luv += [0.0, 0.0, 1.0, 0.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1.0, 0.0, 1.0]
+    s.meshes.append(Mesh(id="/leaves", positions=np.asarray(lv, np.float32).ravel(),
+                         indices=np.asarray(lf, np.uint32).ravel(), texcoords=luv, material_id="/leaf"))
+    mask = (rng.random((mask_size, mask_size)) >= 0.25).astype(np.float32)
+    rgba = np.repeat(mask[..., None], 4, axis=2)
+    rgba[..., 3] = 1.0
+    s.textures.append(Texture(id="leafmask#raw", source_path="synthetic", width=mask_size, height=mask_size,
+                              srgb=False, rgba_float=rgba.ravel()))
+
+    dw, dh = dome_size
+    dome = _dome_texture(dw, dh, seed + 11) * 0.25
+    s.textures.append(Texture(id="stressdome#hdr", width=dw, height=dh, rgba_float=dome.ravel()))
+    s.lights.append(Light(id="/dome", type=DOME, intensity=1.0, texture="stressdome#hdr", texture_format=LATLONG))
+    s.lights.append(Light(id="/key", type=RECT, color=[1.0, 0.9, 0.8], intensity=12.0, normalize=False,
+                          position=[0.0, 5.0, 2.0], basis_x=[1.0, 0.0, 0.0], basis_y=[0.0, 0.0, 1.0],
+                          basis_z=[0.0, 1.0, 0.0], axis_u=[1.0, 0.0, 0.0], axis_v=[0.0, 0.0, 1.0],
+                          width=2.0, height=2.0, area=4.0))
+    cam = look_at_camera((0.0, 3.0, 7.8), (0.0, 0.9, 0.0), (0.0, 1.0, 0.0), 40.0, width / height)
+    return Workload("spectral-stress-200k-tri", s, cam, width, height, spp, max_bounces)
+
+
 def triangle_count(scene: Scene) -> int:
     return sum(len(m.indices) // 3 for m in scene.meshes)

@@ -148,3 +148,31 @@ def test_wave_size_does_not_change_results(gpu):
     b = gpu.render(cam, W, H, 0, 8, 8).copy()
     gpu.set_wave_size(0)
     assert np.array_equal(a, b)
+
+
+def test_spectral_stress_parity(oracle_lib, gpu):
+    # 200k triangles, dispersive glass with Beer absorption and interior
+    # scattering, subsurface random walks and opacity-cutout leaves (the
+    # non-opaque any-hit path on every extension ray).
+    wl = workloads.spectral_stress(width=96, height=54, dome_size=(256, 128))
+    o = oracle_lib.OracleTracer()
+    o.set_scene(wl.scene)
+    gpu.set_scene(wl.scene)
+    # A first render, then a progressive one on top of it.
+    for sample_index, spp in ((0, 4), (4, 3)):
+        ref = o.render(wl.camera, wl.width, wl.height, sample_index, wl.max_bounces, spp)
+        img = gpu.render(wl.camera, wl.width, wl.height, sample_index, wl.max_bounces, spp)
+        frac, rel = compare(img, ref)
+        assert frac >= MIN_IDENTICAL and rel <= MAX_REL_L1, f"{sample_index}: identical={frac:.4f} relL1={rel:.2e}"
+
+
+def test_primary_ids_spectral_stress(oracle_lib, gpu):
+    wl = workloads.spectral_stress(width=320, height=180, dome_size=(64, 32))
+    o = oracle_lib.OracleTracer()
+    o.set_scene(wl.scene)
+    gpu.set_scene(wl.scene)
+    for sample in (0, 5):
+        ref_p, ref_t = o.trace_primary(wl.camera, wl.width, wl.height, sample)
+        got_p, got_t = gpu.trace_primary(wl.camera, wl.width, wl.height, sample)
+        assert np.array_equal(got_p, ref_p)
+        assert np.array_equal(got_t.view(np.uint32), ref_t.view(np.uint32))
