@@ -50,9 +50,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hdcx", choices=["hdcx", "reference"])
-    ap.add_argument("--workload", default="heavy", choices=["heavy", "box", "stress"],
+    ap.add_argument("--workload", default="heavy", choices=["heavy", "box", "stress", "batch"],
                     help="heavy: 1.0M triangles, 1920x1080, 64 spp (the headline); box: 34-triangle closed box, "
-                         "256x256, 16 spp; stress: 200k-triangle spectral stress scene, 1280x720, 256 spp")
+                         "256x256, 16 spp; stress: 200k-triangle spectral stress scene, 1280x720, 256 spp; "
+                         "batch: --jobs scenes of 10k-2M triangles rendered by hdcx_render_batch")
+    ap.add_argument("--jobs", type=int, default=64, help="jobs of the batch workload")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -224,7 +226,11 @@ def workload_config(wl, world):
 def run_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return  # rank 0 alone times the CPU reference
-    wl = make_workload(args.workload)
+    if args.workload == "batch":
+        from hdcodex_b200 import workloads
+        wl = workloads.batch_job(0)
+    else:
+        wl = make_workload(args.workload)
     import oracle as O
     if O.ref_available():
         t, kind = O.ReferenceTracer(), "reference"
@@ -257,6 +263,87 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def run_batch(args):
+    """The multi-job workload: every step renders all jobs (each job's own
+    resolution and spp) through hdcx_render_batch, with the images read back to
+    pinned host memory; the serial loop of hdcx_render calls over the same
+    jobs is timed beside it. Under torchrun the jobs are dealt round-robin to
+    the ranks (total work fixed: strong scaling)."""
+    import torch
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    from hdcodex_b200 import PathTracer, render_batch, workloads
+
+    jobs = [wl for i, wl in enumerate(workloads.batch_jobs(args.jobs)) if i % world == rank]
+    tracers = []
+    for wl in jobs:
+        t = PathTracer(local)
+        t.set_scene(wl.scene)
+        tracers.append(t)
+    hosts = [torch.empty((wl.height, wl.width, 4), dtype=torch.float32, pin_memory=True) for wl in jobs]
+    paths = sum(wl.spectral_paths for wl in jobs)
+
+    def batch_step(step):
+        spec = [(t, wl.camera, wl.width, wl.height, step * wl.spp, wl.max_bounces, wl.spp, h.data_ptr())
+                for t, wl, h in zip(tracers, jobs, hosts)]
+        return render_batch(spec)
+
+    def serial_step(step):
+        for t, wl, h in zip(tracers, jobs, hosts):
+            t.render(wl.camera, wl.width, wl.height, step * wl.spp, wl.max_bounces, wl.spp, out=h.data_ptr())
+
+    for i in range(args.warmup):
+        batch_step(i)
+    sampler = ClockSampler(local)
+    barrier_sync(world)
+    sampler.start()
+    t0 = time.perf_counter()
+    per_job_ms = [0.0] * len(jobs)
+    for i in range(args.steps):
+        res = batch_step(args.warmup + i)
+        for k, r in enumerate(res):
+            per_job_ms[k] += r["render_ms"]
+    barrier_sync(world)
+    batch_s = max_over_ranks(time.perf_counter() - t0, world)
+    clocks = sampler.stop()
+    barrier_sync(world)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        serial_step(args.warmup + args.steps + i)
+    barrier_sync(world)
+    serial_s = max_over_ranks(time.perf_counter() - t0, world)
+    total_paths = float(paths)
+    if world > 1:
+        import torch.distributed as dist
+        tp = torch.tensor([float(paths)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tp)
+        total_paths = float(tp.item())
+    if rank == 0:
+        value = total_paths * args.steps / batch_s
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * batch_s / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batch-{args.jobs}-jobs", "jobs": args.jobs,
+                       "spectral_paths_per_step": total_paths,
+                       "triangles": sum(workloads.triangle_count(wl.scene) for wl in jobs) if world == 1 else None,
+                       "l2": "inputs larger than L2", "parallelism": f"jobs dealt round-robin to {world} GPU(s)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 48 * len(jobs),
+                    "d2h_bytes_per_step": sum(wl.width * wl.height * 16 for wl in jobs)},
+            "serial_loop": {"value": total_paths * args.steps / serial_s, "unit": UNIT,
+                            "ms_per_step": 1000.0 * serial_s / args.steps},
+            "batch_over_serial": serial_s / batch_s,
+            "per_job_device_ms_rank0": [round(ms / args.steps, 2) for ms in per_job_ms],
+            "clocks": clocks,
+        }), flush=True)
+    for t in tracers:
+        t.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def run_hdcx(args):
@@ -393,6 +480,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_hdcx(args)
 

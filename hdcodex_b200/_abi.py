@@ -227,9 +227,26 @@ class RenderStats(C.Structure):
     ]
 
 
+class BatchJob(C.Structure):
+    """hdcx_batch_job: one job of hdcx_render_batch."""
+    _fields_ = [
+        ("tracer", C.c_void_p),
+        ("camera", Camera),
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("sample_index", C.c_uint32),
+        ("max_bounces", C.c_uint32),
+        ("sample_count", C.c_uint32),
+        ("rgba_out", C.c_void_p),
+        ("written", C.c_int32),
+        ("status", C.c_int32),
+        ("render_ms", C.c_double),
+    ]
+
+
 STRUCTS_IN_ABI_ORDER = [
     Camera, MeshDesc, MaterialDesc, TextureDesc, LightDesc, SceneDesc, PackedTexture, PackedScene,
-    RenderStats,
+    RenderStats, BatchJob,
 ]
 
 GPU_MATERIAL_BYTES = 368

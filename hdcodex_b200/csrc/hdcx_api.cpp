@@ -276,10 +276,15 @@ void ensureOutput(hdcx_tracer* t, uint32_t w, uint32_t h)
     t->xyzSamples = 0;
 }
 
-void ensurePaths(hdcx_tracer* t, uint64_t needed, uint32_t shadowPerPath)
+constexpr uint64_t kAutomaticWavePaths = 12ull << 20;  // ~12.6M paths per wave
+// Device bytes of path state per path (PathBuffers with three shadow slots).
+constexpr uint64_t kPathStateBytes = 131 + 3 * 56;
+
+// `capOverride` (0 = none) bounds the wave when the tracer has no wave size
+// of its own; hdcx_render_batch uses it to share device memory among jobs.
+void ensurePaths(hdcx_tracer* t, uint64_t needed, uint32_t shadowPerPath, uint64_t capOverride = 0)
 {
-    const uint64_t automatic = 12ull << 20;  // ~12.6M paths per wave
-    const uint64_t cap = t->wavePaths ? t->wavePaths : automatic;
+    const uint64_t cap = t->wavePaths ? t->wavePaths : (capOverride ? capOverride : kAutomaticWavePaths);
     const uint64_t capacity = std::max<uint64_t>(3, std::min(needed, cap));
     if (t->paths.capacity >= capacity && t->paths.shadowPerPath >= shadowPerPath) return;
     check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
@@ -340,7 +345,8 @@ HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity)
 {
     const uint64_t all[] = {sizeof(hdcx_camera),         sizeof(hdcx_mesh_desc),  sizeof(hdcx_material_desc),
                             sizeof(hdcx_texture_desc),   sizeof(hdcx_light_desc), sizeof(hdcx_scene_desc),
-                            sizeof(hdcx_packed_texture), sizeof(hdcx_packed_scene), sizeof(hdcx_render_stats)};
+                            sizeof(hdcx_packed_texture), sizeof(hdcx_packed_scene), sizeof(hdcx_render_stats),
+                            sizeof(hdcx_batch_job)};
     const uint32_t n = static_cast<uint32_t>(sizeof(all) / sizeof(all[0]));
     for (uint32_t i = 0; i < std::min(n, capacity); ++i) sizes[i] = all[i];
     return n;
@@ -539,6 +545,90 @@ HDCX_API hdcx_status hdcx_set_wave_size(hdcx_tracer* t, uint64_t paths)
     return HDCX_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// One render in three phases. prepare: output and path buffers, the fallback
+// axis, counters cleared (may allocate and synchronise the tracer's stream).
+// enqueue: the kernels and the optional read-back, asynchronous on the
+// tracer's stream. finish: wait for the stream, fill the counters.
+// hdcx_render runs the phases back to back; hdcx_render_batch runs every
+// job's prepare, then every enqueue, then every finish, so that the jobs'
+// kernels overlap on the GPU.
+struct RenderCall {
+    FrameConst frame{};
+    uint64_t pathsNeeded = 0;
+    StageTimes times;
+    uint64_t launches = 0;
+    bool stageTiming = false;
+    bool counting = false;
+    bool active = false;
+};
+
+void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, uint32_t height, uint32_t sampleIndex,
+                   uint32_t maxBounces, uint32_t sampleCount, uint64_t waveCap, bool allowStageTiming,
+                   RenderCall& call)
+{
+    ensureOutput(t, width, height);
+    if (!t->fallbackAxisInitialized) {
+        t->fallbackZUp = std::fabs(camera.vertical[2]) > std::fabs(camera.vertical[1]);
+        t->fallbackAxisInitialized = true;
+    }
+    call.frame = makeFrame(t, camera, width, height, sampleIndex, maxBounces, sampleCount);
+    call.pathsNeeded = uint64_t(width) * height * 3u * call.frame.sampleCount;
+    const uint32_t shadowPerPath = t->scene.lightCount > 0u ? (t->scene.hasMeshLights ? 2u : 1u)
+                                                            : (t->scene.hasMeshLights ? 2u : 3u);
+    ensurePaths(t, call.pathsNeeded, std::max(shadowPerPath, 3u), waveCap);
+    check(cudaMemsetAsync(t->paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
+    call.stageTiming = allowStageTiming && (t->profiling & HDCX_PROFILE_STAGE_TIMES) != 0u;
+    call.counting = (t->profiling & HDCX_PROFILE_COUNT_TRAVERSAL) != 0u;
+    call.active = true;
+}
+
+void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut)
+{
+    check(cudaEventRecord(t->start, t->stream), "cudaEventRecord");
+    renderFrame(t->scene, call.frame, t->paths, t->fb, t->stream, call.stageTiming ? &call.times : nullptr,
+                call.counting, &call.launches);
+    check(cudaEventRecord(t->stop, t->stream), "cudaEventRecord");
+    if (rgbaOut) {
+        check(cudaMemcpyAsync(rgbaOut, t->fb.rgba, size_t(call.frame.width) * call.frame.height * sizeof(float4),
+                              cudaMemcpyDeviceToHost, t->stream),
+              "read back");
+    }
+}
+
+void finishRender(hdcx_tracer* t, RenderCall& call)
+{
+    check(cudaStreamSynchronize(t->stream), "render");
+    t->xyzSamples = (call.frame.sampleIndex == 0 ? 0 : t->xyzSamples) + call.frame.sampleCount;
+    unsigned long long counters[8];
+    check(cudaMemcpy(counters, t->paths.stats, sizeof counters, cudaMemcpyDeviceToHost), "read stats");
+    float ms = 0.0F;
+    check(cudaEventElapsedTime(&ms, t->start, t->stop), "cudaEventElapsedTime");
+    t->stats = hdcx_render_stats{};
+    t->stats.spectral_paths = call.pathsNeeded;
+    t->stats.extension_rays = counters[0];
+    t->stats.shadow_rays = counters[1];
+    t->stats.subsurface_rays = counters[2];
+    t->stats.render_ms = ms;
+    t->stats.extend_ms = call.times.extendMs;
+    t->stats.shade_ms = call.times.shadeMs;
+    t->stats.shadow_ms = call.times.shadowMs;
+    t->stats.waves = call.times.waves;
+    t->stats.extend_launches = call.times.extendLaunches;
+    t->stats.kernel_launches = call.launches;
+    t->stats.extension_node_visits = counters[3];
+    t->stats.extension_triangle_tests = counters[4];
+    t->stats.shadow_node_visits = counters[5];
+    t->stats.shadow_triangle_tests = counters[6];
+}
+
+}  // namespace
+
+extern "C" {
+
 HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint32_t width, uint32_t height,
                                  uint32_t sampleIndex, uint32_t maxBounces, uint32_t sampleCount, float* rgbaOut,
                                  int32_t* written)
@@ -548,52 +638,103 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint
     if (!t->geometryReady || width == 0 || height == 0) return HDCX_OK;
     if (uint64_t(width) * height > (1ull << 28)) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels");
     return guarded(t, [&] {
-        ensureOutput(t, width, height);
-        if (!t->fallbackAxisInitialized) {
-            t->fallbackZUp = std::fabs(camera->vertical[2]) > std::fabs(camera->vertical[1]);
-            t->fallbackAxisInitialized = true;
-        }
-        const FrameConst f = makeFrame(t, *camera, width, height, sampleIndex, maxBounces, sampleCount);
-        const uint64_t pathsNeeded = uint64_t(width) * height * 3u * f.sampleCount;
-        const uint32_t shadowPerPath = t->scene.lightCount > 0u ? (t->scene.hasMeshLights ? 2u : 1u)
-                                                                : (t->scene.hasMeshLights ? 2u : 3u);
-        ensurePaths(t, pathsNeeded, std::max(shadowPerPath, 3u));
-        check(cudaMemsetAsync(t->paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
-        StageTimes times;
-        const bool stageTiming = (t->profiling & HDCX_PROFILE_STAGE_TIMES) != 0u;
-        const bool counting = (t->profiling & HDCX_PROFILE_COUNT_TRAVERSAL) != 0u;
-        uint64_t launches = 0;
-        check(cudaEventRecord(t->start, t->stream), "cudaEventRecord");
-        renderFrame(t->scene, f, t->paths, t->fb, t->stream, stageTiming ? &times : nullptr, counting, &launches);
-        check(cudaEventRecord(t->stop, t->stream), "cudaEventRecord");
-        if (rgbaOut) {
-            check(cudaMemcpyAsync(rgbaOut, t->fb.rgba, size_t(width) * height * sizeof(float4), cudaMemcpyDeviceToHost, t->stream),
-                  "read back");
-        }
-        check(cudaStreamSynchronize(t->stream), "render");
-        t->xyzSamples = (sampleIndex == 0 ? 0 : t->xyzSamples) + f.sampleCount;
-        unsigned long long counters[8];
-        check(cudaMemcpy(counters, t->paths.stats, sizeof counters, cudaMemcpyDeviceToHost), "read stats");
-        float ms = 0.0F;
-        check(cudaEventElapsedTime(&ms, t->start, t->stop), "cudaEventElapsedTime");
-        t->stats = hdcx_render_stats{};
-        t->stats.spectral_paths = pathsNeeded;
-        t->stats.extension_rays = counters[0];
-        t->stats.shadow_rays = counters[1];
-        t->stats.subsurface_rays = counters[2];
-        t->stats.render_ms = ms;
-        t->stats.extend_ms = times.extendMs;
-        t->stats.shade_ms = times.shadeMs;
-        t->stats.shadow_ms = times.shadowMs;
-        t->stats.waves = times.waves;
-        t->stats.extend_launches = times.extendLaunches;
-        t->stats.kernel_launches = launches;
-        t->stats.extension_node_visits = counters[3];
-        t->stats.extension_triangle_tests = counters[4];
-        t->stats.shadow_node_visits = counters[5];
-        t->stats.shadow_triangle_tests = counters[6];
+        RenderCall call;
+        prepareRender(t, *camera, width, height, sampleIndex, maxBounces, sampleCount, 0, true, call);
+        enqueueRender(t, call, rgbaOut);
+        finishRender(t, call);
         if (written) *written = 1;
     });
+}
+
+HDCX_API hdcx_status hdcx_render_batch(hdcx_batch_job* jobs, uint32_t count, uint64_t pathBudget)
+{
+    if (count == 0) return HDCX_OK;
+    if (!jobs) return HDCX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t j = 0; j < count; ++j) {
+        jobs[j].status = HDCX_OK;
+        jobs[j].written = 0;
+        jobs[j].render_ms = 0.0;
+        if (!jobs[j].tracer) return HDCX_ERROR_INVALID_ARGUMENT;
+        for (uint32_t k = 0; k < j; ++k) {
+            if (jobs[k].tracer == jobs[j].tracer) {
+                return fail(jobs[j].tracer, HDCX_ERROR_INVALID_ARGUMENT,
+                            "hdcx_render_batch: a tracer appears in more than one job of the batch");
+            }
+        }
+    }
+    std::vector<RenderCall> calls(count);
+    // Wave sizes: every job gets min(its paths, the automatic wave) unless the
+    // jobs on one device would then hold more path state than the budget
+    // (default: half of the device's free memory), in which case the waves
+    // shrink in proportion (never below 1M paths).
+    std::vector<uint64_t> caps(count, 0);
+    {
+        std::vector<int> devices;
+        for (uint32_t j = 0; j < count; ++j) {
+            if (std::find(devices.begin(), devices.end(), jobs[j].tracer->device) == devices.end())
+                devices.push_back(jobs[j].tracer->device);
+        }
+        for (int device : devices) {
+            uint64_t budget = pathBudget;
+            if (budget == 0) {
+                size_t freeBytes = 0, totalBytes = 0;
+                if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&freeBytes, &totalBytes) != cudaSuccess)
+                    freeBytes = 0;
+                budget = freeBytes / 2 / kPathStateBytes;
+            }
+            uint64_t wanted = 0;
+            for (uint32_t j = 0; j < count; ++j) {
+                if (jobs[j].tracer->device != device) continue;
+                const hdcx_batch_job& b = jobs[j];
+                const uint64_t need = uint64_t(b.width) * b.height * 3u * std::max(b.sample_count, 1u);
+                caps[j] = std::max<uint64_t>(3, std::min(need, kAutomaticWavePaths));
+                wanted += caps[j];
+            }
+            if (budget > 0 && wanted > budget) {
+                for (uint32_t j = 0; j < count; ++j) {
+                    if (jobs[j].tracer->device != device) continue;
+                    const double share = static_cast<double>(caps[j]) / static_cast<double>(wanted);
+                    caps[j] = std::max<uint64_t>(std::min<uint64_t>(caps[j], 1ull << 20),
+                                                 static_cast<uint64_t>(share * static_cast<double>(budget)));
+                }
+            }
+        }
+    }
+    auto record = [&](uint32_t j, hdcx_status status) {
+        if (status != HDCX_OK) {
+            jobs[j].status = status;
+            calls[j].active = false;
+        }
+    };
+    for (uint32_t j = 0; j < count; ++j) {
+        hdcx_batch_job& b = jobs[j];
+        hdcx_tracer* t = b.tracer;
+        if (!t->geometryReady || b.width == 0 || b.height == 0) continue;
+        if (uint64_t(b.width) * b.height > (1ull << 28)) {
+            record(j, fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels"));
+            continue;
+        }
+        record(j, guarded(t, [&] {
+            prepareRender(t, b.camera, b.width, b.height, b.sample_index, b.max_bounces, b.sample_count, caps[j], false,
+                          calls[j]);
+        }));
+    }
+    for (uint32_t j = 0; j < count; ++j) {
+        if (!calls[j].active) continue;
+        record(j, guarded(jobs[j].tracer, [&] { enqueueRender(jobs[j].tracer, calls[j], jobs[j].rgba_out); }));
+    }
+    hdcx_status overall = HDCX_OK;
+    for (uint32_t j = 0; j < count; ++j) {
+        if (calls[j].active) {
+            record(j, guarded(jobs[j].tracer, [&] {
+                finishRender(jobs[j].tracer, calls[j]);
+                jobs[j].written = 1;
+                jobs[j].render_ms = jobs[j].tracer->stats.render_ms;
+            }));
+        }
+        if (overall == HDCX_OK && jobs[j].status != HDCX_OK) overall = jobs[j].status;
+    }
+    return overall;
 }
 
 HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* t, const hdcx_camera* camera, uint32_t width, uint32_t height,

@@ -57,6 +57,7 @@ SIGNATURES = {
                               C.c_uint32, _P, C.POINTER(C.c_int32)]),
     "hdcx_render_static": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                      C.c_uint32, _P, C.POINTER(C.c_int32)]),
+    "hdcx_render_batch": (C.c_int, [C.POINTER(_abi.BatchJob), C.c_uint32, C.c_uint64]),
     "hdcx_read_rgba": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint64]),
     "hdcx_read_xyz": (C.c_int, [_P, C.POINTER(C.c_double), C.c_uint64, C.POINTER(C.c_uint64)]),
     "hdcx_device_rgba": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
@@ -198,6 +199,39 @@ class PathTracer:
         st = _abi.RenderStats()
         self._check(lib().hdcx_get_stats(self._h, C.byref(st)), "get_stats")
         return {name: getattr(st, name) for name, _ in _abi.RenderStats._fields_}
+
+
+def render_batch(jobs, path_budget: int = 0):
+    """hdcx_render_batch over `jobs`: (tracer, camera, width, height,
+    sample_index, max_bounces, sample_count, out) tuples, `out` a float32
+    (height, width, 4) array, a device pointer (int) or None. Returns the list
+    of hdcx_batch_job results (status, written, render_ms per job); raises if
+    any job failed."""
+    arr = (_abi.BatchJob * len(jobs))()
+    keep = []
+    for i, (tracer, camera, width, height, sample_index, max_bounces, sample_count, out) in enumerate(jobs):
+        b = arr[i]
+        b.tracer = tracer.handle
+        b.camera = camera
+        b.width, b.height = width, height
+        b.sample_index, b.max_bounces, b.sample_count = sample_index, max_bounces, sample_count
+        if isinstance(out, np.ndarray):
+            assert out.dtype == np.float32 and out.size >= width * height * 4 and out.flags.c_contiguous
+            keep.append(out)
+            b.rgba_out = out.ctypes.data
+        else:
+            b.rgba_out = out
+    status = lib().hdcx_render_batch(arr, len(jobs), path_budget)
+    if status != 0:
+        failed = [(i, arr[i].status) for i in range(len(jobs)) if arr[i].status != 0]
+        i, st = failed[0]
+        msg = lib().hdcx_last_error(jobs[i][0].handle) or b""
+        raise RuntimeError(f"render_batch failed: job {i}: {STATUS.get(st, st)}: {msg.decode()}")
+    for i, job in enumerate(jobs):
+        if arr[i].written:
+            job[0].width, job[0].height = job[2], job[3]
+    return [{"status": arr[i].status, "written": arr[i].written, "render_ms": arr[i].render_ms}
+            for i in range(len(jobs))]
 
 
 def pack_scene(scene: Scene) -> dict:

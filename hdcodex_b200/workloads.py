@@ -379,5 +379,96 @@ def spectral_stress(width=1280, height=720, spp=256, max_bounces=8, seed=0, sphe
     return Workload("spectral-stress-200k-tri", s, cam, width, height, spp, max_bounces)
 
 
+BATCH_RESOLUTIONS = ((256, 256), (512, 512), (1280, 720), (1920, 1080))
+
+
+def _c2_palette(rng, prefix=""):
+    """The heavy-geometry material families: Lambert, GGX dielectric over
+    diffuse, GGX conductor."""
+    mats = []
+    for i in range(4):
+        mats.append(Material(id=f"{prefix}/lambert{i}", base_color=rng.uniform(0.1, 0.9, 3).tolist(),
+                             specular_weight=0.0))
+    for i in range(4):
+        m = Material(id=f"{prefix}/dielectric{i}", base_color=rng.uniform(0.05, 0.8, 3).tolist(),
+                     roughness=float(rng.uniform(0.05, 0.8)), index_of_refraction=1.5, specular_weight=1.0)
+        m.roughness_v = m.roughness
+        mats.append(m)
+    for i in range(4):
+        m = Material(id=f"{prefix}/conductor{i}", base_color=rng.uniform(0.5, 1.0, 3).tolist(), metalness=1.0,
+                     roughness=float(rng.uniform(0.05, 0.6)))
+        m.roughness_v = m.roughness
+        mats.append(m)
+    return mats
+
+
+def batch_job(index: int, seed: int = 0, dome_size=(1024, 512)) -> Workload:
+    """Job `index` of the multi-job batch: triangles log-uniform in [10k, 2M]
+    (a heightfield carrying ~70% of them plus displaced level-3 icospheres),
+    resolution drawn from BATCH_RESOLUTIONS, spp uniform in {4..128},
+    per-triangle materials of the heavy-geometry families, one lat-long dome
+    and 1-8 rect/disk/sphere lights. A pure function of (index, seed)."""
+    from .scene import DISK, SPHERE
+    rng = np.random.default_rng([seed, index])
+    target = int(round(math.exp(rng.uniform(math.log(10_000), math.log(2_000_000)))))
+    width, height = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
+    spp = int(rng.integers(4, 129))
+    s = Scene(revision=1)
+    s.materials = _c2_palette(rng)
+    ids = [m.id for m in s.materials]
+    n = max(8, int(round(math.sqrt(0.7 * target / 2.0))) + 1)
+    half = 10.0
+    xs = np.linspace(-half, half, n)
+    X, Z = np.meshgrid(xs, xs)
+    pts = np.stack([X.ravel(), np.zeros(n * n), Z.ravel()], axis=1)
+    pts[:, 1] = 0.6 * _noise3(pts * 0.35, rng, 4)
+    ii, jj = np.meshgrid(np.arange(n - 1), np.arange(n - 1), indexing="ij")
+    a = (ii * n + jj).ravel()
+    tris = np.stack([np.stack([a, a + n, a + 1], 1), np.stack([a + 1, a + n, a + n + 1], 1)], 1)
+    tris = tris.reshape(-1, 3).astype(np.uint32)
+    pick = rng.integers(0, len(ids), size=len(tris))
+    s.meshes.append(Mesh(id="/ground", positions=pts.astype(np.float32).ravel(), indices=tris.ravel(),
+                         material_id=ids[0], triangle_material_ids=[ids[k] for k in pick]))
+    spheres = max(0, int(round((target - len(tris)) / 1280.0)))
+    if spheres:
+        base_v, base_f = _icosphere(3)
+        all_v, all_f = [], []
+        for k in range(spheres):
+            r = rng.uniform(0.2, 0.5)
+            c = np.array([rng.uniform(-half + 1, half - 1), 1.0 + r, rng.uniform(-half + 1, half - 1)])
+            disp = 1.0 + 0.15 * np.sin(base_v @ rng.normal(size=(3,)) * 3.0 + rng.uniform(0, 6.28))
+            all_v.append(base_v * (r * disp)[:, None] + c)
+            all_f.append(base_f + k * len(base_v))
+        sf = np.concatenate(all_f).astype(np.uint32)
+        pick = rng.integers(0, len(ids), size=len(sf))
+        s.meshes.append(Mesh(id="/spheres", positions=np.concatenate(all_v).astype(np.float32).ravel(),
+                             indices=sf.ravel(), material_id=ids[0], triangle_material_ids=[ids[k] for k in pick]))
+    dw, dh = dome_size
+    s.textures.append(Texture(id="dome#hdr", width=dw, height=dh, rgba_float=_dome_texture(dw, dh, seed + 1000 + index).ravel()))
+    s.lights.append(Light(id="/dome", type=DOME, intensity=1.0, texture="dome#hdr", texture_format=LATLONG))
+    for k in range(int(rng.integers(1, 9))):
+        kind = (RECT, DISK, SPHERE)[int(rng.integers(0, 3))]
+        pos = [float(rng.uniform(-6, 6)), float(rng.uniform(3, 7)), float(rng.uniform(-6, 6))]
+        color = rng.uniform(0.6, 1.0, 3).tolist()
+        size = float(rng.uniform(0.3, 1.2))
+        if kind == SPHERE:
+            light = Light(id=f"/light{k}", type=SPHERE, color=color, intensity=float(rng.uniform(5, 30)),
+                          position=pos, radius=size * 0.5)
+        else:
+            light = Light(id=f"/light{k}", type=kind, color=color, intensity=float(rng.uniform(5, 30)),
+                          position=pos, basis_x=[1.0, 0.0, 0.0], basis_y=[0.0, 0.0, 1.0], basis_z=[0.0, 1.0, 0.0],
+                          axis_u=[size, 0.0, 0.0], axis_v=[0.0, 0.0, size], width=size, height=size,
+                          radius=size * 0.5, area=size * size if kind == RECT else math.pi * (size * 0.5) ** 2)
+        s.lights.append(light)
+    eye = (float(rng.uniform(-4, 4)), float(rng.uniform(5, 8)), float(rng.uniform(12, 16)))
+    cam = look_at_camera(eye, (0.0, 0.5, 0.0), (0.0, 1.0, 0.0), 45.0, width / height)
+    return Workload(f"batch-job-{index}", s, cam, width, height, spp, 8)
+
+
+def batch_jobs(count: int = 64, seed: int = 0, **kw):
+    """The multi-job batch: `count` jobs of batch_job."""
+    return [batch_job(i, seed, **kw) for i in range(count)]
+
+
 def triangle_count(scene: Scene) -> int:
     return sum(len(m.indices) // 3 for m in scene.meshes)

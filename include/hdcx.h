@@ -307,6 +307,22 @@ typedef struct hdcx_render_stats {
     uint64_t shadow_triangle_tests;  /* triangle tests of shadow rays (counting mode) */
 } hdcx_render_stats;
 
+/* One job of hdcx_render_batch: the arguments of one hdcx_render call and
+ * the job's results. */
+typedef struct hdcx_batch_job {
+    hdcx_tracer* tracer;     /* the job renders this tracer's scene */
+    hdcx_camera camera;
+    uint32_t width;
+    uint32_t height;
+    uint32_t sample_index;
+    uint32_t max_bounces;
+    uint32_t sample_count;
+    float* rgba_out;         /* width*height*4 floats (host or device), or NULL */
+    int32_t written;         /* out: as hdcx_render's *written */
+    hdcx_status status;      /* out: this job's status (hdcx_last_error(tracer) has the message) */
+    double render_ms;        /* out: device time of the job on its tracer's stream */
+} hdcx_batch_job;
+
 /* Profiling switches for hdcx_set_profiling. */
 #define HDCX_PROFILE_STAGE_TIMES 1u      /* CUDA events around every extend/shade/shadow launch */
 #define HDCX_PROFILE_COUNT_TRAVERSAL 2u  /* traversal kernels count node visits and triangle tests */
@@ -319,8 +335,8 @@ typedef struct hdcx_render_stats {
 HDCX_API uint32_t hdcx_abi_version(void);
 
 /* Byte size of each ABI struct, indexed 0..7: camera, mesh, material, texture,
- * light, scene, packed_texture, packed_scene; 8: render_stats. Lets bindings
- * check their struct mirrors. Returns the number of entries written. */
+ * light, scene, packed_texture, packed_scene; 8: render_stats; 9: batch_job.
+ * Lets bindings check their struct mirrors. Returns the number of entries. */
 HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity);
 
 /* Fills the reference defaults of SceneMaterial / SceneLight / SceneMesh
@@ -424,6 +440,23 @@ HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* tracer, const hdcx_camera* 
                                         uint32_t sample_index, uint32_t max_bounces,
                                         uint32_t sample_count, float* rgba_device,
                                         int32_t* written);
+
+/* Renders several jobs, each exactly as hdcx_render would (same images, same
+ * running means, same counters), with their kernels overlapping on the GPU:
+ * every job runs on its own tracer's stream, all jobs are launched before any
+ * is waited for. No counterpart in the reference, whose caller renders one
+ * delegate at a time; it replaces a serial loop of Render calls over many
+ * scenes (a farm of small shots, turntables, look-development variants).
+ * Each tracer appears in at most one job (HDCX_ERROR_INVALID_ARGUMENT
+ * otherwise). Tracers may live on different devices. Per-stage times are not
+ * recorded for batched jobs. Path state: every job gets waves of
+ * min(its paths, the automatic wave) unless the jobs on a device would then
+ * hold more than `path_budget` paths of path state (0: half of the device's
+ * free memory at the call), in which case the waves shrink in proportion
+ * (never below 1,048,576 paths); a wave size set with hdcx_set_wave_size
+ * wins. Returns HDCX_OK when every job succeeded, else the first failing
+ * job's status; each job's own status is in its `status`. */
+HDCX_API hdcx_status hdcx_render_batch(hdcx_batch_job* jobs, uint32_t count, uint64_t path_budget);
 
 /* Copies the current device RGBA32F accumulation (width*height*4 floats). */
 HDCX_API hdcx_status hdcx_read_rgba(hdcx_tracer* tracer, float* rgba_out, uint64_t float_count);
