@@ -86,6 +86,12 @@ struct TexDesc {
     uint32_t height;
     uint32_t format;  // 0 RGBA8 UNORM, 1 RGBA8 sRGB, 2 RGBA32F
     uint32_t reserved;
+    // Dome importance textures only (else null): the CDFs as compact floats
+    // with every 32nd value repeated in skip arrays, in this order:
+    //   marginal[h] (texel (0, row).y), marginalSkip[ceil(h/32)],
+    //   conditional[h * w] (texel (col, row).x), conditionalSkip[h * ceil(w/32)],
+    // where skip[k] = values[min(32k + 31, n - 1)].
+    const float* cdf;
 };
 
 // 8-wide BVH node with quantised child boxes (80 bytes). The layout is the

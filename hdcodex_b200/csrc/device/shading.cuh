@@ -683,6 +683,30 @@ HDCX_D float domeLightPdf(const DeviceScene& s, const GpuLight& light, float3 wo
     return gmax(texelFetch(t, tx, ty).z, 0.0f);
 }
 
+// min(first i with target <= values[i], n - 1): the index the reference's
+// binary search returns (:600-650), found through the skip array first (one
+// 128-byte line per 32 values) and then inside one 32-value segment. Equal to
+// the plain binary search when the values are non-decreasing, which the host
+// checks before it builds the arrays.
+HDCX_D int cdfSearch(const float* values, const float* skip, int n, float target)
+{
+    int low = 0;
+    int high = (n + 31) / 32 - 1;
+    while (low < high) {
+        const int middle = (low + high) / 2;
+        if (target <= __ldg(skip + middle)) high = middle;
+        else low = middle + 1;
+    }
+    high = min(low * 32 + 31, n - 1);
+    low = low * 32;
+    while (low < high) {
+        const int middle = (low + high) / 2;
+        if (target <= __ldg(values + middle)) high = middle;
+        else low = middle + 1;
+    }
+    return low;
+}
+
 HDCX_D void sampleDomeLight(const DeviceScene& s, const GpuLight& light, uint32_t& rng, float3& worldDirection, float& pdf)
 {
     // :600-650
@@ -696,26 +720,40 @@ HDCX_D void sampleDomeLight(const DeviceScene& s, const GpuLight& light, uint32_
     const int w = static_cast<int>(t.width), h = static_cast<int>(t.height);
     const float4* texels = reinterpret_cast<const float4*>(t.texels);
     const float rowTarget = randomFloat(rng);
-    int low = 0;
-    int high = h - 1;
-    while (low < high) {
-        const int middle = (low + high) / 2;
-        const float cdf = __ldg(&texels[static_cast<size_t>(middle) * t.width].y);
-        if (rowTarget <= cdf) high = middle;
-        else low = middle + 1;
+    int row, column;
+    if (t.cdf) {
+        const float* marginal = t.cdf;
+        const float* marginalSkip = marginal + h;
+        const float* conditional = marginalSkip + (h + 31) / 32;
+        const int ws = (w + 31) / 32;
+        const float* conditionalSkip = conditional + static_cast<size_t>(h) * w;
+        row = cdfSearch(marginal, marginalSkip, h, rowTarget);
+        const float columnTarget = randomFloat(rng);
+        column = cdfSearch(conditional + static_cast<size_t>(row) * w, conditionalSkip + static_cast<size_t>(row) * ws, w,
+                           columnTarget);
+    } else {
+        int low = 0;
+        int high = h - 1;
+        while (low < high) {
+            const int middle = (low + high) / 2;
+            const float cdf = __ldg(&texels[static_cast<size_t>(middle) * t.width].y);
+            if (rowTarget <= cdf) high = middle;
+            else low = middle + 1;
+        }
+        row = low;
+        const float columnTarget = randomFloat(rng);
+        low = 0;
+        high = w - 1;
+        const float4* rowTexels = texels + static_cast<size_t>(row) * t.width;
+        while (low < high) {
+            const int middle = (low + high) / 2;
+            const float cdf = __ldg(&rowTexels[middle].x);
+            if (columnTarget <= cdf) high = middle;
+            else low = middle + 1;
+        }
+        column = low;
     }
-    const int row = low;
-    const float columnTarget = randomFloat(rng);
-    low = 0;
-    high = w - 1;
     const float4* rowTexels = texels + static_cast<size_t>(row) * t.width;
-    while (low < high) {
-        const int middle = (low + high) / 2;
-        const float cdf = __ldg(&rowTexels[middle].x);
-        if (columnTarget <= cdf) high = middle;
-        else low = middle + 1;
-    }
-    const int column = low;
     const float v0 = static_cast<float>(row) / static_cast<float>(h);
     const float v1 = static_cast<float>(row + 1) / static_cast<float>(h);
     const float cosine0 = gcos(kPi * (1.0f - v0));

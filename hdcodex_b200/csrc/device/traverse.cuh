@@ -110,7 +110,152 @@ HDCX_D bool intersectTriangle(const RayPre& r, float3 v0, float3 v1, float3 v2, 
     return true;
 }
 
-HDCX_D float byteToFloat(uint32_t word, int index) { return __uint2float_rn((word >> (8 * index)) & 0xffu); }
+// Byte `index` of `word` as a float: the byte is placed in the low mantissa
+// bits of 2^23 (bit pattern 0x4B0000bb) and 2^23 is subtracted, which is exact.
+// A byte permute and an add run on full-rate pipes, where an integer-to-float
+// conversion would queue on the quarter-rate conversion pipe (eight children
+// x six planes per node).
+HDCX_D float byteToFloat(uint32_t word, int index)
+{
+    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u + static_cast<uint32_t>(index))) - 8388608.0f;
+}
+
+// State of one ray's traversal: the ray, the closest confirmed hit so far,
+// the current node group and triangle group; pending node groups live on a
+// per-thread stack of kTraversalStack entries held by the caller.
+struct Traversal {
+    RayPre pre;
+    float idx, idy, idz;
+    uint32_t octInv;
+    float tmin;
+    float bestT;
+    uint32_t bestPrim;
+    float bestB1, bestB2;
+    uint2 nodeGroup;  // x: base index of the internal children; y: hit bits in 24..31 (by visiting order) | imask
+    uint2 triGroup;   // x: first triangle slot; y: bits of the triangles left to test
+    int sp;
+    uint32_t budget;  // every node is entered at most once; guards against a malformed node array
+    uint32_t rayRng;
+};
+
+enum : int { kStepContinue = 0, kStepDone = 1, kStepAnyHit = 2 };
+
+HDCX_D void beginTraversal(Traversal& st, const DeviceScene& s, float3 o, float3 d, float tmin, float tmax,
+                           uint32_t rayRng)
+{
+    st.pre = precomputeRay(o, d);
+    const float tiny = 8.271806e-25f;  // 2^-80: direction components below it are treated as 2^-80
+    st.idx = 1.0f / (fabsf(d.x) > tiny ? d.x : copysignf(tiny, d.x));
+    st.idy = 1.0f / (fabsf(d.y) > tiny ? d.y : copysignf(tiny, d.y));
+    st.idz = 1.0f / (fabsf(d.z) > tiny ? d.z : copysignf(tiny, d.z));
+    st.octInv = ((d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u)) ^ 7u;
+    st.tmin = tmin;
+    st.bestT = tmax;
+    st.bestPrim = kInvalidPrimitive;
+    st.bestB1 = 0.0f;
+    st.bestB2 = 0.0f;
+    // The root is child slot 0 of a virtual parent whose children start at node 0.
+    st.nodeGroup = s.nodeCount == 0u ? make_uint2(0u, 0u) : make_uint2(0u, (1u << (24u + (0u ^ st.octInv))) | 1u);
+    st.triGroup = make_uint2(0u, 0u);
+    st.sp = 0;
+    st.budget = s.nodeCount + 1u;
+    st.rayRng = rayRng;
+}
+
+// One traversal step: the triangles of the current triangle group, then one
+// node (its eight children are tested; hit internal children become the new
+// node group, hit leaf triangles the new triangle group). Returns
+// kStepContinue, kStepDone (closest hit, if any, in st.best*) or, for kAny,
+// kStepAnyHit at the first confirmed candidate.
+template <Accept kMode, bool kAny, bool kCount = false>
+HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint2* work)
+{
+    while (st.triGroup.y != 0u) {
+        const int bit = __ffs(st.triGroup.y) - 1;
+        st.triGroup.y &= st.triGroup.y - 1u;
+        const uint32_t slot = st.triGroup.x + static_cast<uint32_t>(bit);
+        const float4 w0 = __ldg(s.triVerts + slot * 3u + 0u);
+        const float4 w1 = __ldg(s.triVerts + slot * 3u + 1u);
+        const float4 w2 = __ldg(s.triVerts + slot * 3u + 2u);
+        if (kCount) work->y++;
+        float t, b1, b2;
+        if (!intersectTriangle(st.pre, xyz(w0), xyz(w1), xyz(w2), st.tmin, st.bestT, t, b1, b2)) continue;
+        const uint32_t prim = __float_as_uint(w0.w);
+        if (!kAny) {
+            if (t > st.bestT) continue;
+            if (t == st.bestT && prim > st.bestPrim) continue;
+        }
+        if (kMode == Accept::Stochastic) {
+            if (!(anyHitThreshold(st.rayRng, prim) <= surfaceOpacity(s, prim, b1, b2))) continue;
+        } else if (kMode == Accept::Threshold) {
+            if (!(surfaceOpacity(s, prim, b1, b2) >= 0.5f)) continue;
+        }
+        if (kAny) return kStepAnyHit;
+        st.bestT = t;
+        st.bestPrim = prim;
+        st.bestB1 = b1;
+        st.bestB2 = b2;
+    }
+    if ((st.nodeGroup.y & 0xff000000u) == 0u) {
+        if (st.sp == 0) return kStepDone;
+        st.nodeGroup = stack[--st.sp];
+    }
+    if (st.budget-- == 0u) return kStepDone;
+    // Next child of the current group, nearest octant first.
+    const uint32_t hitBits = st.nodeGroup.y >> 24;
+    const uint32_t pos = 31u - __clz(hitBits);
+    st.nodeGroup.y &= ~(1u << (24u + pos));
+    const uint32_t childSlot = pos ^ st.octInv;
+    const uint32_t parentMask = st.nodeGroup.y & 0xffu;
+    const uint32_t nodeIndex = st.nodeGroup.x + __popc(parentMask & ((1u << childSlot) - 1u));
+    if ((st.nodeGroup.y & 0xff000000u) != 0u && st.sp < kTraversalStack) stack[st.sp++] = st.nodeGroup;
+
+    if (kCount) work->x++;
+    const uint4* np = reinterpret_cast<const uint4*>(s.nodes + nodeIndex);
+    const uint4 n0 = __ldg(np + 0), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+    const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+    const uint32_t e = n0.w;
+    const float scx = __uint_as_float((e & 0xffu) << 23);
+    const float scy = __uint_as_float(((e >> 8) & 0xffu) << 23);
+    const float scz = __uint_as_float(((e >> 16) & 0xffu) << 23);
+    const uint32_t imask = e >> 24;
+    const float3 o = st.pre.o;
+    const float idx = st.idx, idy = st.idy, idz = st.idz;
+    // t = q * (scale * invd) + (p - o) * invd per plane.
+    const float ax = scx * idx, ay = scy * idy, az = scz * idz;
+    const float bx = (px - o.x) * idx, by = (py - o.y) * idy, bz = (pz - o.z) * idz;
+    // Near/far planes by direction sign: words of qlo (n2.x..n3.y) and qhi (n3.z..n4.w).
+    const uint32_t loX0 = n2.x, loX1 = n2.y, loY0 = n2.z, loY1 = n2.w, loZ0 = n3.x, loZ1 = n3.y;
+    const uint32_t hiX0 = n3.z, hiX1 = n3.w, hiY0 = n4.x, hiY1 = n4.y, hiZ0 = n4.z, hiZ1 = n4.w;
+    const bool sx = idx >= 0.0f, sy = idy >= 0.0f, sz = idz >= 0.0f;
+    const uint32_t nearX0 = sx ? loX0 : hiX0, nearX1 = sx ? loX1 : hiX1, farX0 = sx ? hiX0 : loX0, farX1 = sx ? hiX1 : loX1;
+    const uint32_t nearY0 = sy ? loY0 : hiY0, nearY1 = sy ? loY1 : hiY1, farY0 = sy ? hiY0 : loY0, farY1 = sy ? hiY1 : loY1;
+    const uint32_t nearZ0 = sz ? loZ0 : hiZ0, nearZ1 = sz ? loZ1 : hiZ1, farZ0 = sz ? hiZ0 : loZ0, farZ1 = sz ? hiZ1 : loZ1;
+    const uint32_t meta0 = n1.z, meta1 = n1.w;
+    const uint32_t octInv = st.octInv;
+    const float bestT = st.bestT;
+    uint32_t nodeHits = 0u, triHits = 0u;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int k = i & 3;
+        const uint32_t meta = ((i < 4 ? meta0 : meta1) >> (8 * k)) & 0xffu;
+        const float tnx = fmaf(byteToFloat(i < 4 ? nearX0 : nearX1, k), ax, bx);
+        const float tny = fmaf(byteToFloat(i < 4 ? nearY0 : nearY1, k), ay, by);
+        const float tnz = fmaf(byteToFloat(i < 4 ? nearZ0 : nearZ1, k), az, bz);
+        const float tfx = fmaf(byteToFloat(i < 4 ? farX0 : farX1, k), ax, bx);
+        const float tfy = fmaf(byteToFloat(i < 4 ? farY0 : farY1, k), ay, by);
+        const float tfz = fmaf(byteToFloat(i < 4 ? farZ0 : farZ1, k), az, bz);
+        const float tNear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+        const float tFar = fminf(fminf(tfx, tfy), fminf(tfz, bestT));
+        if (meta != 0u && tNear <= tFar) {
+            if ((imask >> i) & 1u) nodeHits |= 1u << (static_cast<uint32_t>(i) ^ octInv);
+            else triHits |= (meta >> 5) << (meta & 31u);
+        }
+    }
+    st.nodeGroup = make_uint2(n1.x, (nodeHits << 24) | imask);
+    st.triGroup = make_uint2(n1.y, triHits);
+    return kStepContinue;
+}
 
 // Traverses the wide BVH. kAny: stop at the first confirmed candidate.
 // Returns true on a (confirmed) hit; for closest queries fills `hit`.
@@ -120,115 +265,18 @@ HDCX_D bool traceRay(const DeviceScene& s, float3 o, float3 d, float tmin, float
                      uint2* work = nullptr)
 {
     if (s.nodeCount == 0u) return false;
-    const RayPre pre = precomputeRay(o, d);
-    const float tiny = 8.271806e-25f;  // 2^-80: direction components below it are treated as 2^-80
-    const float idx = 1.0f / (fabsf(d.x) > tiny ? d.x : copysignf(tiny, d.x));
-    const float idy = 1.0f / (fabsf(d.y) > tiny ? d.y : copysignf(tiny, d.y));
-    const float idz = 1.0f / (fabsf(d.z) > tiny ? d.z : copysignf(tiny, d.z));
-    const uint32_t octInv = ((d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u)) ^ 7u;
-
-    float bestT = tmax;
-    uint32_t bestPrim = kInvalidPrimitive;
-    float bestB1 = 0.0f, bestB2 = 0.0f;
-
+    Traversal st;
+    beginTraversal(st, s, o, d, tmin, tmax, rayRng);
     uint2 stack[kTraversalStack];
-    int sp = 0;
-    // A node group: x = base index of the internal children, y = hit bits in
-    // 24..31 (by visiting order) | parent imask in 0..7. The root is child
-    // slot 0 of a virtual parent whose children start at node 0.
-    uint2 nodeGroup = make_uint2(0u, (1u << (24u + (0u ^ octInv))) | 1u);
-    uint2 triGroup = make_uint2(0u, 0u);
-    // Every node is entered at most once in a tree; the cap only guards
-    // against a malformed node array.
-    uint32_t budget = s.nodeCount + 1u;
-
-    while (true) {
-        while (triGroup.y != 0u) {
-            const int bit = __ffs(triGroup.y) - 1;
-            triGroup.y &= triGroup.y - 1u;
-            const uint32_t slot = triGroup.x + static_cast<uint32_t>(bit);
-            const float4 w0 = __ldg(s.triVerts + slot * 3u + 0u);
-            const float4 w1 = __ldg(s.triVerts + slot * 3u + 1u);
-            const float4 w2 = __ldg(s.triVerts + slot * 3u + 2u);
-            if (kCount) work->y++;
-            float t, b1, b2;
-            if (!intersectTriangle(pre, xyz(w0), xyz(w1), xyz(w2), tmin, tmax, t, b1, b2)) continue;
-            const uint32_t prim = __float_as_uint(w0.w);
-            if (!kAny) {
-                if (t > bestT) continue;
-                if (t == bestT && prim > bestPrim) continue;
-            }
-            if (kMode == Accept::Stochastic) {
-                if (!(anyHitThreshold(rayRng, prim) <= surfaceOpacity(s, prim, b1, b2))) continue;
-            } else if (kMode == Accept::Threshold) {
-                if (!(surfaceOpacity(s, prim, b1, b2) >= 0.5f)) continue;
-            }
-            if (kAny) return true;
-            bestT = t;
-            bestPrim = prim;
-            bestB1 = b1;
-            bestB2 = b2;
-        }
-        if ((nodeGroup.y & 0xff000000u) == 0u) {
-            if (sp == 0) break;
-            nodeGroup = stack[--sp];
-        }
-        if (budget-- == 0u) break;
-        // Next child of the current group, nearest octant first.
-        const uint32_t hitBits = nodeGroup.y >> 24;
-        const uint32_t pos = 31u - __clz(hitBits);
-        nodeGroup.y &= ~(1u << (24u + pos));
-        const uint32_t childSlot = pos ^ octInv;
-        const uint32_t parentMask = nodeGroup.y & 0xffu;
-        const uint32_t nodeIndex = nodeGroup.x + __popc(parentMask & ((1u << childSlot) - 1u));
-        if ((nodeGroup.y & 0xff000000u) != 0u && sp < kTraversalStack) stack[sp++] = nodeGroup;
-
-        if (kCount) work->x++;
-        const uint4* np = reinterpret_cast<const uint4*>(s.nodes + nodeIndex);
-        const uint4 n0 = __ldg(np + 0), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
-        const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
-        const uint32_t e = n0.w;
-        const float scx = __uint_as_float((e & 0xffu) << 23);
-        const float scy = __uint_as_float(((e >> 8) & 0xffu) << 23);
-        const float scz = __uint_as_float(((e >> 16) & 0xffu) << 23);
-        const uint32_t imask = e >> 24;
-        // t = q * (scale * invd) + (p - o) * invd per plane.
-        const float ax = scx * idx, ay = scy * idy, az = scz * idz;
-        const float bx = (px - o.x) * idx, by = (py - o.y) * idy, bz = (pz - o.z) * idz;
-        // Near/far planes by direction sign: words of qlo (n2.x..n3.y) and qhi (n3.z..n4.w).
-        const uint32_t loX0 = n2.x, loX1 = n2.y, loY0 = n2.z, loY1 = n2.w, loZ0 = n3.x, loZ1 = n3.y;
-        const uint32_t hiX0 = n3.z, hiX1 = n3.w, hiY0 = n4.x, hiY1 = n4.y, hiZ0 = n4.z, hiZ1 = n4.w;
-        const bool sx = idx >= 0.0f, sy = idy >= 0.0f, sz = idz >= 0.0f;
-        const uint32_t nearX0 = sx ? loX0 : hiX0, nearX1 = sx ? loX1 : hiX1, farX0 = sx ? hiX0 : loX0, farX1 = sx ? hiX1 : loX1;
-        const uint32_t nearY0 = sy ? loY0 : hiY0, nearY1 = sy ? loY1 : hiY1, farY0 = sy ? hiY0 : loY0, farY1 = sy ? hiY1 : loY1;
-        const uint32_t nearZ0 = sz ? loZ0 : hiZ0, nearZ1 = sz ? loZ1 : hiZ1, farZ0 = sz ? hiZ0 : loZ0, farZ1 = sz ? hiZ1 : loZ1;
-        const uint32_t meta0 = n1.z, meta1 = n1.w;
-        uint32_t nodeHits = 0u, triHits = 0u;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int k = i & 3;
-            const uint32_t meta = ((i < 4 ? meta0 : meta1) >> (8 * k)) & 0xffu;
-            const float tnx = fmaf(byteToFloat(i < 4 ? nearX0 : nearX1, k), ax, bx);
-            const float tny = fmaf(byteToFloat(i < 4 ? nearY0 : nearY1, k), ay, by);
-            const float tnz = fmaf(byteToFloat(i < 4 ? nearZ0 : nearZ1, k), az, bz);
-            const float tfx = fmaf(byteToFloat(i < 4 ? farX0 : farX1, k), ax, bx);
-            const float tfy = fmaf(byteToFloat(i < 4 ? farY0 : farY1, k), ay, by);
-            const float tfz = fmaf(byteToFloat(i < 4 ? farZ0 : farZ1, k), az, bz);
-            const float tNear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-            const float tFar = fminf(fminf(tfx, tfy), fminf(tfz, bestT));
-            if (meta != 0u && tNear <= tFar) {
-                if ((imask >> i) & 1u) nodeHits |= 1u << (static_cast<uint32_t>(i) ^ octInv);
-                else triHits |= (meta >> 5) << (meta & 31u);
-            }
-        }
-        nodeGroup = make_uint2(n1.x, (nodeHits << 24) | imask);
-        triGroup = make_uint2(n1.y, triHits);
+    int r;
+    while ((r = traversalStep<kMode, kAny, kCount>(st, stack, s, work)) == kStepContinue) {
     }
-    if (kAny || bestPrim == kInvalidPrimitive) return false;
-    hit.t = bestT;
-    hit.primitive = bestPrim;
-    hit.b1 = bestB1;
-    hit.b2 = bestB2;
+    if (kAny) return r == kStepAnyHit;
+    if (st.bestPrim == kInvalidPrimitive) return false;
+    hit.t = st.bestT;
+    hit.primitive = st.bestPrim;
+    hit.b1 = st.bestB1;
+    hit.b2 = st.bestB2;
     return true;
 }
 

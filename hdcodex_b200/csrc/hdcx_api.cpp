@@ -194,6 +194,37 @@ bool needsFullShading(const PackedSceneData& d)
     return false;
 }
 
+// The arrays behind TexDesc::cdf for a dome importance texture (R: the
+// row's conditional CDF, G at column 0: the marginal CDF). Returns false, and
+// the device keeps the plain binary search, unless every CDF is finite and
+// non-decreasing: only then does the two-level search find the same index.
+bool buildCdfArrays(const PackedTexture& pt, std::vector<float>& block)
+{
+    const size_t w = pt.width, h = pt.height;
+    if (w == 0 || h == 0 || pt.floats.size() < w * h * 4u) return false;
+    const size_t hs = (h + 31) / 32, ws = (w + 31) / 32;
+    block.assign(h + hs + w * h + h * ws, 0.0F);
+    float* marginal = block.data();
+    float* marginalSkip = marginal + h;
+    float* conditional = marginalSkip + hs;
+    float* conditionalSkip = conditional + w * h;
+    auto monotone = [](const float* v, size_t n) {
+        for (size_t i = 0; i < n; ++i) {
+            if (!std::isfinite(v[i]) || (i > 0 && v[i] < v[i - 1])) return false;
+        }
+        return true;
+    };
+    for (size_t row = 0; row < h; ++row) {
+        marginal[row] = pt.floats[(row * w) * 4u + 1u];
+        for (size_t col = 0; col < w; ++col) conditional[row * w + col] = pt.floats[(row * w + col) * 4u + 0u];
+        if (!monotone(conditional + row * w, w)) return false;
+        for (size_t k = 0; k < ws; ++k) conditionalSkip[row * ws + k] = conditional[row * w + std::min(32 * k + 31, w - 1)];
+    }
+    if (!monotone(marginal, h)) return false;
+    for (size_t k = 0; k < hs; ++k) marginalSkip[k] = marginal[std::min(32 * k + 31, h - 1)];
+    return true;
+}
+
 void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
 {
     check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
@@ -217,6 +248,18 @@ void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
         td.texels = pt.format == HDCX_TEXEL_RGBA32F ? static_cast<const void*>(t->upload(pt.floats))
                                                     : static_cast<const void*>(t->upload(pt.bytes));
         descs.push_back(td);
+    }
+    // Dome importance textures get the compact CDF arrays of TexDesc::cdf.
+    for (uint32_t l = 0; l < d.lightCount && (size_t(l) + 1) * sizeof(GpuLight) <= d.lights.size(); ++l) {
+        GpuLight light;
+        std::memcpy(&light, d.lights.data() + size_t(l) * sizeof(GpuLight), sizeof(GpuLight));
+        const uint32_t index = light.textureInfo.w;
+        if (light.textureInfo.z != 0u || index >= descs.size() || descs[index].cdf) continue;
+        const PackedTexture& pt = d.textures[index];
+        std::vector<float> block;
+        if (pt.format == HDCX_TEXEL_RGBA32F && buildCdfArrays(pt, block)) {
+            descs[index].cdf = t->upload(block);
+        }
     }
     t->texDescs.allocate(std::max<size_t>(1, descs.size()) * sizeof(TexDesc));
     if (!descs.empty()) {

@@ -265,7 +265,10 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
     return false;
 }
 
-template <bool kFull>
+// kLit: the scene has analytic or dome lights and no emissive triangles, so
+// neither the fallback sun and sky (:1593-1668) nor emissive-triangle
+// sampling (:1670-1731) can run; both are compiled out.
+template <bool kFull, bool kLit>
 __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce,
                                                    const uint32_t* queue, const uint32_t* count, uint32_t* nextQueue,
                                                    uint32_t* nextCount)
@@ -481,8 +484,8 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
             const float baseEnergy = diffuseEnergy + translucentEnergy;
             const float specularProbability = clampf(specularEnergy / gmax(specularEnergy + baseEnergy, 1e-5f), 0.05f, 0.95f);
             const float translucentProbability = baseEnergy > 1e-5f ? translucentEnergy / baseEnergy : 0.0f;
-            const uint32_t lightCount = s.lightCount;
-            const bool hasMeshLights = s.hasMeshLights != 0u;
+            const uint32_t lightCount = kLit ? 1u : s.lightCount;
+            const bool hasMeshLights = kLit ? false : s.hasMeshLights != 0u;
 
             SurfaceParams sp;
             sp.diffuseColor = diffuseColor;
@@ -595,7 +598,7 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
                                                 maximumShadowDistance, a, inversePdf, misWeight, gmax(lightSelectionPdf, 1e-8f));
                     }
                 }
-            } else if (!hasMeshLights) {
+            } else if (!kLit && !hasMeshLights) {
                 // :1593-1668 fallback sun and sky
                 const bool zUp = f.zUp != 0u;
                 const float3 up = zUp ? f3(0.0f, 0.0f, 1.0f) : f3(0.0f, 1.0f, 0.0f);
@@ -632,7 +635,7 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
                 }
             }
 
-            if (hasMeshLights) {
+            if (!kLit && hasMeshLights) {
                 // :1670-1731 emissive-triangle sample
                 const uint32_t primitiveCount = s.primitiveCount;
                 const float target = randomFloat(rng);
@@ -1046,10 +1049,13 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
             CUDA_OK(cudaMemsetAsync(outCount, 0, sizeof(uint32_t), stream));
             CUDA_OK(cudaMemsetAsync(paths.counters + 2, 0, sizeof(uint32_t), stream));
             timed(1, [&] {
+                const bool lit = scene.lightCount > 0u && !scene.hasMeshLights;
                 if (scene.fullShading) {
-                    shadeKernel<true><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+                    if (lit) shadeKernel<true, true><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+                    else shadeKernel<true, false><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
                 } else {
-                    shadeKernel<false><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+                    if (lit) shadeKernel<false, true><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+                    else shadeKernel<false, false><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
                 }
             });
             CUDA_OK(cudaGetLastError());
