@@ -277,7 +277,8 @@ def run_batch(args):
     torch.cuda.set_device(local)
     from hdcodex_b200 import PathTracer, render_batch, workloads
 
-    jobs = [wl for i, wl in enumerate(workloads.batch_jobs(args.jobs)) if i % world == rank]
+    from hdcodex_b200.multigpu import job_shard
+    jobs = [workloads.batch_job(i) for i in job_shard(args.jobs, world, rank)]
     tracers = []
     for wl in jobs:
         t = PathTracer(local)
@@ -366,8 +367,10 @@ def run_hdcx(args):
         return
     paths_per_step = wl.spectral_paths
 
+    from hdcodex_b200.multigpu import sample_range
+
     def sample_index(step):
-        return (step * world + rank) * wl.spp
+        return sample_range(step, world, rank, wl.spp)
 
     # Warm-up, then one counting pass for the roofline's algorithmic bytes.
     for i in range(args.warmup):

@@ -26,6 +26,7 @@ namespace hdcx {
 
 #define HDCX_D __device__ __forceinline__
 #define HDCX_HD __host__ __device__ __forceinline__
+#define HDCX_NOINLINE static __device__ __noinline__
 
 constexpr uint32_t kMissingTexture = 0xffffffffu;
 constexpr float kPi = 3.14159265359f;

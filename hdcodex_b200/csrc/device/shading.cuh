@@ -500,7 +500,9 @@ HDCX_D float evaluateDirectSurface(float3 normal, float3 tangent, float3 viewDir
     return baseLayer * (1.0f - clampf(p.sheen * sheenAlbedo, 0.0f, 1.0f)) + sheenLayer;
 }
 
-HDCX_D float surfaceReflectionPdf(float3 normal, float3 tangent, float3 viewDirection, float3 lightDirection,
+// Not inlined: called from several sites of the shade kernel, one shared
+// copy keeps the kernel's instruction footprint smaller (measured faster).
+HDCX_NOINLINE float surfaceReflectionPdf(float3 normal, float3 tangent, float3 viewDirection, float3 lightDirection,
                                   float2 roughness, float2 coatRoughness, float sheenProbability, float coatProbability,
                                   float specularProbability, float translucentProbability)
 {
@@ -841,7 +843,9 @@ HDCX_D void sampleAnalyticLight(const DeviceScene& s, float3 position, float3 no
     selectionPdf = lightSelectionWeight(s.lights[lightIndex], position, normal, diffuseEnergy, specularEnergy, translucentEnergy) / total;
 }
 
-HDCX_D float environmentLightPdf(const DeviceScene& s, float3 position, float3 normal, float3 direction,
+// Not inlined: called from several sites of the shade kernel, one shared
+// copy keeps the kernel's instruction footprint smaller (measured faster).
+HDCX_NOINLINE float environmentLightPdf(const DeviceScene& s, float3 position, float3 normal, float3 direction,
                                  float diffuseEnergy, float specularEnergy, float translucentEnergy)
 {
     // :739-758

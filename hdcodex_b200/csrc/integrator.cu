@@ -120,7 +120,7 @@ __global__ void generateKernel(FrameConst f, WaveDesc w, PathBuffers p)
 // extend: closest hit of every queued ray (vulkan_path_tracer.cpp:1228-1243)
 // ---------------------------------------------------------------------------
 template <Accept kMode, bool kCount>
-__global__ void __launch_bounds__(128) extendKernel(DeviceScene s, PathBuffers p, const uint32_t* queue,
+__global__ void __launch_bounds__(128, 8) extendKernel(DeviceScene s, PathBuffers p, const uint32_t* queue,
                                                     const uint32_t* count)
 {
     const uint32_t n = *count;
@@ -834,7 +834,7 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
 // shadow: visibility of light samples (vulkan_path_tracer.cpp:855-912)
 // ---------------------------------------------------------------------------
 template <bool kOpaque, bool kCount>
-__global__ void __launch_bounds__(128) shadowKernel(DeviceScene s, PathBuffers p)
+__global__ void __launch_bounds__(128, 8) shadowKernel(DeviceScene s, PathBuffers p)
 {
     const uint32_t n = p.counters[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(p.stats + 1, static_cast<unsigned long long>(n));
