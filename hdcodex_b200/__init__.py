@@ -9,10 +9,10 @@ VulkanPathTracer and ``scene`` mirrors its SceneSnapshot types.
 from . import scene
 from .scene import (AUTOMATIC, CYLINDER, DISK, DISTANT, DOME, LATLONG, RECT, SPHERE, Light, Material, Mesh,
                     Scene, Texture, camera)
-from .tracer import FUSED, MODULAR, RASTER_PREVIEW, PathTracer, lib, pack_scene, probe_devices, render_batch
+from .tracer import FUSED, MODULAR, RASTER_PREVIEW, PathTracer, lib, pack_scene, probe_devices, render_batch, RadianceCache
 
 __all__ = [
-    "scene", "Scene", "Mesh", "Material", "Texture", "Light", "camera", "PathTracer", "pack_scene", "render_batch",
+    "scene", "Scene", "Mesh", "Material", "Texture", "Light", "camera", "PathTracer", "pack_scene", "render_batch", "RadianceCache",
     "probe_devices", "lib", "FUSED", "MODULAR", "RASTER_PREVIEW", "DOME", "RECT", "DISK", "SPHERE",
     "CYLINDER", "DISTANT", "AUTOMATIC", "LATLONG",
 ]

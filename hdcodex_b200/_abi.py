@@ -227,6 +227,20 @@ class RenderStats(C.Structure):
     ]
 
 
+class NrcConfig(C.Structure):
+    """hdcx_nrc_config."""
+    _fields_ = [
+        ("log2_table_size", C.c_uint32),
+        ("base_resolution", C.c_uint32),
+        ("finest_resolution", C.c_uint32),
+        ("learning_rate", C.c_float),
+        ("beta1", C.c_float),
+        ("beta2", C.c_float),
+        ("epsilon", C.c_float),
+        ("seed", C.c_uint32),
+    ]
+
+
 class BatchJob(C.Structure):
     """hdcx_batch_job: one job of hdcx_render_batch."""
     _fields_ = [
@@ -246,7 +260,7 @@ class BatchJob(C.Structure):
 
 STRUCTS_IN_ABI_ORDER = [
     Camera, MeshDesc, MaterialDesc, TextureDesc, LightDesc, SceneDesc, PackedTexture, PackedScene,
-    RenderStats, BatchJob,
+    RenderStats, BatchJob, NrcConfig,
 ]
 
 GPU_MATERIAL_BYTES = 368

@@ -24,6 +24,7 @@ INCLUDE = os.path.join(ROOT, "include")
 SOURCES = [
     "bvh_build.cu",
     "integrator.cu",
+    "nrc.cu",
     "render_static.cu",
     "scene_pack.cpp",
     "hdcx_api.cpp",

@@ -19,6 +19,7 @@
 
 #include "bvh_build.h"
 #include "integrator.h"
+#include "nrc.h"
 #include "render_static.h"
 #include "scene_pack.h"
 
@@ -389,7 +390,7 @@ HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity)
     const uint64_t all[] = {sizeof(hdcx_camera),         sizeof(hdcx_mesh_desc),  sizeof(hdcx_material_desc),
                             sizeof(hdcx_texture_desc),   sizeof(hdcx_light_desc), sizeof(hdcx_scene_desc),
                             sizeof(hdcx_packed_texture), sizeof(hdcx_packed_scene), sizeof(hdcx_render_stats),
-                            sizeof(hdcx_batch_job)};
+                            sizeof(hdcx_batch_job), sizeof(hdcx_nrc_config)};
     const uint32_t n = static_cast<uint32_t>(sizeof(all) / sizeof(all[0]));
     for (uint32_t i = 0; i < std::min(n, capacity); ++i) sizes[i] = all[i];
     return n;
@@ -861,6 +862,156 @@ HDCX_API hdcx_status hdcx_get_stats(const hdcx_tracer* t, hdcx_render_stats* sta
     if (!t || !stats) return HDCX_ERROR_INVALID_ARGUMENT;
     *stats = t->stats;
     return HDCX_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Neural radiance cache
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct hdcx_nrc {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    hdcx::nrc::Cache* cache = nullptr;
+    std::string lastError;
+    ~hdcx_nrc()
+    {
+        if (stream) cudaStreamSynchronize(stream);
+        hdcx::nrc::destroy(cache);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+template <typename F>
+hdcx_status nrcGuarded(hdcx_nrc* n, F&& body)
+{
+    try {
+        n->lastError.clear();
+        check(cudaSetDevice(n->device), "cudaSetDevice");
+        body();
+        return HDCX_OK;
+    } catch (const StatusError& e) {
+        n->lastError = e.what();
+        return e.status;
+    } catch (const std::invalid_argument& e) {
+        n->lastError = e.what();
+        return HDCX_ERROR_INVALID_ARGUMENT;
+    } catch (const std::bad_alloc&) {
+        n->lastError = "host allocation failed";
+        return HDCX_ERROR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        n->lastError = e.what();
+        const bool timeout = std::strstr(e.what(), "timed out") != nullptr;
+        const bool oom = std::strstr(e.what(), "out of memory") != nullptr;
+        return timeout ? HDCX_ERROR_TIMEOUT : (oom ? HDCX_ERROR_OUT_OF_MEMORY : HDCX_ERROR_CUDA);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+HDCX_API void hdcx_nrc_defaults(hdcx_nrc_config* c)
+{
+    if (!c) return;
+    const hdcx::nrc::Config d;
+    c->log2_table_size = d.log2TableSize;
+    c->base_resolution = d.baseResolution;
+    c->finest_resolution = d.finestResolution;
+    c->learning_rate = d.learningRate;
+    c->beta1 = d.beta1;
+    c->beta2 = d.beta2;
+    c->epsilon = d.epsilon;
+    c->seed = d.seed;
+}
+
+HDCX_API hdcx_status hdcx_nrc_create(int32_t device, const hdcx_nrc_config* config, hdcx_nrc** out)
+{
+    if (!out) return HDCX_ERROR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int supported = 0, count = 0;
+    hdcx_probe_devices(&supported, &count);
+    if (!supported || device < 0 || device >= count) return HDCX_ERROR_NO_DEVICE;
+    auto* n = new (std::nothrow) hdcx_nrc();
+    if (!n) return HDCX_ERROR_OUT_OF_MEMORY;
+    n->device = device;
+    const hdcx_status s = nrcGuarded(n, [&] {
+        hdcx::nrc::Config c;
+        if (config) {
+            c.log2TableSize = config->log2_table_size;
+            c.baseResolution = config->base_resolution;
+            c.finestResolution = config->finest_resolution;
+            c.learningRate = config->learning_rate;
+            c.beta1 = config->beta1;
+            c.beta2 = config->beta2;
+            c.epsilon = config->epsilon;
+            c.seed = config->seed;
+        }
+        check(cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        n->cache = hdcx::nrc::create(device, c);
+    });
+    if (s != HDCX_OK) {
+        delete n;
+        return s;
+    }
+    *out = n;
+    return HDCX_OK;
+}
+
+HDCX_API void hdcx_nrc_destroy(hdcx_nrc* n)
+{
+    if (!n) return;
+    cudaSetDevice(n->device);
+    delete n;
+}
+
+HDCX_API const char* hdcx_nrc_last_error(const hdcx_nrc* n) { return n ? n->lastError.c_str() : "null cache"; }
+
+HDCX_API uint64_t hdcx_nrc_grid_parameter_count(const hdcx_nrc* n) { return n ? hdcx::nrc::gridParameterCount(n->cache) : 0; }
+
+HDCX_API hdcx_status hdcx_nrc_resolutions(const hdcx_nrc* n, uint32_t* r)
+{
+    if (!n || !r) return HDCX_ERROR_INVALID_ARGUMENT;
+    for (int l = 0; l < hdcx::nrc::kLevels; ++l) r[l] = hdcx::nrc::resolution(n->cache, l);
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_nrc_query(hdcx_nrc* n, const float* queries, uint32_t count, float* radiance)
+{
+    if (!n || (count && (!queries || !radiance))) return HDCX_ERROR_INVALID_ARGUMENT;
+    return nrcGuarded(n, [&] { hdcx::nrc::query(n->cache, queries, count, radiance, n->stream); });
+}
+
+HDCX_API hdcx_status hdcx_nrc_train(hdcx_nrc* n, const float* queries, const float* targets, uint32_t count, uint32_t steps,
+                                    float* meanLoss)
+{
+    if (!n || (count && (!queries || !targets))) return HDCX_ERROR_INVALID_ARGUMENT;
+    return nrcGuarded(n, [&] {
+        const float loss = hdcx::nrc::train(n->cache, queries, targets, count, steps, n->stream);
+        if (meanLoss) *meanLoss = loss;
+    });
+}
+
+HDCX_API hdcx_status hdcx_nrc_gradients(hdcx_nrc* n, const float* queries, const float* targets, uint32_t count,
+                                        float* mlpGradient, float* gridGradient)
+{
+    if (!n || (count && (!queries || !targets))) return HDCX_ERROR_INVALID_ARGUMENT;
+    return nrcGuarded(n, [&] { hdcx::nrc::gradients(n->cache, queries, targets, count, mlpGradient, gridGradient, n->stream); });
+}
+
+HDCX_API hdcx_status hdcx_nrc_get_parameters(hdcx_nrc* n, float* mlp, float* grid)
+{
+    if (!n) return HDCX_ERROR_INVALID_ARGUMENT;
+    return nrcGuarded(n, [&] { hdcx::nrc::getParameters(n->cache, mlp, grid); });
+}
+
+HDCX_API hdcx_status hdcx_nrc_set_parameters(hdcx_nrc* n, const float* mlp, const float* grid)
+{
+    if (!n || !mlp || !grid) return HDCX_ERROR_INVALID_ARGUMENT;
+    return nrcGuarded(n, [&] { hdcx::nrc::setParameters(n->cache, mlp, grid); });
 }
 
 }  // extern "C"

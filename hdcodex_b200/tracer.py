@@ -59,6 +59,17 @@ SIGNATURES = {
                                      C.c_uint32, _P, C.POINTER(C.c_int32)]),
     "hdcx_render_batch": (C.c_int, [C.POINTER(_abi.BatchJob), C.c_uint32, C.c_uint64]),
     "hdcx_read_rgba": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint64]),
+    "hdcx_nrc_defaults": (None, [C.POINTER(_abi.NrcConfig)]),
+    "hdcx_nrc_create": (C.c_int, [C.c_int32, C.POINTER(_abi.NrcConfig), C.POINTER(C.c_void_p)]),
+    "hdcx_nrc_destroy": (None, [_P]),
+    "hdcx_nrc_last_error": (C.c_char_p, [_P]),
+    "hdcx_nrc_grid_parameter_count": (C.c_uint64, [_P]),
+    "hdcx_nrc_resolutions": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
+    "hdcx_nrc_query": (C.c_int, [_P, _P, C.c_uint32, _P]),
+    "hdcx_nrc_train": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
+    "hdcx_nrc_gradients": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "hdcx_nrc_get_parameters": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "hdcx_nrc_set_parameters": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "hdcx_read_xyz": (C.c_int, [_P, C.POINTER(C.c_double), C.c_uint64, C.POINTER(C.c_uint64)]),
     "hdcx_device_rgba": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
     "hdcx_trace_primary": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32,
@@ -199,6 +210,89 @@ class PathTracer:
         st = _abi.RenderStats()
         self._check(lib().hdcx_get_stats(self._h, C.byref(st)), "get_stats")
         return {name: getattr(st, name) for name, _ in _abi.RenderStats._fields_}
+
+
+NRC_QUERY_FLOATS = 12
+NRC_WEIGHT_COUNT = 17408
+NRC_LEVELS = 16
+
+
+class RadianceCache:
+    """hdcx_nrc: the neural radiance cache (hash grid + tensor-core MLP).
+    Query, target and output arguments are device pointers (ints)."""
+
+    def __init__(self, device: int = 0, **config):
+        cfg = _abi.NrcConfig()
+        lib().hdcx_nrc_defaults(C.byref(cfg))
+        for k, v in config.items():
+            setattr(cfg, k, v)
+        self.config = cfg
+        h = C.c_void_p()
+        status = lib().hdcx_nrc_create(device, C.byref(cfg), C.byref(h))
+        if status != 0:
+            raise RuntimeError(f"hdcx_nrc_create failed: {STATUS.get(status, status)}")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hdcx_nrc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, status, what):
+        if status != 0:
+            msg = lib().hdcx_nrc_last_error(self._h) or b""
+            raise RuntimeError(f"{what} failed: {STATUS.get(status, status)}: {msg.decode()}")
+
+    @property
+    def grid_parameter_count(self) -> int:
+        return int(lib().hdcx_nrc_grid_parameter_count(self._h))
+
+    def resolutions(self):
+        r = (C.c_uint32 * NRC_LEVELS)()
+        self._check(lib().hdcx_nrc_resolutions(self._h, r), "resolutions")
+        return list(r)
+
+    def query(self, queries_ptr: int, count: int, out_ptr: int):
+        self._check(lib().hdcx_nrc_query(self._h, queries_ptr, count, out_ptr), "query")
+
+    def train(self, queries_ptr: int, targets_ptr: int, count: int, steps: int = 1) -> float:
+        loss = C.c_float(0.0)
+        self._check(lib().hdcx_nrc_train(self._h, queries_ptr, targets_ptr, count, steps, C.byref(loss)), "train")
+        return float(loss.value)
+
+    def gradients(self, queries_ptr: int, targets_ptr: int, count: int):
+        mlp = np.zeros(NRC_WEIGHT_COUNT, np.float32)
+        grid = np.zeros(self.grid_parameter_count, np.float32)
+        self._check(lib().hdcx_nrc_gradients(self._h, queries_ptr, targets_ptr, count,
+                                             mlp.ctypes.data_as(C.POINTER(C.c_float)),
+                                             grid.ctypes.data_as(C.POINTER(C.c_float))), "gradients")
+        return mlp, grid
+
+    def parameters(self):
+        mlp = np.zeros(NRC_WEIGHT_COUNT, np.float32)
+        grid = np.zeros(self.grid_parameter_count, np.float32)
+        self._check(lib().hdcx_nrc_get_parameters(self._h, mlp.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  grid.ctypes.data_as(C.POINTER(C.c_float))), "get_parameters")
+        return mlp, grid
+
+    def set_parameters(self, mlp, grid):
+        mlp = np.ascontiguousarray(mlp, np.float32)
+        grid = np.ascontiguousarray(grid, np.float32)
+        self._check(lib().hdcx_nrc_set_parameters(self._h, mlp.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  grid.ctypes.data_as(C.POINTER(C.c_float))), "set_parameters")
 
 
 def render_batch(jobs, path_budget: int = 0):

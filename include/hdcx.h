@@ -335,7 +335,8 @@ typedef struct hdcx_batch_job {
 HDCX_API uint32_t hdcx_abi_version(void);
 
 /* Byte size of each ABI struct, indexed 0..7: camera, mesh, material, texture,
- * light, scene, packed_texture, packed_scene; 8: render_stats; 9: batch_job.
+ * light, scene, packed_texture, packed_scene; 8: render_stats; 9: batch_job;
+ * 10: nrc_config.
  * Lets bindings check their struct mirrors. Returns the number of entries. */
 HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity);
 
@@ -490,6 +491,59 @@ HDCX_API hdcx_status hdcx_set_profiling(hdcx_tracer* tracer, uint32_t flags);
 /* Number of paths resident per wave (0 = automatic). Larger waves use more
  * device memory for path state; results do not depend on it. */
 HDCX_API hdcx_status hdcx_set_wave_size(hdcx_tracer* tracer, uint64_t paths_per_wave);
+
+/* ---------------------------------------------------------------------------
+ * Neural radiance cache (no counterpart in the reference; the learned part of
+ * the B200 build): a multiresolution hash-grid encoding of position (16
+ * levels x 2 FP16 features, 2^log2_table_size entries per level) plus
+ * direction, shading normal, roughness and wavelength, feeding a 64-wide MLP
+ * with four ReLU hidden layers whose forward and backward passes run as BF16
+ * tcgen05 tensor-core GEMMs with FP32 accumulation; FP32 Adam on the relative
+ * L2 loss. A query record is HDCX_NRC_QUERY_FLOATS floats: position (3,
+ * normalised to [0, 1]), direction (3), shading normal (3), roughness,
+ * (wavelength - 380) / 400, 0. Query, target and output pointers of the
+ * query/train/gradient calls are device memory.
+ * ------------------------------------------------------------------------- */
+#define HDCX_NRC_QUERY_FLOATS 12u
+#define HDCX_NRC_WEIGHT_COUNT 17408u /* 4 x 64 x 64 + 16 x 64 FP32 weights, row-major [out][in] per layer */
+#define HDCX_NRC_LEVELS 16u
+
+typedef struct hdcx_nrc hdcx_nrc;
+
+typedef struct hdcx_nrc_config {
+    uint32_t log2_table_size;   /* entries per level = 2^n (default 19) */
+    uint32_t base_resolution;   /* cells per axis of the coarsest level (default 16) */
+    uint32_t finest_resolution; /* cells per axis of the finest level (default 2048) */
+    float learning_rate;        /* Adam step size (default 1e-2) */
+    float beta1;                /* default 0.9 */
+    float beta2;                /* default 0.99 */
+    float epsilon;              /* default 1e-8 */
+    uint32_t seed;              /* initialisation seed */
+} hdcx_nrc_config;
+
+HDCX_API void hdcx_nrc_defaults(hdcx_nrc_config* config);
+HDCX_API hdcx_status hdcx_nrc_create(int32_t device, const hdcx_nrc_config* config, hdcx_nrc** out);
+HDCX_API void hdcx_nrc_destroy(hdcx_nrc* cache);
+HDCX_API const char* hdcx_nrc_last_error(const hdcx_nrc* cache);
+/* FP32 parameters of the hash table: levels x 2^log2_table_size x 2. */
+HDCX_API uint64_t hdcx_nrc_grid_parameter_count(const hdcx_nrc* cache);
+/* Cells per axis of each of the HDCX_NRC_LEVELS levels. */
+HDCX_API hdcx_status hdcx_nrc_resolutions(const hdcx_nrc* cache, uint32_t* resolutions);
+/* radiance[i] = the cache's prediction for query record i. */
+HDCX_API hdcx_status hdcx_nrc_query(hdcx_nrc* cache, const float* queries, uint32_t count, float* radiance);
+/* `steps` Adam steps on the batch; *mean_loss (host, optional) = the last
+ * step's mean relative L2 loss. */
+HDCX_API hdcx_status hdcx_nrc_train(hdcx_nrc* cache, const float* queries, const float* targets, uint32_t count,
+                                    uint32_t steps, float* mean_loss);
+/* Gradients of the mean loss of the batch, without an update, into host
+ * arrays of HDCX_NRC_WEIGHT_COUNT and hdcx_nrc_grid_parameter_count floats
+ * (either may be NULL). */
+HDCX_API hdcx_status hdcx_nrc_gradients(hdcx_nrc* cache, const float* queries, const float* targets, uint32_t count,
+                                        float* mlp_gradient, float* grid_gradient);
+/* Host copies of the FP32 parameters (either may be NULL). Setting them
+ * resets the Adam state. */
+HDCX_API hdcx_status hdcx_nrc_get_parameters(hdcx_nrc* cache, float* mlp, float* grid);
+HDCX_API hdcx_status hdcx_nrc_set_parameters(hdcx_nrc* cache, const float* mlp, const float* grid);
 
 #ifdef __cplusplus
 }
