@@ -68,6 +68,19 @@ struct DeviceBuffer {
 
 }  // namespace
 
+struct hdcx_nrc {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    hdcx::nrc::Cache* cache = nullptr;
+    std::string lastError;
+    ~hdcx_nrc()
+    {
+        if (stream) cudaStreamSynchronize(stream);
+        hdcx::nrc::destroy(cache);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
 struct hdcx_tracer {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -91,12 +104,22 @@ struct hdcx_tracer {
     uint64_t xyzSamples = 0;
     hdcx_render_stats stats{};
     cudaEvent_t start = nullptr, stop = nullptr;
+    // Radiance-cache mode (hdcx_set_radiance_cache).
+    hdcx_nrc* radianceCache = nullptr;
+    uint32_t cachePrefix = 2;
+    uint32_t cacheTrainingPaths = 1u << 14;
+    std::vector<DeviceBuffer*> cacheBuffers;
+    CacheDevice cacheDevice;
+    uint64_t cacheCapacity = 0;
+    CacheRun cacheRun;
+    float3 sceneMin{}, sceneScale{};
 
     ~hdcx_tracer()
     {
         if (stream) cudaStreamSynchronize(stream);
         clearScene();
         clearPaths();
+        clearCache();
         if (start) cudaEventDestroy(start);
         if (stop) cudaEventDestroy(stop);
         if (stream) cudaStreamDestroy(stream);
@@ -109,6 +132,21 @@ struct hdcx_tracer {
         freeWideBvh(bvh);
         scene = DeviceScene{};
         geometryReady = false;
+    }
+    void clearCache()
+    {
+        for (DeviceBuffer* b : cacheBuffers) delete b;
+        cacheBuffers.clear();
+        cacheDevice = CacheDevice{};
+        cacheCapacity = 0;
+    }
+    template <typename T>
+    T* cacheAlloc(size_t count)
+    {
+        auto* b = new DeviceBuffer();
+        cacheBuffers.push_back(b);
+        b->allocate(count * sizeof(T));
+        return b->as<T>();
     }
     void clearPaths()
     {
@@ -274,6 +312,28 @@ void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
     s.opaque = d.opaque ? 1u : 0u;
     s.fullShading = needsFullShading(d) ? 1u : 0u;
     s.hasMeshLights = (d.triangleCount() > 0 && d.emissive[(size_t(d.triangleCount()) - 1) * 4u] > 0.0F) ? 1u : 0u;
+    {
+        // Scene box (padded by 0.1% per side) for the radiance-cache positions.
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (size_t v = 0; v < d.vertices.size() / 4; ++v) {
+            for (int a = 0; a < 3; ++a) {
+                const float x = d.vertices[v * 4 + a];
+                if (std::isfinite(x)) {
+                    lo[a] = std::min(lo[a], x);
+                    hi[a] = std::max(hi[a], x);
+                }
+            }
+        }
+        float extent[3];
+        for (int a = 0; a < 3; ++a) {
+            if (!(hi[a] >= lo[a])) lo[a] = hi[a] = 0.0F;
+            extent[a] = std::max(hi[a] - lo[a], 1e-6F);
+            lo[a] -= 1e-3F * extent[a];
+            extent[a] *= 1.002F;
+        }
+        t->sceneMin = make_float3(lo[0], lo[1], lo[2]);
+        t->sceneScale = make_float3(1.0F / extent[0], 1.0F / extent[1], 1.0F / extent[2]);
+    }
     // Padding floor of the BVH quantisation: the scene's coordinate scale.
     float scale = 0.0F;
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -360,6 +420,30 @@ void ensurePaths(hdcx_tracer* t, uint64_t needed, uint32_t shadowPerPath, uint64
     p.shadowInfo = t->pathAlloc<uint32_t>(ns);
     p.counters = t->pathAlloc<uint32_t>(4);
     p.stats = t->pathAlloc<unsigned long long>(8);
+}
+
+// Buffers of the radiance-cache mode for waves of up to `capacity` paths.
+void ensureCacheBuffers(hdcx_tracer* t, uint64_t capacity)
+{
+    const uint64_t trainCapacity = 2ull * t->cacheTrainingPaths;
+    if (t->cacheCapacity >= capacity && t->cacheDevice.trainCapacity == trainCapacity && t->cacheDevice.queries) return;
+    check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+    t->clearCache();
+    CacheDevice& c = t->cacheDevice;
+    const uint64_t records = trainCapacity * kCacheMaxVertices;
+    c.queries = t->cacheAlloc<float>(capacity * 12u);
+    c.querySlot = t->cacheAlloc<uint32_t>(capacity);
+    c.predictions = t->cacheAlloc<float>(capacity);
+    c.trainIndex = t->cacheAlloc<uint32_t>(capacity);
+    c.trainSlot = t->cacheAlloc<uint32_t>(trainCapacity);
+    c.trainVertices = t->cacheAlloc<uint32_t>(trainCapacity);
+    c.trainRecords = t->cacheAlloc<float>(records * 12u);
+    c.trainState = t->cacheAlloc<float2>(records);
+    c.sampleQueries = t->cacheAlloc<float>(records * 12u);
+    c.sampleTargets = t->cacheAlloc<float>(records);
+    c.counters = t->cacheAlloc<uint32_t>(4);
+    c.trainCapacity = static_cast<uint32_t>(trainCapacity);
+    t->cacheCapacity = capacity;
 }
 
 FrameConst makeFrame(const hdcx_tracer* t, const hdcx_camera& c, uint32_t w, uint32_t h, uint32_t sampleIndex,
@@ -625,6 +709,19 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
                                                             : (t->scene.hasMeshLights ? 2u : 3u);
     ensurePaths(t, call.pathsNeeded, std::max(shadowPerPath, 3u), waveCap);
     check(cudaMemsetAsync(t->paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
+    t->paths.cache = CacheDevice{};
+    if (t->radianceCache) {
+        ensureCacheBuffers(t, t->paths.capacity);
+        CacheDevice c = t->cacheDevice;
+        c.enabled = 1u;
+        c.prefixBounces = t->cachePrefix;
+        const double wave = static_cast<double>(std::min<uint64_t>(call.pathsNeeded, t->paths.capacity));
+        c.trainThreshold = static_cast<uint32_t>(std::min(4294967295.0, double(t->cacheTrainingPaths) / wave * 4294967296.0));
+        c.sceneMin = t->sceneMin;
+        c.sceneScale = t->sceneScale;
+        t->paths.cache = c;
+        t->cacheRun.cache = t->radianceCache->cache;
+    }
     call.stageTiming = allowStageTiming && (t->profiling & HDCX_PROFILE_STAGE_TIMES) != 0u;
     call.counting = (t->profiling & HDCX_PROFILE_COUNT_TRAVERSAL) != 0u;
     call.active = true;
@@ -634,7 +731,7 @@ void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut)
 {
     check(cudaEventRecord(t->start, t->stream), "cudaEventRecord");
     renderFrame(t->scene, call.frame, t->paths, t->fb, t->stream, call.stageTiming ? &call.times : nullptr,
-                call.counting, &call.launches);
+                call.counting, &call.launches, t->radianceCache ? &t->cacheRun : nullptr);
     check(cudaEventRecord(t->stop, t->stream), "cudaEventRecord");
     if (rgbaOut) {
         check(cudaMemcpyAsync(rgbaOut, t->fb.rgba, size_t(call.frame.width) * call.frame.height * sizeof(float4),
@@ -870,19 +967,6 @@ HDCX_API hdcx_status hdcx_get_stats(const hdcx_tracer* t, hdcx_render_stats* sta
 // ---------------------------------------------------------------------------
 }  // extern "C"
 
-struct hdcx_nrc {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    hdcx::nrc::Cache* cache = nullptr;
-    std::string lastError;
-    ~hdcx_nrc()
-    {
-        if (stream) cudaStreamSynchronize(stream);
-        hdcx::nrc::destroy(cache);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
 namespace {
 
 template <typename F>
@@ -1012,6 +1096,36 @@ HDCX_API hdcx_status hdcx_nrc_set_parameters(hdcx_nrc* n, const float* mlp, cons
 {
     if (!n || !mlp || !grid) return HDCX_ERROR_INVALID_ARGUMENT;
     return nrcGuarded(n, [&] { hdcx::nrc::setParameters(n->cache, mlp, grid); });
+}
+
+HDCX_API hdcx_status hdcx_set_radiance_cache(hdcx_tracer* t, hdcx_nrc* cache, uint32_t prefixBounces,
+                                             uint32_t trainingPaths, uint32_t trainSteps)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (!cache) {
+        t->radianceCache = nullptr;
+        return HDCX_OK;
+    }
+    if (cache->device != t->device) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "the radiance cache lives on another device");
+    if (prefixBounces < 1 || prefixBounces >= HDCX_MAX_PATH_BOUNCES)
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "prefix_bounces must be in [1, 11]");
+    if (trainingPaths < 128 || trainingPaths > (1u << 20))
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "training_paths must be in [128, 2^20]");
+    t->radianceCache = cache;
+    t->cachePrefix = prefixBounces;
+    t->cacheTrainingPaths = trainingPaths;
+    t->cacheRun = CacheRun{};
+    t->cacheRun.trainSteps = std::max(trainSteps, 1u);
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_get_radiance_cache_stats(const hdcx_tracer* t, uint64_t* queries, uint64_t* samples, float* loss)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (queries) *queries = t->cacheRun.queries;
+    if (samples) *samples = t->cacheRun.samples;
+    if (loss) *loss = t->cacheRun.lastLoss;
+    return HDCX_OK;
 }
 
 }  // extern "C"

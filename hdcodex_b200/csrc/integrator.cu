@@ -18,6 +18,7 @@
 // Queues are compacted with warp-aggregated atomics; kernels loop over the
 // device-side queue length, so a frame needs no host round trip.
 #include "integrator.h"
+#include "nrc.h"
 
 #include <cooperative_groups.h>
 
@@ -44,6 +45,7 @@ namespace {
 constexpr uint32_t kFlagEnvironmentOnMiss = 1u;
 constexpr uint32_t kFlagPreviousWasDelta = 2u;
 constexpr uint32_t kFlagInsideMedium = 4u;
+constexpr uint32_t kFlagTraining = 8u;  // radiance-cache mode: a full-length training path
 
 enum ShadowKind : uint32_t {
     kShadowAnalytic = 0,
@@ -107,7 +109,23 @@ __global__ void generateKernel(FrameConst f, WaveDesc w, PathBuffers p)
     p.radiance[slot] = 0.0f;
     p.rayOrigin[slot] = make_float4(f.origin.x, f.origin.y, f.origin.z, 0.0f);
     p.rayDirection[slot] = make_float4(direction.x, direction.y, direction.z, 0.0f);
-    p.flags[slot] = kFlagEnvironmentOnMiss | kFlagPreviousWasDelta;
+    uint32_t flags = kFlagEnvironmentOnMiss | kFlagPreviousWasDelta;
+    if (p.cache.enabled) {
+        // Training paths: a deterministic subset chosen by the path identity.
+        const uint32_t key = hashState(pixel ^ hashState(sampleNumber * 0x9e3779b9u + lane * 0x85ebca6bu + 0x27d4eb2fu));
+        if (key < p.cache.trainThreshold) {
+            const uint32_t t = atomicAdd(p.cache.counters + 1, 1u);
+            if (t < p.cache.trainCapacity) {
+                flags |= kFlagTraining;
+                p.cache.trainIndex[slot] = t;
+                p.cache.trainSlot[t] = slot;
+                p.cache.trainVertices[t] = 0u;
+                for (uint32_t b = 0; b < kCacheMaxVertices; ++b)
+                    p.cache.trainState[t * kCacheMaxVertices + b] = make_float2(-1.0f, 0.0f);
+            }
+        }
+    }
+    p.flags[slot] = flags;
     p.previousPdf[slot] = make_float2(0.0f, 0.0f);
     p.medium[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     p.contributionValid[slot] = 0;
@@ -268,7 +286,9 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
 // kLit: the scene has analytic or dome lights and no emissive triangles, so
 // neither the fallback sun and sky (:1593-1668) nor emissive-triangle
 // sampling (:1670-1731) can run; both are compiled out.
-template <bool kFull, bool kLit>
+// kCache: radiance-cache mode (PathBuffers::cache): queries and training
+// records at surface vertices; the plain kernels compile without it.
+template <bool kFull, bool kLit, bool kCache>
 __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce,
                                                    const uint32_t* queue, const uint32_t* count, uint32_t* nextQueue,
                                                    uint32_t* nextCount)
@@ -380,6 +400,37 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
             if (kFull) normal = applyNormalMap(s, material->textureIndices1.y, material->coatWeightRoughnessIor.w > 0.5f,
                                     material->subsurfaceWeightScale.w, surfaceUv, normal, p0, p1, p2, uv0, uv1, uv2);
             const float3 tangent = surfaceTangent(normal, p0, p1, p2, uv0, uv1, uv2);
+            if (kCache) {
+                const bool training = (flags & kFlagTraining) != 0u;
+                if (training || bounce >= p.cache.prefixBounces) {
+                    const float3 qp = (hit - p.cache.sceneMin) * p.cache.sceneScale;
+                    const float4 q0 = make_float4(qp.x, qp.y, qp.z, -rayDirection.x);
+                    const float4 q1 = make_float4(-rayDirection.y, -rayDirection.z, normal.x, normal.y);
+                    const float4 q2 = make_float4(normal.z, roughness.x, (wavelength - 380.0f) / 400.0f, 0.0f);
+                    if (training) {
+                        if (bounce < kCacheMaxVertices) {
+                            const uint32_t r = p.cache.trainIndex[slot] * kCacheMaxVertices + bounce;
+                            float4* rec = reinterpret_cast<float4*>(p.cache.trainRecords) + r * 3u;
+                            rec[0] = q0;
+                            rec[1] = q1;
+                            rec[2] = q2;
+                            p.cache.trainState[r] = make_float2(throughput, radiance);
+                            p.cache.trainVertices[p.cache.trainIndex[slot]] = bounce + 1u;
+                        }
+                    } else {
+                        // The cache replaces everything from this vertex on.
+                        const uint32_t j = appendIndex(p.cache.counters + 0);
+                        float4* rec = reinterpret_cast<float4*>(p.cache.queries) + static_cast<size_t>(j) * 3u;
+                        rec[0] = q0;
+                        rec[1] = q1;
+                        rec[2] = q2;
+                        p.cache.querySlot[j] = slot;
+                        p.throughput[slot] = throughput;
+                        alive = false;
+                        break;
+                    }
+                }
+            }
             const float3 emissionRgb = surfaceEmissionRgb(s, primitive, surfaceUv);
             const float emission = illuminantSpectrum(emissionRgb, spec);
             float emissionMisWeight = 1.0f;
@@ -821,7 +872,7 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
         p.rng[slot] = rng;
         p.throughput[slot] = throughput;
         p.flags[slot] = (environmentOnMiss ? kFlagEnvironmentOnMiss : 0u) | (previousWasDelta ? kFlagPreviousWasDelta : 0u) |
-                        (insideMedium ? kFlagInsideMedium : 0u);
+                        (insideMedium ? kFlagInsideMedium : 0u) | (kCache ? (flags & kFlagTraining) : 0u);
         p.previousPdf[slot] = make_float2(previousBsdfPdf, previousEnvironmentLightPdf);
         p.medium[slot] = make_float4(mediumAbsorption, mediumScattering, mediumAnisotropy, 0.0f);
         p.rayOrigin[slot] = make_float4(rayOrigin.x, rayOrigin.y, rayOrigin.z, 0.0f);
@@ -960,6 +1011,46 @@ __global__ void primaryKernel(DeviceScene s, FrameConst f, uint32_t sampleNumber
     distances[pixel] = found ? h.t : 0.0f;
 }
 
+// ---------------------------------------------------------------------------
+// radiance-cache mode: predictions into the terminated paths, suffix targets
+// of the training paths
+// ---------------------------------------------------------------------------
+__global__ void cacheApplyKernel(PathBuffers p)
+{
+    const uint32_t n = p.cache.counters[0];
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t slot = p.cache.querySlot[j];
+        p.radiance[slot] += p.throughput[slot] * fmaxf(p.cache.predictions[j], 0.0f);
+    }
+}
+
+__global__ void cacheTargetsKernel(PathBuffers p)
+{
+    const uint32_t n = min(p.cache.counters[1], p.cache.trainCapacity);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t slot = p.cache.trainSlot[t];
+        float total = p.radiance[slot];
+        for (uint32_t k = 0; k < 3u; ++k) {
+            if (p.contributionValid[k * p.capacity + slot]) total += p.contribution[k * p.capacity + slot];
+        }
+        const uint32_t vertices = min(p.cache.trainVertices[t], kCacheMaxVertices);
+        for (uint32_t b = 0; b < vertices; ++b) {
+            const uint32_t r = t * kCacheMaxVertices + b;
+            const float2 st = p.cache.trainState[r];
+            if (!(st.x > 0.0f)) continue;
+            const float target = (total - st.y) / st.x;
+            if (!(target >= 0.0f && target < 3.0e38f)) continue;
+            const uint32_t j = atomicAdd(p.cache.counters + 2, 1u);
+            const float4* src = reinterpret_cast<const float4*>(p.cache.trainRecords) + r * 3u;
+            float4* dst = reinterpret_cast<float4*>(p.cache.sampleQueries) + static_cast<size_t>(j) * 3u;
+            dst[0] = src[0];
+            dst[1] = src[1];
+            dst[2] = src[2];
+            p.cache.sampleTargets[j] = target;
+        }
+    }
+}
+
 int gridFor(uint32_t maxItems, int perSm)
 {
     int device = 0, sms = 148;
@@ -1003,9 +1094,25 @@ void uploadSrgbTable(const float* table256, cudaStream_t stream)
     CUDA_OK(cudaMemcpyToSymbolAsync(cSrgbToLinear, table256, 256 * sizeof(float), 0, cudaMemcpyHostToDevice, stream));
 }
 
-void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, FrameBuffers& fb,
-                 cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches)
+template <bool kCache>
+void launchShade(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, uint32_t bounce, const uint32_t* inQueue,
+                 const uint32_t* inCount, uint32_t* outQueue, uint32_t* outCount, int grid, cudaStream_t stream)
 {
+    const bool lit = scene.lightCount > 0u && !scene.hasMeshLights;
+    if (scene.fullShading) {
+        if (lit) shadeKernel<true, true, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+        else shadeKernel<true, false, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+    } else {
+        if (lit) shadeKernel<false, true, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+        else shadeKernel<false, false, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+    }
+}
+
+void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, FrameBuffers& fb,
+                 cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches, CacheRun* cacheRun)
+{
+    const bool cacheMode = cacheRun != nullptr && cacheRun->cache != nullptr && paths.cache.enabled != 0u;
+    if (!cacheMode) paths.cache.enabled = 0u;
     uint64_t launched = 0;
     const uint32_t pixels = frame.width * frame.height;
     CUDA_OK(cudaMemsetAsync(fb.batch, 0, sizeof(float4) * pixels, stream));
@@ -1029,6 +1136,7 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
         events.push_back(e);
     };
     for (const WaveDesc& w : waves) {
+        if (cacheMode) CUDA_OK(cudaMemsetAsync(paths.cache.counters, 0, 3 * sizeof(uint32_t), stream));
         generateKernel<<<(w.count + 255u) / 256u, 256, 0, stream>>>(frame, w, paths);
         CUDA_OK(cudaGetLastError());
         for (uint32_t bounce = 0; bounce < frame.maxBounces; ++bounce) {
@@ -1049,14 +1157,8 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
             CUDA_OK(cudaMemsetAsync(outCount, 0, sizeof(uint32_t), stream));
             CUDA_OK(cudaMemsetAsync(paths.counters + 2, 0, sizeof(uint32_t), stream));
             timed(1, [&] {
-                const bool lit = scene.lightCount > 0u && !scene.hasMeshLights;
-                if (scene.fullShading) {
-                    if (lit) shadeKernel<true, true><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
-                    else shadeKernel<true, false><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
-                } else {
-                    if (lit) shadeKernel<false, true><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
-                    else shadeKernel<false, false><<<shadeGrid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
-                }
+                if (cacheMode) launchShade<true>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount, shadeGrid, stream);
+                else launchShade<false>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount, shadeGrid, stream);
             });
             CUDA_OK(cudaGetLastError());
             timed(2, [&] {
@@ -1070,6 +1172,26 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
             });
             CUDA_OK(cudaGetLastError());
             launched += 3;
+        }
+        if (cacheMode) {
+            // Predictions for the terminated paths, then one training round on
+            // this wave's suffix samples (the next wave sees the update).
+            uint32_t counts[3] = {0, 0, 0};
+            CUDA_OK(cudaMemcpyAsync(counts, paths.cache.counters, sizeof counts, cudaMemcpyDeviceToHost, stream));
+            CUDA_OK(cudaStreamSynchronize(stream));
+            nrc::query(cacheRun->cache, paths.cache.queries, counts[0], paths.cache.predictions, stream);
+            cacheApplyKernel<<<gridFor(std::max(counts[0], 1u), 8), 128, 0, stream>>>(paths);
+            cacheTargetsKernel<<<gridFor(std::max(std::min(counts[1], paths.cache.trainCapacity), 1u), 8), 128, 0, stream>>>(paths);
+            CUDA_OK(cudaGetLastError());
+            CUDA_OK(cudaMemcpyAsync(counts, paths.cache.counters, sizeof counts, cudaMemcpyDeviceToHost, stream));
+            CUDA_OK(cudaStreamSynchronize(stream));
+            cacheRun->queries += counts[0];
+            cacheRun->samples += counts[2];
+            if (counts[2] > 0u) {
+                cacheRun->lastLoss = nrc::train(cacheRun->cache, paths.cache.sampleQueries, paths.cache.sampleTargets, counts[2],
+                                                cacheRun->trainSteps, stream);
+            }
+            launched += 2;
         }
         launched += 2;
         accumulateKernel<<<(w.pixels + 255u) / 256u, 256, 0, stream>>>(frame, w, paths, fb.batch, fb.batchXyz);

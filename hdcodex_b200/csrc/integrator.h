@@ -8,6 +8,32 @@
 
 namespace hdcx {
 
+// Radiance-cache mode (device side): paths that are not training paths stop
+// at the first surface vertex after `prefixBounces` bounces and record a cache
+// query there; a sparse, deterministic set of training paths runs the full
+// bounce budget and records every vertex (query features, throughput and
+// radiance on arrival) for the suffix targets.
+constexpr uint32_t kCacheMaxVertices = 12;  // HDCX_MAX_PATH_BOUNCES
+struct CacheDevice {
+    uint32_t enabled = 0;
+    uint32_t prefixBounces = 2;
+    uint32_t trainThreshold = 0;  // a path trains when its identity hash < this
+    uint32_t trainCapacity = 0;   // training paths per wave
+    float3 sceneMin{};            // query positions are (hit - sceneMin) * sceneScale, in [0, 1]
+    float3 sceneScale{};
+    float* queries = nullptr;          // wave capacity x 12: termination queries
+    uint32_t* querySlot = nullptr;     // path slot of each query
+    uint32_t* trainIndex = nullptr;    // per path: its training record block
+    uint32_t* trainSlot = nullptr;     // per training path: its path slot
+    uint32_t* trainVertices = nullptr; // per training path: vertices recorded
+    float* trainRecords = nullptr;     // trainCapacity x kCacheMaxVertices x 12
+    float2* trainState = nullptr;      // (throughput, radiance) on arrival at each recorded vertex
+    float* sampleQueries = nullptr;    // compacted training batch: trainCapacity x kCacheMaxVertices x 12
+    float* sampleTargets = nullptr;
+    float* predictions = nullptr;      // wave capacity
+    uint32_t* counters = nullptr;      // [0] queries, [1] training paths, [2] training samples
+};
+
 // Device buffers of one wave of paths (structure of arrays, 16-byte records).
 struct PathBuffers {
     uint64_t capacity = 0;          // paths per wave
@@ -35,6 +61,7 @@ struct PathBuffers {
     // extension, shadow, subsurface rays; extension node visits and triangle
     // tests; shadow node visits and triangle tests (counting mode)
     unsigned long long* stats = nullptr;
+    CacheDevice cache;
 };
 
 // Per-pixel accumulation buffers of the current output size.
@@ -58,8 +85,21 @@ void uploadSrgbTable(const float* table256, cudaStream_t stream);
 // `timing` non-null records per-stage device times with CUDA events.
 // countTraversal selects the traversal kernels that count node visits and
 // triangle tests (into paths.stats[3..6]); *launches gets the kernel count.
+namespace nrc {
+struct Cache;
+}
+
+// Host side of the radiance-cache mode: the cache and its training schedule.
+struct CacheRun {
+    nrc::Cache* cache = nullptr;
+    uint32_t trainSteps = 1;  // Adam steps per wave on the wave's suffix samples
+    float lastLoss = 0.0f;
+    uint64_t queries = 0, samples = 0;
+};
+
 void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, FrameBuffers& fb,
-                 cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches);
+                 cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches,
+                 CacheRun* cacheRun = nullptr);
 
 // Primary-hit ids and distances of sample `sampleNumber` (device outputs).
 void tracePrimary(const DeviceScene& scene, const FrameConst& frame, uint32_t sampleNumber, uint32_t* primitives,

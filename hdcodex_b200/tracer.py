@@ -59,6 +59,8 @@ SIGNATURES = {
                                      C.c_uint32, _P, C.POINTER(C.c_int32)]),
     "hdcx_render_batch": (C.c_int, [C.POINTER(_abi.BatchJob), C.c_uint32, C.c_uint64]),
     "hdcx_read_rgba": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint64]),
+    "hdcx_set_radiance_cache": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32]),
+    "hdcx_get_radiance_cache_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
     "hdcx_nrc_defaults": (None, [C.POINTER(_abi.NrcConfig)]),
     "hdcx_nrc_create": (C.c_int, [C.c_int32, C.POINTER(_abi.NrcConfig), C.POINTER(C.c_void_p)]),
     "hdcx_nrc_destroy": (None, [_P]),
@@ -205,6 +207,17 @@ class PathTracer:
                                              prims.ctypes.data_as(C.POINTER(C.c_uint32)),
                                              dist.ctypes.data_as(C.POINTER(C.c_float))), "trace_primary")
         return prims, dist
+
+    def set_radiance_cache(self, cache, prefix_bounces=2, training_paths=1 << 14, train_steps=1):
+        """Attach a RadianceCache (None detaches it)."""
+        self._check(lib().hdcx_set_radiance_cache(self._h, cache.handle if cache is not None else None, prefix_bounces,
+                                                  training_paths, train_steps), "set_radiance_cache")
+
+    def radiance_cache_stats(self) -> dict:
+        q, n, loss = C.c_uint64(0), C.c_uint64(0), C.c_float(0.0)
+        self._check(lib().hdcx_get_radiance_cache_stats(self._h, C.byref(q), C.byref(n), C.byref(loss)),
+                    "get_radiance_cache_stats")
+        return {"queries": int(q.value), "samples": int(n.value), "last_loss": float(loss.value)}
 
     def stats(self) -> dict:
         st = _abi.RenderStats()

@@ -545,6 +545,21 @@ HDCX_API hdcx_status hdcx_nrc_gradients(hdcx_nrc* cache, const float* queries, c
 HDCX_API hdcx_status hdcx_nrc_get_parameters(hdcx_nrc* cache, float* mlp, float* grid);
 HDCX_API hdcx_status hdcx_nrc_set_parameters(hdcx_nrc* cache, const float* mlp, const float* grid);
 
+/* Renders of `tracer` use the radiance cache (NULL: the plain integrator).
+ * Paths stop at the first surface vertex after `prefix_bounces` bounces and
+ * add throughput x the cache's prediction there; about `training_paths`
+ * paths per wave (a deterministic subset by path identity) run the full
+ * bounce budget, and the radiance each gathered after every vertex trains the
+ * cache (`train_steps` Adam steps per wave) before the next wave. The cache
+ * must live on the tracer's device; it is not owned by the tracer. Renders in
+ * this mode synchronise with the host once per wave. */
+HDCX_API hdcx_status hdcx_set_radiance_cache(hdcx_tracer* tracer, hdcx_nrc* cache, uint32_t prefix_bounces,
+                                             uint32_t training_paths, uint32_t train_steps);
+/* Totals since the cache was attached: queries answered, training samples
+ * used, and the mean loss of the last training step. */
+HDCX_API hdcx_status hdcx_get_radiance_cache_stats(const hdcx_tracer* tracer, uint64_t* queries, uint64_t* samples,
+                                                   float* last_loss);
+
 #ifdef __cplusplus
 }
 #endif
