@@ -50,11 +50,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hdcx", choices=["hdcx", "reference"])
-    ap.add_argument("--workload", default="heavy", choices=["heavy", "box", "stress", "batch"],
+    ap.add_argument("--workload", default="heavy", choices=["heavy", "box", "stress", "batch", "nrc"],
                     help="heavy: 1.0M triangles, 1920x1080, 64 spp (the headline); box: 34-triangle closed box, "
                          "256x256, 16 spp; stress: 200k-triangle spectral stress scene, 1280x720, 256 spp; "
-                         "batch: --jobs scenes of 10k-2M triangles rendered by hdcx_render_batch")
+                         "batch: --jobs scenes of 10k-2M triangles rendered by hdcx_render_batch; "
+                         "nrc: time to a relative XYZ RMSE on the stress scene, radiance cache vs plain")
     ap.add_argument("--jobs", type=int, default=64, help="jobs of the batch workload")
+    ap.add_argument("--ref-spp", type=int, default=4096, help="nrc workload: spp of the FP64 reference")
+    ap.add_argument("--target-rmse", type=float, default=0.02, help="nrc workload: relative XYZ RMSE to reach")
+    ap.add_argument("--chunk-spp", type=int, default=4, help="nrc workload: spp per progressive render call")
+    ap.add_argument("--max-spp", type=int, default=4096, help="nrc workload: give up after this many spp")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -347,6 +352,90 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+def run_nrc(args):
+    """Time to --target-rmse relative XYZ RMSE (||X - X_ref|| / ||X_ref|| over
+    all pixels and X, Y, Z) on the spectral-stress scene, the plain 8-bounce
+    integrator against the radiance-cache form (2-bounce prefix, online
+    training); X_ref = the plain integrator's FP64 XYZ at --ref-spp. Both arms
+    render progressively, --chunk-spp samples per call; the clock covers the
+    render calls (training included), not the error evaluation."""
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(0)
+    from hdcodex_b200 import PathTracer, RadianceCache, workloads
+
+    wl = workloads.spectral_stress()
+    if args.width or args.height:
+        wl = workloads.spectral_stress(width=args.width or wl.width, height=args.height or wl.height)
+    w, h = wl.width, wl.height
+
+    def xyz_mean(t):
+        total, samples = t.read_xyz()
+        return total / max(samples, 1)
+
+    with PathTracer(0) as t:
+        t.set_scene(wl.scene)
+        t0 = time.perf_counter()
+        done = 0
+        # Sample indices disjoint from the measured arms' (which start at 0).
+        first = 1 << 22
+        half = None
+        while done < args.ref_spp:
+            k = min(256, args.ref_spp - done)
+            t.render_device(wl.camera, w, h, first + done, wl.max_bounces, k)
+            done += k
+            if half is None and done >= args.ref_spp // 2:
+                half = t.read_xyz()
+        ref_s = time.perf_counter() - t0
+        total = t.read_xyz()
+        reference = total[0] / total[1]
+    ref_norm = float(np.linalg.norm(reference))
+    # Noise floor of the reference: its two halves differ by about twice its own error.
+    second = (total[0] - half[0]) / (total[1] - half[1])
+    reference_noise = 0.5 * float(np.linalg.norm(half[0] / half[1] - second)) / ref_norm
+
+    def converge(cache):
+        curve = []
+        with PathTracer(0) as t:
+            t.set_scene(wl.scene)
+            if cache is not None:
+                t.set_radiance_cache(cache, prefix_bounces=2, training_paths=1 << 14, train_steps=4)
+            elapsed, spp, err = 0.0, 0, float("inf")
+            torch.cuda.synchronize()
+            while spp < args.max_spp:
+                t0 = time.perf_counter()
+                t.render_device(wl.camera, w, h, spp, wl.max_bounces, args.chunk_spp)
+                torch.cuda.synchronize()
+                elapsed += time.perf_counter() - t0
+                spp += args.chunk_spp
+                err = float(np.linalg.norm(xyz_mean(t) - reference)) / ref_norm
+                curve.append((spp, round(elapsed, 4), round(err, 5)))
+                if err < args.target_rmse:
+                    break
+            stats = t.radiance_cache_stats() if cache is not None else None
+        reached = err < args.target_rmse
+        return {"seconds": elapsed if reached else None, "spp": spp, "final_rel_rmse": err, "reached": reached,
+                "curve": curve[:: max(1, len(curve) // 24)] + curve[-1:], "cache_stats": stats}
+
+    plain = converge(None)
+    with RadianceCache(0) as cache:
+        cached = converge(cache)
+    ratio = (cached["seconds"] / plain["seconds"]) if (plain["seconds"] and cached["seconds"]) else None
+    print(json.dumps({
+        "metric": "time to 2% relative XYZ RMSE, radiance cache vs plain", "unit": "s",
+        "value": cached["seconds"], "plain_seconds": plain["seconds"], "cache_over_plain": ratio,
+        "higher_is_better": False, "n_gpus": 1, "dtype": "f32 path tracing, bf16 tensor-core MLP",
+        "data": "synthetic",
+        "config": {"workload": wl.name, "width": w, "height": h, "reference_spp": args.ref_spp,
+                   "reference_seconds": ref_s, "reference_rel_noise": reference_noise,
+                   "target_rel_rmse": args.target_rmse, "chunk_spp": args.chunk_spp,
+                   "cache": "16 levels x 2 features, 2^19 entries/level fp16; MLP 64x4 ReLU bf16; prefix 2 bounces; "
+                            "2^14 training paths per wave, 4 Adam steps per wave"},
+        "plain": plain, "cache": cached,
+    }), flush=True)
+
+
 def run_hdcx(args):
     import numpy as np
     import torch
@@ -485,6 +574,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "nrc":
+        run_nrc(args)
     else:
         run_hdcx(args)
 

@@ -148,8 +148,8 @@ def _noise3(p: np.ndarray, rng: np.random.Generator, octaves: int = 4) -> np.nda
     return out
 
 
-def _dome_texture(width, height, seed) -> np.ndarray:
-    """Lat-long RGBA32F dome: log-normal luminance (sigma 2) + 3 Gaussian hotspots."""
+def _dome_texture(width, height, seed, hotspots=3) -> np.ndarray:
+    """Lat-long RGBA32F dome: log-normal luminance (sigma 2) + `hotspots` Gaussian hotspots."""
     rng = np.random.default_rng(seed)
     # Smooth log-normal field: low-resolution Gaussian noise upsampled.
     lw, lh = 64, 32
@@ -169,7 +169,7 @@ def _dome_texture(width, height, seed) -> np.ndarray:
     v = (np.arange(height) + 0.5) / height
     u = (np.arange(width) + 0.5) / width
     uu, vv = np.meshgrid(u, v)
-    for _ in range(3):
+    for _ in range(hotspots):
         cu, cv = rng.uniform(0.0, 1.0), rng.uniform(0.55, 0.9)
         s = rng.uniform(0.01, 0.03)
         du = np.minimum(np.abs(uu - cu), 1.0 - np.abs(uu - cu))
@@ -368,7 +368,9 @@ def spectral_stress(width=1280, height=720, spp=256, max_bounces=8, seed=0, sphe
                               srgb=False, rgba_float=rgba.ravel()))
 
     dw, dh = dome_size
-    dome = _dome_texture(dw, dh, seed + 11) * 0.25
+    # A sky without sun-like hotspots: a hotspot seen through the delta glass
+    # can only be found by BSDF sampling and would dominate the variance.
+    dome = _dome_texture(dw, dh, seed + 11, hotspots=0) * 0.5
     s.textures.append(Texture(id="stressdome#hdr", width=dw, height=dh, rgba_float=dome.ravel()))
     s.lights.append(Light(id="/dome", type=DOME, intensity=1.0, texture="stressdome#hdr", texture_format=LATLONG))
     s.lights.append(Light(id="/key", type=RECT, color=[1.0, 0.9, 0.8], intensity=12.0, normalize=False,
