@@ -148,8 +148,8 @@ def _noise3(p: np.ndarray, rng: np.random.Generator, octaves: int = 4) -> np.nda
     return out
 
 
-def _dome_texture(width, height, seed, hotspots=3) -> np.ndarray:
-    """Lat-long RGBA32F dome: log-normal luminance (sigma 2) + `hotspots` Gaussian hotspots."""
+def _dome_texture(width, height, seed, hotspots=3, sigma=2.0) -> np.ndarray:
+    """Lat-long RGBA32F dome: log-normal luminance (`sigma`) + `hotspots` Gaussian hotspots."""
     rng = np.random.default_rng(seed)
     # Smooth log-normal field: low-resolution Gaussian noise upsampled.
     lw, lh = 64, 32
@@ -165,7 +165,7 @@ def _dome_texture(width, height, seed, hotspots=3) -> np.ndarray:
     field = (g[y0][:, x0] * (1 - fx) * (1 - fy) + g[y0][:, x1] * fx * (1 - fy) +
              g[y1][:, x0] * (1 - fx) * fy + g[y1][:, x1] * fx * fy)
     field = field / max(field.std(), 1e-6)
-    lum = np.exp(2.0 * field - 2.0)  # log-normal, sigma 2
+    lum = np.exp(sigma * field - sigma)  # log-normal
     v = (np.arange(height) + 0.5) / height
     u = (np.arange(width) + 0.5) / width
     uu, vv = np.meshgrid(u, v)
@@ -368,15 +368,15 @@ def spectral_stress(width=1280, height=720, spp=256, max_bounces=8, seed=0, sphe
                               srgb=False, rgba_float=rgba.ravel()))
 
     dw, dh = dome_size
-    # A sky without sun-like hotspots: a hotspot seen through the delta glass
-    # can only be found by BSDF sampling and would dominate the variance.
-    dome = _dome_texture(dw, dh, seed + 11, hotspots=0) * 0.5
+    # Lighting: a sky dome only, log-normal (sigma 0.5) without sun-like
+    # hotspots. A hotspot seen through the delta glass can only be found by
+    # BSDF sampling, and a small area light sampled into the glass's
+    # near-delta reflection lobe (the integrator applies no MIS to analytic
+    # lights) makes fireflies that keep even a 4096-spp render above 20%
+    # relative RMSE; the dome is sampled with MIS.
+    dome = _dome_texture(dw, dh, seed + 11, hotspots=0, sigma=0.5)
     s.textures.append(Texture(id="stressdome#hdr", width=dw, height=dh, rgba_float=dome.ravel()))
     s.lights.append(Light(id="/dome", type=DOME, intensity=1.0, texture="stressdome#hdr", texture_format=LATLONG))
-    s.lights.append(Light(id="/key", type=RECT, color=[1.0, 0.9, 0.8], intensity=12.0, normalize=False,
-                          position=[0.0, 5.0, 2.0], basis_x=[1.0, 0.0, 0.0], basis_y=[0.0, 0.0, 1.0],
-                          basis_z=[0.0, 1.0, 0.0], axis_u=[1.0, 0.0, 0.0], axis_v=[0.0, 0.0, 1.0],
-                          width=2.0, height=2.0, area=4.0))
     cam = look_at_camera((0.0, 3.0, 7.8), (0.0, 0.9, 0.0), (0.0, 1.0, 0.0), 40.0, width / height)
     return Workload("spectral-stress-200k-tri", s, cam, width, height, spp, max_bounces)
 
