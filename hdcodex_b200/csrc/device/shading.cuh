@@ -183,10 +183,13 @@ HDCX_D float2 surfaceTextureCoordinates(const DeviceScene& s, uint32_t primitive
 
 HDCX_D float surfaceOpacity(const DeviceScene& s, uint32_t primitive, float b1, float b2)
 {
-    // :797-803
+    // :797-803. Without an opacity texture the value is the material's
+    // opacity, so the texture coordinates are not needed.
     const GpuMaterial* m = s.materials + __ldg(s.triangleMaterials + primitive);
+    const uint32_t texture = m->textureIndices1.x;
+    if (texture == kMissingTexture) return clampf(m->transmissionOpacityIor.y, 0.0f, 1.0f);
     const float2 uv = surfaceTextureCoordinates(s, primitive, b1, b2);
-    return clampf(sampleMaterialTexture(s, m->textureIndices1.x, uv, f4(m->transmissionOpacityIor.y)).x, 0.0f, 1.0f);
+    return clampf(sampleMaterialTexture(s, texture, uv, f4(m->transmissionOpacityIor.y)).x, 0.0f, 1.0f);
 }
 
 HDCX_D float3 surfaceEmissionRgb(const DeviceScene& s, uint32_t primitive, float2 uv)

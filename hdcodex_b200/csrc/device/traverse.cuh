@@ -186,7 +186,9 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
             if (t == st.bestT && prim > st.bestPrim) continue;
         }
         if (kMode == Accept::Stochastic) {
-            if (!(anyHitThreshold(st.rayRng, prim) <= surfaceOpacity(s, prim, b1, b2))) continue;
+            // The threshold lies in [0, 1]: an opacity of 1 always confirms.
+            const float opacity = surfaceOpacity(s, prim, b1, b2);
+            if (opacity < 1.0f && !(anyHitThreshold(st.rayRng, prim) <= opacity)) continue;
         } else if (kMode == Accept::Threshold) {
             if (!(surfaceOpacity(s, prim, b1, b2) >= 0.5f)) continue;
         }
