@@ -50,11 +50,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hdcx", choices=["hdcx", "reference"])
-    ap.add_argument("--workload", default="heavy", choices=["heavy", "box", "stress", "batch", "nrc"],
+    ap.add_argument("--workload", default="heavy", choices=["heavy", "box", "stress", "batch", "nrc", "cache-kernels"],
                     help="heavy: 1.0M triangles, 1920x1080, 64 spp (the headline); box: 34-triangle closed box, "
                          "256x256, 16 spp; stress: 200k-triangle spectral stress scene, 1280x720, 256 spp; "
                          "batch: --jobs scenes of 10k-2M triangles rendered by hdcx_render_batch; "
-                         "nrc: time to a relative XYZ RMSE on the stress scene, radiance cache vs plain")
+                         "nrc: time to a relative XYZ RMSE on the stress scene, radiance cache vs plain; "
+                         "cache-kernels: radiance-cache query and training throughput")
     ap.add_argument("--jobs", type=int, default=64, help="jobs of the batch workload")
     ap.add_argument("--ref-spp", type=int, default=4096, help="nrc workload: spp of the FP64 reference")
     ap.add_argument("--target-rmse", type=float, default=0.02, help="nrc workload: relative XYZ RMSE to reach")
@@ -436,6 +437,62 @@ def run_nrc(args):
     }), flush=True)
 
 
+def run_cache_kernels(args):
+    """Radiance-cache kernel throughput with the default cache (2^19 entries
+    per level): queries of 2^21 records and training steps on 2^16 samples
+    (Adam over all parameters included), CUDA events on the device, after
+    --warmup untimed calls of each."""
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(0)
+    from hdcodex_b200 import RadianceCache
+
+    rng = np.random.default_rng(0)
+
+    def records(n):
+        q = np.zeros((n, 12), np.float32)
+        q[:, :3] = rng.uniform(0, 1, (n, 3))
+        d = rng.normal(size=(n, 3))
+        q[:, 3:6] = d / np.linalg.norm(d, axis=1, keepdims=True)
+        q[:, 6:9] = -q[:, 3:6]
+        q[:, 9] = rng.uniform(0, 1, n)
+        q[:, 10] = rng.uniform(0, 1, n)
+        return torch.from_numpy(q).cuda()
+
+    nq, nt = 1 << 21, 1 << 16
+    with RadianceCache(0) as cache:
+        train_q, train_y = records(nt), torch.rand(nt, device="cuda") + 0.5
+        query_q, out = records(nq), torch.empty(nq, device="cuda")
+        for _ in range(max(args.warmup, 1)):
+            cache.train(train_q.data_ptr(), train_y.data_ptr(), nt, 1)
+            cache.query(query_q.data_ptr(), nq, out.data_ptr())
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            cache.query(query_q.data_ptr(), nq, out.data_ptr())
+        stop.record()
+        torch.cuda.synchronize()
+        query_ms = start.elapsed_time(stop) / args.steps
+        start.record()
+        for _ in range(args.steps):
+            loss = cache.train(train_q.data_ptr(), train_y.data_ptr(), nt, 1)
+        stop.record()
+        torch.cuda.synchronize()
+        train_ms = start.elapsed_time(stop) / args.steps
+        flops_per_query = 2 * (4 * 64 * 64 + 16 * 64)
+        print(json.dumps({
+            "metric": "radiance-cache queries/s", "value": nq / (query_ms / 1000.0), "unit": "queries/s",
+            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "dtype": "bf16 tensor-core MLP, fp16 hash grid, fp32 Adam", "data": "synthetic",
+            "config": {"workload": "cache-kernels", "queries_per_call": nq, "samples_per_train_step": nt,
+                       "grid_parameters": cache.grid_parameter_count},
+            "query_ms": query_ms, "train_step_ms": train_ms, "last_loss": loss,
+            "mlp_tflops_in_query": nq * flops_per_query / (query_ms / 1000.0) / 1e12,
+        }), flush=True)
+
+
 def run_hdcx(args):
     import numpy as np
     import torch
@@ -576,6 +633,8 @@ def main():
         run_batch(args)
     elif args.workload == "nrc":
         run_nrc(args)
+    elif args.workload == "cache-kernels":
+        run_cache_kernels(args)
     else:
         run_hdcx(args)
 
