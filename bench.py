@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--target-rmse", type=float, default=0.02, help="nrc workload: relative XYZ RMSE to reach")
     ap.add_argument("--chunk-spp", type=int, default=4, help="nrc workload: spp per progressive render call")
     ap.add_argument("--max-spp", type=int, default=4096, help="nrc workload: give up after this many spp")
+    ap.add_argument("--nrc-prefix", default="2,1",
+                    help="nrc workload: comma-separated prefix bounces of the cache arms (the first is `value`)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -396,12 +398,12 @@ def run_nrc(args):
     second = (total[0] - half[0]) / (total[1] - half[1])
     reference_noise = 0.5 * float(np.linalg.norm(half[0] / half[1] - second)) / ref_norm
 
-    def converge(cache):
+    def converge(cache, prefix=2):
         curve = []
         with PathTracer(0) as t:
             t.set_scene(wl.scene)
             if cache is not None:
-                t.set_radiance_cache(cache, prefix_bounces=2, training_paths=1 << 14, train_steps=4)
+                t.set_radiance_cache(cache, prefix_bounces=prefix, training_paths=1 << 14, train_steps=4)
             elapsed, spp, err = 0.0, 0, float("inf")
             torch.cuda.synchronize()
             while spp < args.max_spp:
@@ -420,8 +422,13 @@ def run_nrc(args):
                 "curve": curve[:: max(1, len(curve) // 24)] + curve[-1:], "cache_stats": stats}
 
     plain = converge(None)
-    with RadianceCache(0) as cache:
-        cached = converge(cache)
+    prefixes = [int(x) for x in str(args.nrc_prefix).split(",") if x.strip()]
+    arms = {}
+    for prefix in prefixes:
+        with RadianceCache(0) as cache:
+            arms[prefix] = converge(cache, prefix)
+            arms[prefix]["prefix_bounces"] = prefix
+    cached = arms[prefixes[0]]
     ratio = (cached["seconds"] / plain["seconds"]) if (plain["seconds"] and cached["seconds"]) else None
     print(json.dumps({
         "metric": "time to 2% relative XYZ RMSE, radiance cache vs plain", "unit": "s",
@@ -431,9 +438,13 @@ def run_nrc(args):
         "config": {"workload": wl.name, "width": w, "height": h, "reference_spp": args.ref_spp,
                    "reference_seconds": ref_s, "reference_rel_noise": reference_noise,
                    "target_rel_rmse": args.target_rmse, "chunk_spp": args.chunk_spp,
-                   "cache": "16 levels x 2 features, 2^19 entries/level fp16; MLP 64x4 ReLU bf16; prefix 2 bounces; "
-                            "2^14 training paths per wave, 4 Adam steps per wave"},
+                   "cache": "16 levels x 2 features, 2^19 entries/level fp16; MLP 64x4 ReLU bf16; "
+                            f"prefix {prefixes[0]} bounces; 2^14 training paths per wave, 4 Adam steps per wave"},
         "plain": plain, "cache": cached,
+        "cache_by_prefix": {str(k): {"seconds": v["seconds"], "spp": v["spp"], "final_rel_rmse": v["final_rel_rmse"],
+                                     "ratio_to_plain": (v["seconds"] / plain["seconds"])
+                                     if (v["seconds"] and plain["seconds"]) else None}
+                            for k, v in arms.items()},
     }), flush=True)
 
 
