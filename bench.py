@@ -65,6 +65,9 @@ def parse():
                     help="nrc workload: comma-separated prefix bounces of the cache arms (the first is `value`)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip hdcx_autotune (by default it picks wave and grid sizes before the warm-up; setup, "
+                         "not timed)")
     ap.add_argument("--profile", action="store_true",
                     help="render exactly one frame and exit (for ncu launch lists and captures)")
     ap.add_argument("--width", type=int, default=0, help="override the workload width (profiling only)")
@@ -523,6 +526,7 @@ def run_hdcx(args):
         tracer.close()
         return
     paths_per_step = wl.spectral_paths
+    tuning = tracer.autotune(wl.camera, wl.width, wl.height, wl.max_bounces, wl.spp) if args.autotune else None
 
     from hdcodex_b200.multigpu import sample_range
 
@@ -625,6 +629,7 @@ def run_hdcx(args):
                                   "shadow": shadow_ms / args.steps,
                                   "other": (render_ms - extend_ms - shade_ms - shadow_ms) / args.steps},
             "roofline": roofline,
+            "tuning": tuning if tuning is not None else tracer.tuning(),
             "cpu_baseline": baseline,
             "clocks": clocks,
             "wall_s_timed": wall,

@@ -258,9 +258,22 @@ class BatchJob(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    """hdcx_tuning."""
+    _fields_ = [
+        ("wave_paths", C.c_uint64),
+        ("trace_blocks_per_sm", C.c_uint32),
+        ("shade_blocks_per_sm", C.c_uint32),
+        ("milliseconds", C.c_double),
+        ("default_milliseconds", C.c_double),
+        ("candidates", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
 STRUCTS_IN_ABI_ORDER = [
     Camera, MeshDesc, MaterialDesc, TextureDesc, LightDesc, SceneDesc, PackedTexture, PackedScene,
-    RenderStats, BatchJob, NrcConfig,
+    RenderStats, BatchJob, NrcConfig, Tuning,
 ]
 
 GPU_MATERIAL_BYTES = 368

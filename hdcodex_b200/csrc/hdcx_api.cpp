@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -90,6 +91,8 @@ struct hdcx_tracer {
     bool fallbackAxisInitialized = false;
     bool fallbackZUp = false;
     uint64_t wavePaths = 0;  // 0 = automatic
+    uint32_t traceBlocksPerSm = 16;
+    uint32_t shadeBlocksPerSm = 8;
     uint32_t profiling = 0;  // HDCX_PROFILE_* bits
     // Scene.
     std::vector<DeviceBuffer*> sceneBuffers;
@@ -474,7 +477,7 @@ HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity)
     const uint64_t all[] = {sizeof(hdcx_camera),         sizeof(hdcx_mesh_desc),  sizeof(hdcx_material_desc),
                             sizeof(hdcx_texture_desc),   sizeof(hdcx_light_desc), sizeof(hdcx_scene_desc),
                             sizeof(hdcx_packed_texture), sizeof(hdcx_packed_scene), sizeof(hdcx_render_stats),
-                            sizeof(hdcx_batch_job), sizeof(hdcx_nrc_config)};
+                            sizeof(hdcx_batch_job), sizeof(hdcx_nrc_config), sizeof(hdcx_tuning)};
     const uint32_t n = static_cast<uint32_t>(sizeof(all) / sizeof(all[0]));
     for (uint32_t i = 0; i < std::min(n, capacity); ++i) sizes[i] = all[i];
     return n;
@@ -708,6 +711,8 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
     const uint32_t shadowPerPath = t->scene.lightCount > 0u ? (t->scene.hasMeshLights ? 2u : 1u)
                                                             : (t->scene.hasMeshLights ? 2u : 3u);
     ensurePaths(t, call.pathsNeeded, std::max(shadowPerPath, 3u), waveCap);
+    t->paths.traceBlocksPerSm = t->traceBlocksPerSm;
+    t->paths.shadeBlocksPerSm = t->shadeBlocksPerSm;
     check(cudaMemsetAsync(t->paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
     t->paths.cache = CacheDevice{};
     if (t->radianceCache) {
@@ -1096,6 +1101,125 @@ HDCX_API hdcx_status hdcx_nrc_set_parameters(hdcx_nrc* n, const float* mlp, cons
 {
     if (!n || !mlp || !grid) return HDCX_ERROR_INVALID_ARGUMENT;
     return nrcGuarded(n, [&] { hdcx::nrc::setParameters(n->cache, mlp, grid); });
+}
+
+HDCX_API hdcx_status hdcx_get_tuning(const hdcx_tracer* t, hdcx_tuning* out)
+{
+    if (!t || !out) return HDCX_ERROR_INVALID_ARGUMENT;
+    *out = hdcx_tuning{};
+    out->wave_paths = t->wavePaths;
+    out->trace_blocks_per_sm = t->traceBlocksPerSm;
+    out->shade_blocks_per_sm = t->shadeBlocksPerSm;
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_set_tuning(hdcx_tracer* t, const hdcx_tuning* in)
+{
+    if (!t || !in) return HDCX_ERROR_INVALID_ARGUMENT;
+    if ((in->wave_paths != 0 && in->wave_paths < 3) || in->trace_blocks_per_sm < 1 || in->trace_blocks_per_sm > 64 ||
+        in->shade_blocks_per_sm < 1 || in->shade_blocks_per_sm > 64)
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "tuning out of range (wave >= 3 paths or 0, 1..64 blocks per SM)");
+    t->wavePaths = in->wave_paths;
+    t->traceBlocksPerSm = in->trace_blocks_per_sm;
+    t->shadeBlocksPerSm = in->shade_blocks_per_sm;
+    return HDCX_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+struct TuningKey {
+    int device;
+    uint32_t triangles, width, height, samples, bounces, full, lit, opaque;
+    bool operator==(const TuningKey& o) const
+    {
+        return device == o.device && triangles == o.triangles && width == o.width && height == o.height &&
+               samples == o.samples && bounces == o.bounces && full == o.full && lit == o.lit && opaque == o.opaque;
+    }
+};
+
+std::mutex gTuningLock;
+std::vector<std::pair<TuningKey, hdcx_tuning>> gTunings;
+
+}  // namespace
+
+extern "C" {
+
+HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, uint32_t width, uint32_t height,
+                                   uint32_t maxBounces, uint32_t sampleCount, hdcx_tuning* result)
+{
+    if (!t || !camera || width == 0 || height == 0) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (!t->geometryReady) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "no geometry");
+    if (t->radianceCache) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "detach the radiance cache before tuning");
+    const TuningKey key{t->device, t->scene.primitiveCount, width, height, std::max(sampleCount, 1u),
+                        std::clamp(maxBounces, 1u, HDCX_MAX_PATH_BOUNCES), t->scene.fullShading,
+                        (t->scene.lightCount > 0u && !t->scene.hasMeshLights) ? 1u : 0u, t->scene.opaque};
+    {
+        std::lock_guard<std::mutex> lock(gTuningLock);
+        for (const auto& entry : gTunings) {
+            if (entry.first == key) {
+                hdcx_tuning cached = entry.second;
+                cached.candidates = 0;
+                t->wavePaths = cached.wave_paths;
+                t->traceBlocksPerSm = cached.trace_blocks_per_sm;
+                t->shadeBlocksPerSm = cached.shade_blocks_per_sm;
+                if (result) *result = cached;
+                return HDCX_OK;
+            }
+        }
+    }
+    hdcx_tuning best{};
+    return guarded(t, [&] {
+        const uint32_t savedProfiling = t->profiling;
+        t->profiling = 0;
+        // Best of two device-timed renders of one configuration.
+        auto measure = [&](uint64_t wave, uint32_t trace, uint32_t shade) {
+            t->wavePaths = wave;
+            t->traceBlocksPerSm = trace;
+            t->shadeBlocksPerSm = shade;
+            double ms = 1e30;
+            for (int rep = 0; rep < 2; ++rep) {
+                RenderCall call;
+                prepareRender(t, *camera, width, height, 0, maxBounces, sampleCount, 0, false, call);
+                enqueueRender(t, call, nullptr);
+                finishRender(t, call);
+                ms = std::min(ms, t->stats.render_ms);
+            }
+            return ms;
+        };
+        const uint64_t needed = uint64_t(width) * height * 3u * key.samples;
+        best.wave_paths = 0;
+        best.trace_blocks_per_sm = 16;
+        best.shade_blocks_per_sm = 8;
+        best.default_milliseconds = measure(0, 16, 8);
+        best.milliseconds = best.default_milliseconds;
+        best.candidates = 1;
+        auto consider = [&](uint64_t wave, uint32_t trace, uint32_t shade) {
+            const double ms = measure(wave, trace, shade);
+            ++best.candidates;
+            if (ms < best.milliseconds) {
+                best.milliseconds = ms;
+                best.wave_paths = wave;
+                best.trace_blocks_per_sm = trace;
+                best.shade_blocks_per_sm = shade;
+            }
+        };
+        for (uint64_t wave : {8ull << 20, 4ull << 20, 2ull << 20, 1ull << 20}) {
+            if (wave < needed) consider(wave, best.trace_blocks_per_sm, best.shade_blocks_per_sm);
+        }
+        for (uint32_t trace : {8u, 32u}) consider(best.wave_paths, trace, best.shade_blocks_per_sm);
+        for (uint32_t shade : {4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade);
+        t->wavePaths = best.wave_paths;
+        t->traceBlocksPerSm = best.trace_blocks_per_sm;
+        t->shadeBlocksPerSm = best.shade_blocks_per_sm;
+        t->profiling = savedProfiling;
+        {
+            std::lock_guard<std::mutex> lock(gTuningLock);
+            gTunings.emplace_back(key, best);
+        }
+        if (result) *result = best;
+    });
 }
 
 HDCX_API hdcx_status hdcx_set_radiance_cache(hdcx_tracer* t, hdcx_nrc* cache, uint32_t prefixBounces,

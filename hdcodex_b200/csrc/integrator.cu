@@ -1118,8 +1118,8 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
     CUDA_OK(cudaMemsetAsync(fb.batch, 0, sizeof(float4) * pixels, stream));
     CUDA_OK(cudaMemsetAsync(fb.batchXyz, 0, sizeof(double) * 3u * pixels, stream));
     const std::vector<WaveDesc> waves = planWaves(pixels, std::max(frame.sampleCount, 1u), paths.capacity);
-    const int traceGrid = gridFor(static_cast<uint32_t>(paths.capacity), 16);
-    const int shadeGrid = gridFor(static_cast<uint32_t>(paths.capacity), 8);
+    const int traceGrid = gridFor(static_cast<uint32_t>(paths.capacity), static_cast<int>(std::max(paths.traceBlocksPerSm, 1u)));
+    const int shadeGrid = gridFor(static_cast<uint32_t>(paths.capacity), static_cast<int>(std::max(paths.shadeBlocksPerSm, 1u)));
     std::vector<EventPair> events;
     auto timed = [&](int stage, auto&& launch) {
         if (!timing) {

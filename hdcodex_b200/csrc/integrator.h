@@ -62,6 +62,10 @@ struct PathBuffers {
     // tests; shadow node visits and triangle tests (counting mode)
     unsigned long long* stats = nullptr;
     CacheDevice cache;
+    // Launch shape (host side): blocks of 128 threads per SM of the traversal
+    // and shade kernels (the autotuner's knobs; results do not depend on them).
+    uint32_t traceBlocksPerSm = 16;
+    uint32_t shadeBlocksPerSm = 8;
 };
 
 // Per-pixel accumulation buffers of the current output size.

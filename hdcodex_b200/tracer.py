@@ -59,6 +59,10 @@ SIGNATURES = {
                                      C.c_uint32, _P, C.POINTER(C.c_int32)]),
     "hdcx_render_batch": (C.c_int, [C.POINTER(_abi.BatchJob), C.c_uint32, C.c_uint64]),
     "hdcx_read_rgba": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint64]),
+    "hdcx_get_tuning": (C.c_int, [_P, C.POINTER(_abi.Tuning)]),
+    "hdcx_set_tuning": (C.c_int, [_P, C.POINTER(_abi.Tuning)]),
+    "hdcx_autotune": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.POINTER(_abi.Tuning)]),
     "hdcx_set_radiance_cache": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32]),
     "hdcx_get_radiance_cache_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
     "hdcx_nrc_defaults": (None, [C.POINTER(_abi.NrcConfig)]),
@@ -212,6 +216,23 @@ class PathTracer:
         """Attach a RadianceCache (None detaches it)."""
         self._check(lib().hdcx_set_radiance_cache(self._h, cache.handle if cache is not None else None, prefix_bounces,
                                                   training_paths, train_steps), "set_radiance_cache")
+
+    def autotune(self, camera, width, height, max_bounces=8, sample_count=1) -> dict:
+        """hdcx_autotune: picks wave size and grid sizes for this workload shape."""
+        r = _abi.Tuning()
+        self._check(lib().hdcx_autotune(self._h, C.byref(camera), width, height, max_bounces, sample_count,
+                                        C.byref(r)), "autotune")
+        return {name: getattr(r, name) for name, _ in _abi.Tuning._fields_}
+
+    def tuning(self) -> dict:
+        r = _abi.Tuning()
+        self._check(lib().hdcx_get_tuning(self._h, C.byref(r)), "get_tuning")
+        return {name: getattr(r, name) for name, _ in _abi.Tuning._fields_}
+
+    def set_tuning(self, wave_paths=0, trace_blocks_per_sm=16, shade_blocks_per_sm=8):
+        r = _abi.Tuning(wave_paths=wave_paths, trace_blocks_per_sm=trace_blocks_per_sm,
+                        shade_blocks_per_sm=shade_blocks_per_sm)
+        self._check(lib().hdcx_set_tuning(self._h, C.byref(r)), "set_tuning")
 
     def radiance_cache_stats(self) -> dict:
         q, n, loss = C.c_uint64(0), C.c_uint64(0), C.c_float(0.0)

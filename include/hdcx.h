@@ -323,6 +323,19 @@ typedef struct hdcx_batch_job {
     double render_ms;        /* out: device time of the job on its tracer's stream */
 } hdcx_batch_job;
 
+/* Launch tuning of a tracer (hdcx_autotune, hdcx_set_tuning): paths per wave
+ * and blocks of 128 threads per SM of the traversal and shade kernels. Images
+ * do not depend on these values. */
+typedef struct hdcx_tuning {
+    uint64_t wave_paths;           /* 0 = automatic (up to 12,582,912) */
+    uint32_t trace_blocks_per_sm;  /* default 16 */
+    uint32_t shade_blocks_per_sm;  /* default 8 */
+    double milliseconds;           /* hdcx_autotune: device time of the best configuration */
+    double default_milliseconds;   /* hdcx_autotune: device time of the defaults */
+    uint32_t candidates;           /* hdcx_autotune: configurations timed (0: taken from the cache) */
+    uint32_t reserved;
+} hdcx_tuning;
+
 /* Profiling switches for hdcx_set_profiling. */
 #define HDCX_PROFILE_STAGE_TIMES 1u      /* CUDA events around every extend/shade/shadow launch */
 #define HDCX_PROFILE_COUNT_TRAVERSAL 2u  /* traversal kernels count node visits and triangle tests */
@@ -336,7 +349,7 @@ HDCX_API uint32_t hdcx_abi_version(void);
 
 /* Byte size of each ABI struct, indexed 0..7: camera, mesh, material, texture,
  * light, scene, packed_texture, packed_scene; 8: render_stats; 9: batch_job;
- * 10: nrc_config.
+ * 10: nrc_config; 11: tuning.
  * Lets bindings check their struct mirrors. Returns the number of entries. */
 HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity);
 
@@ -491,6 +504,19 @@ HDCX_API hdcx_status hdcx_set_profiling(hdcx_tracer* tracer, uint32_t flags);
 /* Number of paths resident per wave (0 = automatic). Larger waves use more
  * device memory for path state; results do not depend on it. */
 HDCX_API hdcx_status hdcx_set_wave_size(hdcx_tracer* tracer, uint64_t paths_per_wave);
+
+/* Current tuning of the tracer (milliseconds fields 0). */
+HDCX_API hdcx_status hdcx_get_tuning(const hdcx_tracer* tracer, hdcx_tuning* tuning);
+HDCX_API hdcx_status hdcx_set_tuning(hdcx_tracer* tracer, const hdcx_tuning* tuning);
+/* Autotuner (no counterpart in the reference): times renders of this camera,
+ * size, bounce budget and sample count over wave sizes and traversal/shade
+ * grid sizes, one knob at a time from the defaults, keeps the fastest on the
+ * tracer and returns it. Results are cached per device and workload shape
+ * (triangles, pixels, samples, bounces, shading variant) for the process, so
+ * a repeated call times nothing. The tuning renders overwrite the tracer's
+ * accumulation: render with sample_index 0 afterwards. */
+HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* tracer, const hdcx_camera* camera, uint32_t width, uint32_t height,
+                                   uint32_t max_bounces, uint32_t sample_count, hdcx_tuning* result);
 
 /* ---------------------------------------------------------------------------
  * Neural radiance cache (no counterpart in the reference; the learned part of
