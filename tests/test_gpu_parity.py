@@ -176,3 +176,16 @@ def test_primary_ids_spectral_stress(oracle_lib, gpu):
         got_p, got_t = gpu.trace_primary(wl.camera, wl.width, wl.height, sample)
         assert np.array_equal(got_p, ref_p)
         assert np.array_equal(got_t.view(np.uint32), ref_t.view(np.uint32))
+
+
+def test_heavy_geometry_render_parity(oracle_lib, gpu):
+    # 1.0M triangles, per-triangle Lambert / GGX-dielectric / conductor
+    # materials, lit by a textured dome only (the dome-only shade variant).
+    wl = workloads.heavy_geometry(width=160, height=90, spp=2, dome_size=(256, 128))
+    o = oracle_lib.OracleTracer()
+    o.set_scene(wl.scene)
+    ref = o.render(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp)
+    gpu.set_scene(wl.scene)
+    img = gpu.render(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp)
+    frac, rel = compare(img, ref)
+    assert frac >= MIN_IDENTICAL and rel <= MAX_REL_L1, f"identical={frac:.4f} relL1={rel:.2e}"
