@@ -57,6 +57,8 @@ def parse():
                          "nrc: time to a relative XYZ RMSE on the stress scene, radiance cache vs plain; "
                          "cache-kernels: radiance-cache query and training throughput")
     ap.add_argument("--jobs", type=int, default=64, help="jobs of the batch workload")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="batch workload: launch the jobs on their streams instead of one captured CUDA graph")
     ap.add_argument("--ref-spp", type=int, default=4096, help="nrc workload: spp of the FP64 reference")
     ap.add_argument("--target-rmse", type=float, default=0.02, help="nrc workload: relative XYZ RMSE to reach")
     ap.add_argument("--chunk-spp", type=int, default=4, help="nrc workload: spp per progressive render call")
@@ -301,7 +303,7 @@ def run_batch(args):
     def batch_step(step):
         spec = [(t, wl.camera, wl.width, wl.height, step * wl.spp, wl.max_bounces, wl.spp, h.data_ptr())
                 for t, wl, h in zip(tracers, jobs, hosts)]
-        return render_batch(spec)
+        return render_batch(spec, graph=args.graph)
 
     def serial_step(step):
         for t, wl, h in zip(tracers, jobs, hosts):
@@ -342,7 +344,8 @@ def run_batch(args):
             "config": {"workload": f"batch-{args.jobs}-jobs", "jobs": args.jobs,
                        "spectral_paths_per_step": total_paths,
                        "triangles": sum(workloads.triangle_count(wl.scene) for wl in jobs) if world == 1 else None,
-                       "l2": "inputs larger than L2", "parallelism": f"jobs dealt round-robin to {world} GPU(s)"},
+                       "l2": "inputs larger than L2", "parallelism": f"jobs dealt round-robin to {world} GPU(s)",
+                       "launch": "one CUDA graph per batch frame" if args.graph else "jobs on their own streams"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 48 * len(jobs),
                     "d2h_bytes_per_step": sum(wl.width * wl.height * 16 for wl in jobs)},
             "serial_loop": {"value": total_paths * args.steps / serial_s, "unit": UNIT,

@@ -732,12 +732,12 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
     call.active = true;
 }
 
-void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut)
+void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut, bool timeEvents = true)
 {
-    check(cudaEventRecord(t->start, t->stream), "cudaEventRecord");
+    if (timeEvents) check(cudaEventRecord(t->start, t->stream), "cudaEventRecord");
     renderFrame(t->scene, call.frame, t->paths, t->fb, t->stream, call.stageTiming ? &call.times : nullptr,
                 call.counting, &call.launches, t->radianceCache ? &t->cacheRun : nullptr);
-    check(cudaEventRecord(t->stop, t->stream), "cudaEventRecord");
+    if (timeEvents) check(cudaEventRecord(t->stop, t->stream), "cudaEventRecord");
     if (rgbaOut) {
         check(cudaMemcpyAsync(rgbaOut, t->fb.rgba, size_t(call.frame.width) * call.frame.height * sizeof(float4),
                               cudaMemcpyDeviceToHost, t->stream),
@@ -745,14 +745,15 @@ void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut)
     }
 }
 
-void finishRender(hdcx_tracer* t, RenderCall& call)
+// `graphMs` >= 0: the render ran inside a batch graph, whose device time it reports.
+void finishRender(hdcx_tracer* t, RenderCall& call, float graphMs = -1.0F)
 {
     check(cudaStreamSynchronize(t->stream), "render");
     t->xyzSamples = (call.frame.sampleIndex == 0 ? 0 : t->xyzSamples) + call.frame.sampleCount;
     unsigned long long counters[8];
     check(cudaMemcpy(counters, t->paths.stats, sizeof counters, cudaMemcpyDeviceToHost), "read stats");
-    float ms = 0.0F;
-    check(cudaEventElapsedTime(&ms, t->start, t->stop), "cudaEventElapsedTime");
+    float ms = graphMs;
+    if (graphMs < 0.0F) check(cudaEventElapsedTime(&ms, t->start, t->stop), "cudaEventElapsedTime");
     t->stats = hdcx_render_stats{};
     t->stats.spectral_paths = call.pathsNeeded;
     t->stats.extension_rays = counters[0];
@@ -793,6 +794,102 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint
 }
 
 HDCX_API hdcx_status hdcx_render_batch(hdcx_batch_job* jobs, uint32_t count, uint64_t pathBudget)
+{
+    return hdcx_render_batch_ex(jobs, count, pathBudget, 0u);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Captures the kernels of every active job (each on its own tracer's stream,
+// forked from and joined into one capture stream) into a single CUDA graph,
+// launches it once, then queues the read-backs. Returns the graph's device
+// time, or a negative value (nothing launched) when the batch cannot be
+// captured: jobs on several devices, a job in radiance-cache mode (it
+// synchronises with the host per wave) or a capture error.
+float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<RenderCall>& calls)
+{
+    int device = -1;
+    for (uint32_t j = 0; j < count; ++j) {
+        if (!calls[j].active) continue;
+        hdcx_tracer* t = jobs[j].tracer;
+        if (t->radianceCache || (device >= 0 && t->device != device)) return -1.0F;
+        device = t->device;
+    }
+    if (device < 0 || cudaSetDevice(device) != cudaSuccess) return -1.0F;
+    // The prepare phase queued clears on the tracers' streams; the graph runs
+    // on its own stream, so they must have finished.
+    for (uint32_t j = 0; j < count; ++j) {
+        if (calls[j].active && cudaStreamSynchronize(jobs[j].tracer->stream) != cudaSuccess) return -1.0F;
+    }
+    cudaStream_t batch = nullptr;
+    cudaEvent_t fork = nullptr, start = nullptr, stop = nullptr;
+    std::vector<cudaEvent_t> joins;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    float ms = -1.0F;
+    auto cleanup = [&] {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (cudaEvent_t e : joins) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (start) cudaEventDestroy(start);
+        if (stop) cudaEventDestroy(stop);
+        if (batch) cudaStreamDestroy(batch);
+    };
+    if (cudaStreamCreateWithFlags(&batch, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess || cudaEventCreate(&start) != cudaSuccess ||
+        cudaEventCreate(&stop) != cudaSuccess) {
+        cleanup();
+        return -1.0F;
+    }
+    bool captured = cudaStreamBeginCapture(batch, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+    try {
+        if (captured) {
+            check(cudaEventRecord(fork, batch), "fork");
+            for (uint32_t j = 0; j < count; ++j) {
+                if (!calls[j].active) continue;
+                hdcx_tracer* t = jobs[j].tracer;
+                check(cudaStreamWaitEvent(t->stream, fork, 0), "join the capture");
+                enqueueRender(t, calls[j], nullptr, false);
+                cudaEvent_t join = nullptr;
+                check(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), "cudaEventCreate");
+                joins.push_back(join);
+                check(cudaEventRecord(join, t->stream), "join");
+                check(cudaStreamWaitEvent(batch, join, 0), "join");
+            }
+        }
+    } catch (const std::exception&) {
+        captured = false;
+    }
+    cudaGraph_t capturedGraph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(batch, &capturedGraph);
+    graph = capturedGraph;
+    if (!captured || end != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return -1.0F;
+    }
+    if (cudaEventRecord(start, batch) == cudaSuccess && cudaGraphLaunch(exec, batch) == cudaSuccess &&
+        cudaEventRecord(stop, batch) == cudaSuccess && cudaStreamSynchronize(batch) == cudaSuccess) {
+        cudaEventElapsedTime(&ms, start, stop);
+        for (uint32_t j = 0; j < count; ++j) {
+            if (!calls[j].active || !jobs[j].rgba_out) continue;
+            hdcx_tracer* t = jobs[j].tracer;
+            cudaMemcpyAsync(jobs[j].rgba_out, t->fb.rgba, size_t(calls[j].frame.width) * calls[j].frame.height * sizeof(float4),
+                            cudaMemcpyDeviceToHost, t->stream);
+        }
+    }
+    cleanup();
+    return ms < 0.0F ? 0.0F : ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, uint64_t pathBudget, uint32_t flags)
 {
     if (count == 0) return HDCX_OK;
     if (!jobs) return HDCX_ERROR_INVALID_ARGUMENT;
@@ -865,15 +962,18 @@ HDCX_API hdcx_status hdcx_render_batch(hdcx_batch_job* jobs, uint32_t count, uin
                           calls[j]);
         }));
     }
-    for (uint32_t j = 0; j < count; ++j) {
-        if (!calls[j].active) continue;
-        record(j, guarded(jobs[j].tracer, [&] { enqueueRender(jobs[j].tracer, calls[j], jobs[j].rgba_out); }));
+    const float graphMs = (flags & HDCX_BATCH_CUDA_GRAPH) ? enqueueBatchGraph(jobs, count, calls) : -1.0F;
+    if (graphMs < 0.0F) {
+        for (uint32_t j = 0; j < count; ++j) {
+            if (!calls[j].active) continue;
+            record(j, guarded(jobs[j].tracer, [&] { enqueueRender(jobs[j].tracer, calls[j], jobs[j].rgba_out); }));
+        }
     }
     hdcx_status overall = HDCX_OK;
     for (uint32_t j = 0; j < count; ++j) {
         if (calls[j].active) {
             record(j, guarded(jobs[j].tracer, [&] {
-                finishRender(jobs[j].tracer, calls[j]);
+                finishRender(jobs[j].tracer, calls[j], graphMs);
                 jobs[j].written = 1;
                 jobs[j].render_ms = jobs[j].tracer->stats.render_ms;
             }));

@@ -58,6 +58,7 @@ SIGNATURES = {
     "hdcx_render_static": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                      C.c_uint32, _P, C.POINTER(C.c_int32)]),
     "hdcx_render_batch": (C.c_int, [C.POINTER(_abi.BatchJob), C.c_uint32, C.c_uint64]),
+    "hdcx_render_batch_ex": (C.c_int, [C.POINTER(_abi.BatchJob), C.c_uint32, C.c_uint64, C.c_uint32]),
     "hdcx_read_rgba": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint64]),
     "hdcx_get_tuning": (C.c_int, [_P, C.POINTER(_abi.Tuning)]),
     "hdcx_set_tuning": (C.c_int, [_P, C.POINTER(_abi.Tuning)]),
@@ -329,7 +330,10 @@ class RadianceCache:
                                                   grid.ctypes.data_as(C.POINTER(C.c_float))), "set_parameters")
 
 
-def render_batch(jobs, path_budget: int = 0):
+BATCH_CUDA_GRAPH = 1
+
+
+def render_batch(jobs, path_budget: int = 0, graph: bool = False):
     """hdcx_render_batch over `jobs`: (tracer, camera, width, height,
     sample_index, max_bounces, sample_count, out) tuples, `out` a float32
     (height, width, 4) array, a device pointer (int) or None. Returns the list
@@ -349,7 +353,7 @@ def render_batch(jobs, path_budget: int = 0):
             b.rgba_out = out.ctypes.data
         else:
             b.rgba_out = out
-    status = lib().hdcx_render_batch(arr, len(jobs), path_budget)
+    status = lib().hdcx_render_batch_ex(arr, len(jobs), path_budget, BATCH_CUDA_GRAPH if graph else 0)
     if status != 0:
         failed = [(i, arr[i].status) for i in range(len(jobs)) if arr[i].status != 0]
         i, st = failed[0]

@@ -472,6 +472,14 @@ HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* tracer, const hdcx_camera* 
  * job's status; each job's own status is in its `status`. */
 HDCX_API hdcx_status hdcx_render_batch(hdcx_batch_job* jobs, uint32_t count, uint64_t path_budget);
 
+/* hdcx_render_batch with options. HDCX_BATCH_CUDA_GRAPH: the kernels of all
+ * jobs (each on its tracer's stream) are captured into one CUDA graph and
+ * launched at once; every job's render_ms is then the whole graph's device
+ * time. A batch that cannot be captured (jobs on several devices, a job in
+ * radiance-cache mode) runs as hdcx_render_batch does. Same images either way. */
+#define HDCX_BATCH_CUDA_GRAPH 1u
+HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, uint64_t path_budget, uint32_t flags);
+
 /* Copies the current device RGBA32F accumulation (width*height*4 floats). */
 HDCX_API hdcx_status hdcx_read_rgba(hdcx_tracer* tracer, float* rgba_out, uint64_t float_count);
 

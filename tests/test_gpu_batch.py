@@ -1,6 +1,7 @@
 """hdcx_render_batch: several jobs rendered together equal the same jobs
 rendered one hdcx_render call at a time, bit for bit (images, running means
-and counters), whatever wave size each job runs with."""
+and counters), whatever wave size each job runs with, launched on the jobs'
+streams or captured into one CUDA graph (HDCX_BATCH_CUDA_GRAPH)."""
 import numpy as np
 import pytest
 
@@ -40,8 +41,8 @@ def sequential():
     return out
 
 
-@pytest.mark.parametrize("wave", [0, 5000])
-def test_batch_equals_sequential(sequential, wave):
+@pytest.mark.parametrize("wave,graph", [(0, False), (5000, False), (0, True), (5000, True)])
+def test_batch_equals_sequential(sequential, wave, graph):
     spec = jobs_spec()
     tracers = [PathTracer(0) for _ in spec]
     budget = 0
@@ -51,7 +52,7 @@ def test_batch_equals_sequential(sequential, wave):
             t.set_wave_size(wave)  # 5000: many small waves per job
         images = [np.zeros((h, w, 4), np.float32) for _, _, w, h, _ in spec]
         jobs = [(t, cam, w, h, 0, 8, spp, img) for t, (_, cam, w, h, spp), img in zip(tracers, spec, images)]
-        results = render_batch(jobs, budget)
+        results = render_batch(jobs, budget, graph=graph)
         assert all(r["written"] == 1 and r["status"] == 0 and r["render_ms"] > 0 for r in results)
         for k, (img, t) in enumerate(zip(images, tracers)):
             first, _, stats = sequential[k]
@@ -62,7 +63,7 @@ def test_batch_equals_sequential(sequential, wave):
         # A second, progressive batch on top of the first.
         images2 = [np.zeros_like(img) for img in images]
         jobs = [(t, cam, w, h, spp, 8, 2, img) for t, (_, cam, w, h, spp), img in zip(tracers, spec, images2)]
-        render_batch(jobs, budget)
+        render_batch(jobs, budget, graph=graph)
         for k, img in enumerate(images2):
             assert np.array_equal(img, sequential[k][1]), f"job {k} progressive"
     finally:
