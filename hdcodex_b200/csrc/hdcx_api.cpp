@@ -1305,11 +1305,11 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
                 best.shade_blocks_per_sm = shade;
             }
         };
-        for (uint64_t wave : {8ull << 20, 4ull << 20, 2ull << 20, 1ull << 20}) {
+        for (uint64_t wave : {8ull << 20, 6ull << 20, 4ull << 20, 3ull << 20, 2ull << 20, 1ull << 20}) {
             if (wave < needed) consider(wave, best.trace_blocks_per_sm, best.shade_blocks_per_sm);
         }
-        for (uint32_t trace : {8u, 32u}) consider(best.wave_paths, trace, best.shade_blocks_per_sm);
-        for (uint32_t shade : {4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade);
+        for (uint32_t trace : {8u, 32u, 64u}) consider(best.wave_paths, trace, best.shade_blocks_per_sm);
+        for (uint32_t shade : {2u, 4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade);
         t->wavePaths = best.wave_paths;
         t->traceBlocksPerSm = best.trace_blocks_per_sm;
         t->shadeBlocksPerSm = best.shade_blocks_per_sm;
