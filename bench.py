@@ -67,6 +67,9 @@ def parse():
                     help="nrc workload: comma-separated prefix bounces of the cache arms (the first is `value`)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="",
+                    help="wave_paths,trace_blocks_per_sm,shade_blocks_per_sm to use instead of autotuning "
+                         "(to repeat a tuned run, e.g. under a profiler)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip hdcx_autotune (by default it picks wave and grid sizes before the warm-up; setup, "
                          "not timed)")
@@ -522,6 +525,12 @@ def run_hdcx(args):
     wl = make_workload(args.workload, args)
     tracer = PathTracer(local)
     tracer.set_scene(wl.scene)
+    tuning = None
+    if args.tuning:
+        wave, trace, shade = (int(x) for x in args.tuning.split(","))
+        tracer.set_tuning(wave_paths=wave, trace_blocks_per_sm=trace, shade_blocks_per_sm=shade)
+    elif args.autotune and not args.profile:
+        tuning = tracer.autotune(wl.camera, wl.width, wl.height, wl.max_bounces, wl.spp)
     if args.profile:
         tracer.render_device(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp)
         print(json.dumps({"profile_frame": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
@@ -529,7 +538,6 @@ def run_hdcx(args):
         tracer.close()
         return
     paths_per_step = wl.spectral_paths
-    tuning = tracer.autotune(wl.camera, wl.width, wl.height, wl.max_bounces, wl.spp) if args.autotune else None
 
     from hdcodex_b200.multigpu import sample_range
 

@@ -1191,6 +1191,12 @@ HDCX_API hdcx_status hdcx_nrc_gradients(hdcx_nrc* n, const float* queries, const
     return nrcGuarded(n, [&] { hdcx::nrc::gradients(n->cache, queries, targets, count, mlpGradient, gridGradient, n->stream); });
 }
 
+HDCX_API hdcx_status hdcx_nrc_check_wait_timeout(hdcx_nrc* n, uint32_t polls)
+{
+    if (!n || polls == 0) return HDCX_ERROR_INVALID_ARGUMENT;
+    return nrcGuarded(n, [&] { hdcx::nrc::checkWaitTimeout(n->cache, polls, n->stream); });
+}
+
 HDCX_API hdcx_status hdcx_nrc_get_parameters(hdcx_nrc* n, float* mlp, float* grid)
 {
     if (!n) return HDCX_ERROR_INVALID_ARGUMENT;

@@ -104,10 +104,10 @@ __device__ __forceinline__ void barrierInit(uint64_t* bar)
 }
 
 // Bounded wait for the phase `parity` of `bar`; false if the limit ran out.
-__device__ __forceinline__ bool barrierWait(uint64_t* bar, uint32_t parity)
+__device__ __forceinline__ bool barrierWait(uint64_t* bar, uint32_t parity, uint32_t limit = kWaitLimit)
 {
     const uint32_t address = smemAddress(bar);
-    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+    for (uint32_t i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
@@ -469,6 +469,17 @@ __global__ void __launch_bounds__(128) trainKernel(DeviceParams p, const float* 
     if (warp == 0) tmemFree(tmem, 512u);
 }
 
+// The kernels' bounded wait on an mbarrier that nothing arrives at: the wait
+// runs out, the kernel records the timeout and returns (the host reads the
+// error flag; the context stays usable). Used by hdcx_nrc_check_wait_timeout.
+__global__ void waitTimeoutKernel(uint32_t limit, uint32_t* error)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) barrierInit(&bar);
+    __syncthreads();
+    if (__syncthreads_or(barrierWait(&bar, 0u, limit) ? 0 : 1) && threadIdx.x == 0) atomicOr(error, kErrorTimeout);
+}
+
 // Adam on `n` FP32 parameters; refreshes the BF16 tiled weights (mlp) or the
 // FP16 table (grid) and clears the gradients.
 __global__ void adamKernel(float* params, float* grad, float* m, float* v, uint32_t n, float lr, float beta1, float beta2,
@@ -655,6 +666,13 @@ void getParameters(Cache* c, float* mlp, float* grid)
     NRC_OK(cudaDeviceSynchronize());
     if (mlp) NRC_OK(cudaMemcpy(mlp, c->mlp, kWeightCount * sizeof(float), cudaMemcpyDeviceToHost));
     if (grid) NRC_OK(cudaMemcpy(grid, c->grid, c->gridCount * sizeof(float), cudaMemcpyDeviceToHost));
+}
+
+void checkWaitTimeout(Cache* c, uint32_t polls, cudaStream_t stream)
+{
+    waitTimeoutKernel<<<1, 128, 0, stream>>>(polls, c->error);
+    NRC_OK(cudaGetLastError());
+    checkError(c, stream);
 }
 
 uint64_t gridParameterCount(const Cache* c) { return c->gridCount; }

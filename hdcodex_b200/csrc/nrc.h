@@ -55,6 +55,9 @@ float train(Cache* cache, const float* queries, const float* targets, uint32_t c
 // Gradients of the mean loss without an update (host outputs, FP32).
 void gradients(Cache* cache, const float* queries, const float* targets, uint32_t count, float* mlpGrad, float* gridGrad,
                cudaStream_t stream);
+// Runs the kernels' bounded mbarrier wait on a barrier nothing arrives at, for
+// at most `polls` polls; throws the timeout error the host then reads.
+void checkWaitTimeout(Cache* cache, uint32_t polls, cudaStream_t stream);
 uint64_t gridParameterCount(const Cache* cache);
 void getParameters(Cache* cache, float* mlp, float* grid);
 void setParameters(Cache* cache, const float* mlp, const float* grid);

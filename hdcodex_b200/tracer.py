@@ -75,6 +75,7 @@ SIGNATURES = {
     "hdcx_nrc_query": (C.c_int, [_P, _P, C.c_uint32, _P]),
     "hdcx_nrc_train": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
     "hdcx_nrc_gradients": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "hdcx_nrc_check_wait_timeout": (C.c_int, [_P, C.c_uint32]),
     "hdcx_nrc_get_parameters": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "hdcx_nrc_set_parameters": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "hdcx_read_xyz": (C.c_int, [_P, C.POINTER(C.c_double), C.c_uint64, C.POINTER(C.c_uint64)]),
@@ -315,6 +316,11 @@ class RadianceCache:
                                              mlp.ctypes.data_as(C.POINTER(C.c_float)),
                                              grid.ctypes.data_as(C.POINTER(C.c_float))), "gradients")
         return mlp, grid
+
+    def check_wait_timeout(self, polls: int = 1 << 14):
+        """Status and message of the deliberately expiring bounded wait."""
+        status = lib().hdcx_nrc_check_wait_timeout(self._h, polls)
+        return STATUS.get(status, status), (lib().hdcx_nrc_last_error(self._h) or b"").decode()
 
     def parameters(self):
         mlp = np.zeros(NRC_WEIGHT_COUNT, np.float32)

@@ -574,6 +574,11 @@ HDCX_API hdcx_status hdcx_nrc_train(hdcx_nrc* cache, const float* queries, const
  * (either may be NULL). */
 HDCX_API hdcx_status hdcx_nrc_gradients(hdcx_nrc* cache, const float* queries, const float* targets, uint32_t count,
                                         float* mlp_gradient, float* grid_gradient);
+/* Failure-path check: runs the cache kernels' bounded tensor-core wait on an
+ * mbarrier that nothing arrives at, for at most `polls` polls. The wait runs
+ * out, the kernel records it and returns, and the call returns
+ * HDCX_ERROR_TIMEOUT with a message; the device context stays usable. */
+HDCX_API hdcx_status hdcx_nrc_check_wait_timeout(hdcx_nrc* cache, uint32_t polls);
 /* Host copies of the FP32 parameters (either may be NULL). Setting them
  * resets the Adam state. */
 HDCX_API hdcx_status hdcx_nrc_get_parameters(hdcx_nrc* cache, float* mlp, float* grid);

@@ -112,3 +112,15 @@ def test_training_fits_a_radiance_field():
         assert np.isfinite(loss) and loss < 0.1 * first, (first, loss)
         # The trained cache predicts the field; the untrained one does not.
         assert after < 0.1 and after < 0.2 * before, (before, after)
+
+
+def test_bounded_wait_times_out_and_the_context_survives(cache):
+    import torch
+    # An mbarrier that nothing arrives at: the wait runs out instead of hanging.
+    status, message = cache.check_wait_timeout(1 << 12)
+    assert status == "HDCX_ERROR_TIMEOUT" and "timed out" in message
+    q = queries(256, 5)
+    dq = device(q)
+    out = torch.zeros(len(q), dtype=torch.float32, device="cuda")
+    cache.query(dq.data_ptr(), len(q), out.data_ptr())
+    assert np.isfinite(out.cpu().numpy()).all()
