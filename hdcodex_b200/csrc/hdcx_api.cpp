@@ -385,7 +385,7 @@ void ensureOutput(hdcx_tracer* t, uint32_t w, uint32_t h)
 
 constexpr uint64_t kAutomaticWavePaths = 12ull << 20;  // ~12.6M paths per wave
 // Device bytes of path state per path (PathBuffers with three shadow slots).
-constexpr uint64_t kPathStateBytes = 131 + 3 * 56;
+constexpr uint64_t kPathStateBytes = 139 + 3 * 56;
 
 // `capOverride` (0 = none) bounds the wave when the tracer has no wave size
 // of its own; hdcx_render_batch uses it to share device memory among jobs.
@@ -416,12 +416,14 @@ void ensurePaths(hdcx_tracer* t, uint64_t needed, uint32_t shadowPerPath, uint64
     p.contributionValid = t->pathAlloc<uint8_t>(3 * n);
     p.queue[0] = t->pathAlloc<uint32_t>(n);
     p.queue[1] = t->pathAlloc<uint32_t>(n);
+    p.hitQueue = t->pathAlloc<uint32_t>(n);
+    p.missQueue = t->pathAlloc<uint32_t>(n);
     p.shadowOrigin = t->pathAlloc<float4>(ns);
     p.shadowDirection = t->pathAlloc<float4>(ns);
     p.shadowFactors = t->pathAlloc<float4>(ns);
     p.shadowSlot = t->pathAlloc<uint32_t>(ns);
     p.shadowInfo = t->pathAlloc<uint32_t>(ns);
-    p.counters = t->pathAlloc<uint32_t>(4);
+    p.counters = t->pathAlloc<uint32_t>(8);
     p.stats = t->pathAlloc<unsigned long long>(8);
 }
 

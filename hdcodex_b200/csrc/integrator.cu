@@ -152,6 +152,10 @@ __global__ void __launch_bounds__(128, 8) extendKernel(DeviceScene s, PathBuffer
         const bool found = traceRay<kMode, false, kCount>(s, xyz(o), xyz(d), 0.001f, 10000.0f, p.rng[slot], h, &work);
         p.hit[slot] = found ? make_float4(h.t, __uint_as_float(h.primitive), h.b1, h.b2)
                             : make_float4(0.0f, __uint_as_float(kInvalidPrimitive), 0.0f, 0.0f);
+        // Hits and misses go to separate queues, so that shading warps hold
+        // only hits and the short environment path runs in its own kernel.
+        if (found) p.hitQueue[appendIndex(p.counters + 4)] = slot;
+        else p.missQueue[appendIndex(p.counters + 5)] = slot;
     }
     if (kCount) {
         atomicAdd(p.stats + 3, static_cast<unsigned long long>(work.x));
@@ -882,6 +886,36 @@ __global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, 
 }
 
 // ---------------------------------------------------------------------------
+// miss: environment on a miss (vulkan_path_tracer.cpp:1245-1255), the paths
+// of extend's miss queue; the same steps as the top of shadeKernel
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) missKernel(DeviceScene s, FrameConst f, PathBuffers p)
+{
+    const uint32_t n = p.counters[5];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = p.missQueue[i];
+        float radiance = p.radiance[slot];
+        // Light-sample contributions of the previous bounce, in slot order.
+        for (uint32_t k = 0; k < 3u; ++k) {
+            uint8_t& valid = p.contributionValid[k * p.capacity + slot];
+            if (valid) {
+                radiance += p.contribution[k * p.capacity + slot];
+                valid = 0;
+            }
+        }
+        const uint32_t flags = p.flags[slot];
+        if ((flags & kFlagEnvironmentOnMiss) != 0u) {
+            const Spectrum spec = spectrumFromBasis(p.wavelength[slot], p.spectrum[slot]);
+            const float2 previousPdf = p.previousPdf[slot];
+            const float misWeight =
+                (flags & kFlagPreviousWasDelta) != 0u ? 1.0f : powerHeuristic(previousPdf.x, previousPdf.y);
+            radiance += p.throughput[slot] * misWeight * illuminantSpectrum(environment(s, f, xyz(p.rayDirection[slot])), spec);
+        }
+        p.radiance[slot] = radiance;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // shadow: visibility of light samples (vulkan_path_tracer.cpp:855-912)
 // ---------------------------------------------------------------------------
 template <bool kOpaque, bool kCount>
@@ -1120,6 +1154,7 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
     const std::vector<WaveDesc> waves = planWaves(pixels, std::max(frame.sampleCount, 1u), paths.capacity);
     const int traceGrid = gridFor(static_cast<uint32_t>(paths.capacity), static_cast<int>(std::max(paths.traceBlocksPerSm, 1u)));
     const int shadeGrid = gridFor(static_cast<uint32_t>(paths.capacity), static_cast<int>(std::max(paths.shadeBlocksPerSm, 1u)));
+    const int missGrid = gridFor(static_cast<uint32_t>(paths.capacity), 8);
     std::vector<EventPair> events;
     auto timed = [&](int stage, auto&& launch) {
         if (!timing) {
@@ -1144,6 +1179,7 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
             uint32_t* outQueue = paths.queue[(bounce + 1u) & 1u];
             uint32_t* inCount = paths.counters + (bounce & 1u);
             uint32_t* outCount = paths.counters + ((bounce + 1u) & 1u);
+            CUDA_OK(cudaMemsetAsync(paths.counters + 4, 0, 2 * sizeof(uint32_t), stream));
             timed(0, [&] {
                 if (countTraversal) {
                     if (scene.opaque) extendKernel<Accept::Opaque, true><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
@@ -1157,8 +1193,9 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
             CUDA_OK(cudaMemsetAsync(outCount, 0, sizeof(uint32_t), stream));
             CUDA_OK(cudaMemsetAsync(paths.counters + 2, 0, sizeof(uint32_t), stream));
             timed(1, [&] {
-                if (cacheMode) launchShade<true>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount, shadeGrid, stream);
-                else launchShade<false>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount, shadeGrid, stream);
+                if (cacheMode) launchShade<true>(scene, frame, paths, bounce, paths.hitQueue, paths.counters + 4, outQueue, outCount, shadeGrid, stream);
+                else launchShade<false>(scene, frame, paths, bounce, paths.hitQueue, paths.counters + 4, outQueue, outCount, shadeGrid, stream);
+                missKernel<<<missGrid, 128, 0, stream>>>(scene, frame, paths);
             });
             CUDA_OK(cudaGetLastError());
             timed(2, [&] {
@@ -1171,7 +1208,7 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
                 }
             });
             CUDA_OK(cudaGetLastError());
-            launched += 3;
+            launched += 4;
         }
         if (cacheMode) {
             // Predictions for the terminated paths, then one training round on

@@ -52,12 +52,14 @@ struct PathBuffers {
     float* contribution = nullptr;  // 3 * capacity, slot-major per shadow slot k
     uint8_t* contributionValid = nullptr;
     uint32_t* queue[2] = {nullptr, nullptr};
+    uint32_t* hitQueue = nullptr;       // extend's output: paths whose ray hit (shaded)
+    uint32_t* missQueue = nullptr;      // extend's output: paths whose ray missed (environment)
     float4* shadowOrigin = nullptr;     // xyz, tmax
     float4* shadowDirection = nullptr;  // xyz, partial product
     float4* shadowFactors = nullptr;    // f1, f2, f3
     uint32_t* shadowSlot = nullptr;     // path slot * 4 + k
     uint32_t* shadowInfo = nullptr;     // kind | light << 8
-    uint32_t* counters = nullptr;       // [0], [1] extension queues, [2] shadow queue
+    uint32_t* counters = nullptr;       // [0], [1] extension queues, [2] shadow queue, [4] hits, [5] misses (8 entries)
     // extension, shadow, subsurface rays; extension node visits and triangle
     // tests; shadow node visits and triangle tests (counting mode)
     unsigned long long* stats = nullptr;

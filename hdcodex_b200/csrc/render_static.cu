@@ -14,7 +14,7 @@
 // kStaticMaxPixels pixels; waves of kStaticWavePaths paths (a frame needs more
 // waves than the ordinary render, whose waves hold up to ~12.6M paths, so this
 // variant is slower on large frames). Every GPU that loads the library keeps
-// the array, kStaticScratchBytes (about 61 MB), until the process exits.
+// the array, kStaticScratchBytes (about 62 MB), until the process exits.
 //
 // The array's device address is looked up once per device with
 // cudaGetSymbolAddress, by the first call on that device (with that device
@@ -55,12 +55,14 @@ constexpr uint64_t kRegionBytes[] = {
     3 * kN,                        // contributionValid
     4 * kN,                        // queue[0]
     4 * kN,                        // queue[1]
+    4 * kN,                        // hitQueue
+    4 * kN,                        // missQueue
     16 * kShadow,                  // shadowOrigin
     16 * kShadow,                  // shadowDirection
     16 * kShadow,                  // shadowFactors
     4 * kShadow,                   // shadowSlot
     4 * kShadow,                   // shadowInfo
-    4 * 4,                         // counters
+    4 * 8,                         // counters
     8 * 8,                         // stats
     16 * kStaticMaxPixels,         // batch (float4 per pixel)
     24 * kStaticMaxPixels,         // batchXyz (3 doubles per pixel)
@@ -139,20 +141,22 @@ void renderStatic(const DeviceScene& scene, const FrameConst& frame, float4* rgb
     p.contributionValid = reinterpret_cast<uint8_t*>(region[12]);
     p.queue[0] = reinterpret_cast<uint32_t*>(region[13]);
     p.queue[1] = reinterpret_cast<uint32_t*>(region[14]);
-    p.shadowOrigin = reinterpret_cast<float4*>(region[15]);
-    p.shadowDirection = reinterpret_cast<float4*>(region[16]);
-    p.shadowFactors = reinterpret_cast<float4*>(region[17]);
-    p.shadowSlot = reinterpret_cast<uint32_t*>(region[18]);
-    p.shadowInfo = reinterpret_cast<uint32_t*>(region[19]);
-    p.counters = reinterpret_cast<uint32_t*>(region[20]);
-    p.stats = reinterpret_cast<unsigned long long*>(region[21]);
+    p.hitQueue = reinterpret_cast<uint32_t*>(region[15]);
+    p.missQueue = reinterpret_cast<uint32_t*>(region[16]);
+    p.shadowOrigin = reinterpret_cast<float4*>(region[17]);
+    p.shadowDirection = reinterpret_cast<float4*>(region[18]);
+    p.shadowFactors = reinterpret_cast<float4*>(region[19]);
+    p.shadowSlot = reinterpret_cast<uint32_t*>(region[20]);
+    p.shadowInfo = reinterpret_cast<uint32_t*>(region[21]);
+    p.counters = reinterpret_cast<uint32_t*>(region[22]);
+    p.stats = reinterpret_cast<unsigned long long*>(region[23]);
 
     FrameBuffers fb;
     fb.width = frame.width;
     fb.height = frame.height;
     fb.rgba = rgba;
-    fb.batch = reinterpret_cast<float4*>(region[22]);
-    fb.batchXyz = reinterpret_cast<double*>(region[23]);
+    fb.batch = reinterpret_cast<float4*>(region[24]);
+    fb.batchXyz = reinterpret_cast<double*>(region[25]);
     // The frame's FP64 XYZ running sums are not kept by this variant: the
     // finalize pass adds them into the batch sums of the same pixel (each
     // thread reads and writes only its own pixel), which the next call clears.
@@ -160,7 +164,7 @@ void renderStatic(const DeviceScene& scene, const FrameConst& frame, float4* rgb
 
     // The array keeps the previous call's contents: the queue counters and
     // ray statistics must start at zero (renderFrame clears the batch sums).
-    ok(cudaMemsetAsync(p.counters, 0, 4 * sizeof(uint32_t), stream), "clear counters");
+    ok(cudaMemsetAsync(p.counters, 0, 8 * sizeof(uint32_t), stream), "clear counters");
     ok(cudaMemsetAsync(p.stats, 0, 8 * sizeof(unsigned long long), stream), "clear stats");
     renderFrame(scene, frame, p, fb, stream, nullptr, false, nullptr);
     // The lock covers the GPU work too: the next call may reuse the array.

@@ -14,7 +14,7 @@ constexpr uint64_t kStaticMaxPixels = 1ull << 20;
 constexpr uint64_t kStaticWavePaths = 1ull << 16;
 constexpr uint32_t kStaticShadowPerPath = 3;
 // Size of the static scratch array (checked against its layout at compile time).
-constexpr uint64_t kStaticScratchBytes = 61538816ull;
+constexpr uint64_t kStaticScratchBytes = 62063104ull;
 
 // Renders like renderFrame into the caller's running-mean buffer `rgba`
 // (width * height float4, device memory) with all scratch taken from the

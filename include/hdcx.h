@@ -439,7 +439,7 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* tracer, const hdcx_camera* camera,
  * written.
  *
  * The scratch (the path state of one wave of 65,536 paths and the per-pixel
- * sums of one frame) is one static device array of 61,538,816 bytes inside
+ * sums of one frame) is one static device array of 62,063,104 bytes inside
  * the library, which every GPU that loads the library keeps until the process
  * exits. Images above 1,048,576 pixels (width*height) are rejected with
  * HDCX_ERROR_INVALID_ARGUMENT and a message. The first call on a device looks
