@@ -393,6 +393,10 @@ void ensurePaths(hdcx_tracer* t, uint64_t needed, uint32_t shadowPerPath, uint64
 {
     const uint64_t cap = t->wavePaths ? t->wavePaths : (capOverride ? capOverride : kAutomaticWavePaths);
     const uint64_t capacity = std::max<uint64_t>(3, std::min(needed, cap));
+    // Buffers larger than this call's wave are kept (no reallocation when an
+    // image shrinks), but the wave is this call's: the wave size decides the
+    // launch shape, so it must not follow the buffers' capacity.
+    t->paths.wavePaths = capacity;
     if (t->paths.capacity >= capacity && t->paths.shadowPerPath >= shadowPerPath) return;
     check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
     t->clearPaths();
@@ -400,6 +404,7 @@ void ensurePaths(hdcx_tracer* t, uint64_t needed, uint32_t shadowPerPath, uint64
     const uint64_t n = capacity;
     const uint64_t ns = n * shadowPerPath;
     p.capacity = n;
+    p.wavePaths = n;
     p.shadowPerPath = shadowPerPath;
     p.rng = t->pathAlloc<uint32_t>(n);
     p.wavelength = t->pathAlloc<float>(n);
@@ -722,7 +727,7 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
         CacheDevice c = t->cacheDevice;
         c.enabled = 1u;
         c.prefixBounces = t->cachePrefix;
-        const double wave = static_cast<double>(std::min<uint64_t>(call.pathsNeeded, t->paths.capacity));
+        const double wave = static_cast<double>(std::min<uint64_t>(call.pathsNeeded, t->paths.wavePaths));
         c.trainThreshold = static_cast<uint32_t>(std::min(4294967295.0, double(t->cacheTrainingPaths) / wave * 4294967296.0));
         c.sceneMin = t->sceneMin;
         c.sceneScale = t->sceneScale;
@@ -1313,11 +1318,26 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
                 best.shade_blocks_per_sm = shade;
             }
         };
-        for (uint64_t wave : {8ull << 20, 6ull << 20, 4ull << 20, 3ull << 20, 2ull << 20, 1ull << 20}) {
-            if (wave < needed) consider(wave, best.trace_blocks_per_sm, best.shade_blocks_per_sm);
+        // Waves above the automatic size shorten the launches' tails; they are
+        // tried while their path state stays within half the device memory
+        // that is free or already held by this tracer's path buffers.
+        size_t freeBytes = 0, totalBytes = 0;
+        check(cudaMemGetInfo(&freeBytes, &totalBytes), "cudaMemGetInfo");
+        const uint64_t pathBytesLimit = (freeBytes + t->paths.capacity * kPathStateBytes) / 2;
+        for (uint64_t wave : {48ull << 20, 32ull << 20, 24ull << 20, 16ull << 20, 8ull << 20, 4ull << 20, 2ull << 20,
+                              1ull << 20}) {
+            if (wave < needed && wave * kPathStateBytes <= pathBytesLimit)
+                consider(wave, best.trace_blocks_per_sm, best.shade_blocks_per_sm);
         }
         for (uint32_t trace : {8u, 32u, 64u}) consider(best.wave_paths, trace, best.shade_blocks_per_sm);
         for (uint32_t shade : {2u, 4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade);
+        // Buffers grown for a larger candidate than the one chosen are released;
+        // the next render allocates the chosen wave.
+        const uint64_t chosen = std::max<uint64_t>(3, std::min(needed, best.wave_paths ? best.wave_paths : kAutomaticWavePaths));
+        if (t->paths.capacity > chosen) {
+            check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+            t->clearPaths();
+        }
         t->wavePaths = best.wave_paths;
         t->traceBlocksPerSm = best.trace_blocks_per_sm;
         t->shadeBlocksPerSm = best.shade_blocks_per_sm;

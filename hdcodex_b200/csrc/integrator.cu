@@ -292,10 +292,13 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
 // sampling (:1670-1731) can run; both are compiled out.
 // kCache: radiance-cache mode (PathBuffers::cache): queries and training
 // records at surface vertices; the plain kernels compile without it.
+// The lit, non-full variants wait on memory most of the time (long-scoreboard
+// stalls): they are capped at 80 registers so that six blocks fit an SM
+// instead of four, which costs a few spilled values and gains 6% of their time.
 template <bool kFull, bool kLit, bool kCache>
-__global__ void __launch_bounds__(128) shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce,
-                                                   const uint32_t* queue, const uint32_t* count, uint32_t* nextQueue,
-                                                   uint32_t* nextCount)
+__global__ void __launch_bounds__(128, (!kFull && kLit) ? 6 : 1)
+    shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce, const uint32_t* queue,
+                const uint32_t* count, uint32_t* nextQueue, uint32_t* nextCount)
 {
     const uint32_t n = *count;
     const bool lastBounce = bounce + 1u >= f.maxBounces;
@@ -1151,10 +1154,11 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
     const uint32_t pixels = frame.width * frame.height;
     CUDA_OK(cudaMemsetAsync(fb.batch, 0, sizeof(float4) * pixels, stream));
     CUDA_OK(cudaMemsetAsync(fb.batchXyz, 0, sizeof(double) * 3u * pixels, stream));
-    const std::vector<WaveDesc> waves = planWaves(pixels, std::max(frame.sampleCount, 1u), paths.capacity);
-    const int traceGrid = gridFor(static_cast<uint32_t>(paths.capacity), static_cast<int>(std::max(paths.traceBlocksPerSm, 1u)));
-    const int shadeGrid = gridFor(static_cast<uint32_t>(paths.capacity), static_cast<int>(std::max(paths.shadeBlocksPerSm, 1u)));
-    const int missGrid = gridFor(static_cast<uint32_t>(paths.capacity), 8);
+    const uint64_t wavePaths = paths.wavePaths ? std::min(paths.wavePaths, paths.capacity) : paths.capacity;
+    const std::vector<WaveDesc> waves = planWaves(pixels, std::max(frame.sampleCount, 1u), wavePaths);
+    const int traceGrid = gridFor(static_cast<uint32_t>(wavePaths), static_cast<int>(std::max(paths.traceBlocksPerSm, 1u)));
+    const int shadeGrid = gridFor(static_cast<uint32_t>(wavePaths), static_cast<int>(std::max(paths.shadeBlocksPerSm, 1u)));
+    const int missGrid = gridFor(static_cast<uint32_t>(wavePaths), 8);
     std::vector<EventPair> events;
     auto timed = [&](int stage, auto&& launch) {
         if (!timing) {

@@ -36,7 +36,8 @@ struct CacheDevice {
 
 // Device buffers of one wave of paths (structure of arrays, 16-byte records).
 struct PathBuffers {
-    uint64_t capacity = 0;          // paths per wave
+    uint64_t capacity = 0;          // paths the buffers hold (the stride of the per-slot arrays)
+    uint64_t wavePaths = 0;         // paths per wave, at most capacity (0: capacity)
     uint32_t shadowPerPath = 0;     // shadow-ray slots per path per bounce
     uint32_t* rng = nullptr;
     float* wavelength = nullptr;

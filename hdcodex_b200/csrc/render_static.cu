@@ -125,6 +125,7 @@ void renderStatic(const DeviceScene& scene, const FrameConst& frame, float4* rgb
     }
     PathBuffers p;
     p.capacity = kN;
+    p.wavePaths = kN;
     p.shadowPerPath = kStaticShadowPerPath;
     p.rng = reinterpret_cast<uint32_t*>(region[0]);
     p.wavelength = reinterpret_cast<float*>(region[1]);

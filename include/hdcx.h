@@ -519,7 +519,10 @@ HDCX_API hdcx_status hdcx_set_tuning(hdcx_tracer* tracer, const hdcx_tuning* tun
 /* Autotuner (no counterpart in the reference): times renders of this camera,
  * size, bounce budget and sample count over wave sizes and traversal/shade
  * grid sizes, one knob at a time from the defaults, keeps the fastest on the
- * tracer and returns it. Results are cached per device and workload shape
+ * tracer and returns it. Wave sizes of 1M to 48M paths are tried, the larger
+ * ones while their path state (about 307 bytes per path) fits half of the free
+ * device memory; path buffers grown for a candidate larger than the one kept
+ * are released before it returns. Results are cached per device and workload shape
  * (triangles, pixels, samples, bounces, shading variant) for the process, so
  * a repeated call times nothing. The tuning renders overwrite the tracer's
  * accumulation: render with sample_index 0 afterwards. */

@@ -36,3 +36,19 @@ def test_tuning_rejects_out_of_range_values():
             t.set_tuning(trace_blocks_per_sm=0)
         with pytest.raises(RuntimeError, match="tuning out of range"):
             t.set_tuning(wave_paths=2)
+
+
+def test_wave_size_follows_the_tuning_after_larger_buffers():
+    """Path buffers are kept when a later call needs fewer paths, but each call
+    launches waves of its own size: a smaller wave set after a large render
+    takes effect (more waves, more launches) and renders the same image."""
+    wl = workloads.closed_box(width=64, height=64)
+    with PathTracer(0) as t:
+        t.set_scene(wl.scene)
+        one_wave = t.render(wl.camera, 64, 64, 0, 8, 4)  # 49,152 paths: one wave
+        launches_one = t.stats()["kernel_launches"]
+        t.set_tuning(wave_paths=4096)
+        many_waves = t.render(wl.camera, 64, 64, 0, 8, 4)
+        launches_many = t.stats()["kernel_launches"]
+    assert np.array_equal(one_wave, many_waves)
+    assert launches_many > 8 * launches_one, (launches_one, launches_many)
