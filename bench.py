@@ -332,10 +332,14 @@ def run_batch(args):
     barrier_sync(world)
     batch_s = max_over_ranks(time.perf_counter() - t0, world)
     clocks = sampler.stop()
+    # The serial loop gets its own warm-up: each tracer's first hdcx_render
+    # allocates its path buffers (in the batch, the lanes' buffers are shared).
+    for i in range(args.warmup):
+        serial_step(args.warmup + args.steps + i)
     barrier_sync(world)
     t0 = time.perf_counter()
     for i in range(args.steps):
-        serial_step(args.warmup + args.steps + i)
+        serial_step(2 * args.warmup + args.steps + i)
     barrier_sync(world)
     serial_s = max_over_ranks(time.perf_counter() - t0, world)
     total_paths = float(paths)

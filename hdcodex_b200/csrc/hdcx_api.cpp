@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <memory>
 #include <mutex>
 #include <cmath>
 #include <cstring>
@@ -67,6 +68,131 @@ struct DeviceBuffer {
     }
 };
 
+// Path state of one wave of up to paths.capacity paths and the device
+// buffers behind it.
+struct PathStore {
+    std::vector<DeviceBuffer*> buffers;
+    PathBuffers paths;
+    PathStore() = default;
+    PathStore(const PathStore&) = delete;
+    PathStore& operator=(const PathStore&) = delete;
+    ~PathStore() { release(); }
+    void release()
+    {
+        for (DeviceBuffer* b : buffers) delete b;
+        buffers.clear();
+        paths = PathBuffers{};
+    }
+    template <typename T>
+    T* alloc(size_t count)
+    {
+        auto* b = new DeviceBuffer();
+        buffers.push_back(b);
+        b->allocate(count * sizeof(T));
+        return b->as<T>();
+    }
+    // Replaces the buffers by buffers of `n` paths; the GPU must be done with the old ones.
+    void allocate(uint64_t n, uint32_t shadowPerPath)
+    {
+        release();
+        PathBuffers& p = paths;
+        const uint64_t ns = n * shadowPerPath;
+        p.capacity = n;
+        p.wavePaths = n;
+        p.shadowPerPath = shadowPerPath;
+        p.rng = alloc<uint32_t>(n);
+        p.wavelength = alloc<float>(n);
+        p.spectrum = alloc<float4>(n);
+        p.throughput = alloc<float>(n);
+        p.radiance = alloc<float>(n);
+        p.rayOrigin = alloc<float4>(n);
+        p.rayDirection = alloc<float4>(n);
+        p.flags = alloc<uint32_t>(n);
+        p.previousPdf = alloc<float2>(n);
+        p.medium = alloc<float4>(n);
+        p.hit = alloc<float4>(n);
+        p.contribution = alloc<float>(3 * n);
+        p.contributionValid = alloc<uint8_t>(3 * n);
+        p.queue[0] = alloc<uint32_t>(n);
+        p.queue[1] = alloc<uint32_t>(n);
+        p.hitQueue = alloc<uint32_t>(n);
+        p.missQueue = alloc<uint32_t>(n);
+        p.shadowOrigin = alloc<float4>(ns);
+        p.shadowDirection = alloc<float4>(ns);
+        p.shadowFactors = alloc<float4>(ns);
+        p.shadowSlot = alloc<uint32_t>(ns);
+        p.shadowInfo = alloc<uint32_t>(ns);
+        p.counters = alloc<uint32_t>(8);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Path arenas
+//
+// A render needs the path state of its waves (about 307 bytes per path) only
+// while it runs, so path state belongs to a per-device pool of arenas rather
+// than to tracers: hdcx_render and hdcx_autotune check an arena out for the
+// call, hdcx_render_batch one per lane until the batch's work has finished.
+// Many tracers on one device then share a few large buffers instead of each
+// holding its own. An arena grows to the largest wave asked of it and keeps
+// its buffers until the last tracer of its device is destroyed. A device has
+// at most kMaxArenas arenas; a render that finds them all busy waits for one.
+// (A tracer in radiance-cache mode renders on path buffers of its own, sized
+// together with its cache buffers.)
+// ---------------------------------------------------------------------------
+constexpr int kArenaDevices = 64;
+constexpr size_t kMaxArenas = 8;
+
+struct PathArena {
+    std::mutex busy;  // held by the render or batch lane that uses the arena
+    PathStore store;
+};
+
+struct ArenaPool {
+    std::mutex lock;
+    std::vector<std::unique_ptr<PathArena>> arenas;
+    size_t next = 0;
+    int tracers = 0;
+};
+
+ArenaPool& arenaPool(int device)
+{
+    // Never destroyed: the arenas go with their device's last tracer, not at
+    // process exit, when the CUDA runtime may already be gone.
+    static ArenaPool* pools = new ArenaPool[kArenaDevices];
+    if (device < 0 || device >= kArenaDevices) throw std::runtime_error("device ordinal out of range");
+    return pools[device];
+}
+
+struct ArenaLease {
+    PathArena* arena = nullptr;
+    std::unique_lock<std::mutex> hold;
+};
+
+// A free arena of `device`, or a new one while the device has fewer than
+// kMaxArenas. When all are busy: with `wait`, waits for one of them (round
+// robin); without, returns an empty lease.
+ArenaLease checkoutArena(int device, bool wait)
+{
+    ArenaPool& pool = arenaPool(device);
+    PathArena* busy = nullptr;
+    {
+        std::lock_guard<std::mutex> guard(pool.lock);
+        for (auto& a : pool.arenas) {
+            std::unique_lock<std::mutex> hold(a->busy, std::try_to_lock);
+            if (hold.owns_lock()) return ArenaLease{a.get(), std::move(hold)};
+        }
+        if (pool.arenas.size() < kMaxArenas) {
+            pool.arenas.push_back(std::make_unique<PathArena>());
+            PathArena* a = pool.arenas.back().get();
+            return ArenaLease{a, std::unique_lock<std::mutex>(a->busy)};
+        }
+        if (!wait) return ArenaLease{};
+        busy = pool.arenas[pool.next++ % pool.arenas.size()].get();
+    }
+    return ArenaLease{busy, std::unique_lock<std::mutex>(busy->busy)};
+}
+
 }  // namespace
 
 struct hdcx_nrc {
@@ -99,10 +225,10 @@ struct hdcx_tracer {
     DeviceBuffer texDescs;
     DeviceScene scene{};
     WideBvh bvh;
-    // Paths and frame.
-    std::vector<DeviceBuffer*> pathBuffers;
-    PathBuffers paths;
+    // Path state of radiance-cache renders (other renders use the arenas).
+    PathStore own;
     DeviceBuffer rgba, xyz, batch, batchXyz;
+    DeviceBuffer statsBuffer;  // this tracer's ray counters (8 x u64), whichever path buffers it renders with
     FrameBuffers fb;
     uint64_t xyzSamples = 0;
     hdcx_render_stats stats{};
@@ -121,7 +247,7 @@ struct hdcx_tracer {
     {
         if (stream) cudaStreamSynchronize(stream);
         clearScene();
-        clearPaths();
+        own.release();
         clearCache();
         if (start) cudaEventDestroy(start);
         if (stop) cudaEventDestroy(stop);
@@ -151,12 +277,6 @@ struct hdcx_tracer {
         b->allocate(count * sizeof(T));
         return b->as<T>();
     }
-    void clearPaths()
-    {
-        for (DeviceBuffer* b : pathBuffers) delete b;
-        pathBuffers.clear();
-        paths = PathBuffers{};
-    }
     template <typename T>
     T* upload(const std::vector<T>& host)
     {
@@ -164,14 +284,6 @@ struct hdcx_tracer {
         sceneBuffers.push_back(b);
         b->allocate(host.size() * sizeof(T));
         if (!host.empty()) check(cudaMemcpyAsync(b->ptr, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
-        return b->as<T>();
-    }
-    template <typename T>
-    T* pathAlloc(size_t count)
-    {
-        auto* b = new DeviceBuffer();
-        pathBuffers.push_back(b);
-        b->allocate(count * sizeof(T));
         return b->as<T>();
     }
 };
@@ -387,49 +499,42 @@ constexpr uint64_t kAutomaticWavePaths = 12ull << 20;  // ~12.6M paths per wave
 // Device bytes of path state per path (PathBuffers with three shadow slots).
 constexpr uint64_t kPathStateBytes = 139 + 3 * 56;
 
-// `capOverride` (0 = none) bounds the wave when the tracer has no wave size
-// of its own; hdcx_render_batch uses it to share device memory among jobs.
-void ensurePaths(hdcx_tracer* t, uint64_t needed, uint32_t shadowPerPath, uint64_t capOverride = 0)
+// Smallest wave an automatic wave is shrunk to when device memory is short.
+constexpr uint64_t kMinimumAutomaticWave = 1ull << 16;
+
+// Sizes the wave of a render of `needed` paths on `store` and grows the store
+// to it; returns the wave. The wave is the tracer's own wave size if it set
+// one, else min(needed, `capOverride` or the automatic wave). A wave the
+// tracer did not set is also bounded by device memory: its path state takes
+// at most three quarters of what is free plus what the store already holds
+// (the wave size does not change the image). Buffers larger than the wave are
+// kept, but the wave is this call's, since it decides the launch shape.
+// `fixed`: the store is not grown; the wave is bounded by its capacity.
+uint64_t ensureStore(hdcx_tracer* t, PathStore& store, uint64_t needed, uint64_t capOverride, bool fixed)
 {
+    constexpr uint32_t kShadowSlots = 3;
     const uint64_t cap = t->wavePaths ? t->wavePaths : (capOverride ? capOverride : kAutomaticWavePaths);
-    const uint64_t capacity = std::max<uint64_t>(3, std::min(needed, cap));
-    // Buffers larger than this call's wave are kept (no reallocation when an
-    // image shrinks), but the wave is this call's: the wave size decides the
-    // launch shape, so it must not follow the buffers' capacity.
-    t->paths.wavePaths = capacity;
-    if (t->paths.capacity >= capacity && t->paths.shadowPerPath >= shadowPerPath) return;
-    check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
-    t->clearPaths();
-    PathBuffers& p = t->paths;
-    const uint64_t n = capacity;
-    const uint64_t ns = n * shadowPerPath;
-    p.capacity = n;
-    p.wavePaths = n;
-    p.shadowPerPath = shadowPerPath;
-    p.rng = t->pathAlloc<uint32_t>(n);
-    p.wavelength = t->pathAlloc<float>(n);
-    p.spectrum = t->pathAlloc<float4>(n);
-    p.throughput = t->pathAlloc<float>(n);
-    p.radiance = t->pathAlloc<float>(n);
-    p.rayOrigin = t->pathAlloc<float4>(n);
-    p.rayDirection = t->pathAlloc<float4>(n);
-    p.flags = t->pathAlloc<uint32_t>(n);
-    p.previousPdf = t->pathAlloc<float2>(n);
-    p.medium = t->pathAlloc<float4>(n);
-    p.hit = t->pathAlloc<float4>(n);
-    p.contribution = t->pathAlloc<float>(3 * n);
-    p.contributionValid = t->pathAlloc<uint8_t>(3 * n);
-    p.queue[0] = t->pathAlloc<uint32_t>(n);
-    p.queue[1] = t->pathAlloc<uint32_t>(n);
-    p.hitQueue = t->pathAlloc<uint32_t>(n);
-    p.missQueue = t->pathAlloc<uint32_t>(n);
-    p.shadowOrigin = t->pathAlloc<float4>(ns);
-    p.shadowDirection = t->pathAlloc<float4>(ns);
-    p.shadowFactors = t->pathAlloc<float4>(ns);
-    p.shadowSlot = t->pathAlloc<uint32_t>(ns);
-    p.shadowInfo = t->pathAlloc<uint32_t>(ns);
-    p.counters = t->pathAlloc<uint32_t>(8);
-    p.stats = t->pathAlloc<unsigned long long>(8);
+    uint64_t capacity = std::max<uint64_t>(3, std::min(needed, cap));
+    if (fixed) return std::min(capacity, store.paths.capacity);
+    if (t->wavePaths == 0) {
+        size_t freeBytes = 0, totalBytes = 0;
+        check(cudaMemGetInfo(&freeBytes, &totalBytes), "cudaMemGetInfo");
+        const uint64_t held = store.paths.capacity * (139ull + 56ull * store.paths.shadowPerPath);
+        uint64_t fit = (static_cast<uint64_t>(freeBytes) + held) / 4 * 3 / (139ull + 56ull * kShadowSlots);
+        if (store.paths.shadowPerPath >= kShadowSlots) fit = std::max(fit, store.paths.capacity);  // held buffers serve as is
+        capacity = std::min(capacity, std::max(fit, std::min(capacity, kMinimumAutomaticWave)));
+    }
+    if (store.paths.capacity < capacity || store.paths.shadowPerPath < kShadowSlots) {
+        check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+        store.allocate(capacity, kShadowSlots);
+    }
+    return capacity;
+}
+
+unsigned long long* tracerStats(hdcx_tracer* t)
+{
+    if (!t->statsBuffer.ptr) t->statsBuffer.allocate(8 * sizeof(unsigned long long));
+    return t->statsBuffer.as<unsigned long long>();
 }
 
 // Buffers of the radiance-cache mode for waves of up to `capacity` paths.
@@ -596,6 +701,15 @@ HDCX_API hdcx_status hdcx_create(int32_t device, hdcx_tracer** out)
         delete t;
         return s;
     }
+    if (device >= kArenaDevices) {
+        delete t;
+        return HDCX_ERROR_UNSUPPORTED;
+    }
+    {
+        ArenaPool& pool = arenaPool(device);
+        std::lock_guard<std::mutex> guard(pool.lock);
+        ++pool.tracers;
+    }
     *out = t;
     return HDCX_OK;
 }
@@ -603,8 +717,13 @@ HDCX_API hdcx_status hdcx_create(int32_t device, hdcx_tracer** out)
 HDCX_API void hdcx_destroy(hdcx_tracer* t)
 {
     if (!t) return;
-    cudaSetDevice(t->device);
+    const int device = t->device;
+    cudaSetDevice(device);
     delete t;
+    // The device's last tracer takes the path arenas with it.
+    ArenaPool& pool = arenaPool(device);
+    std::lock_guard<std::mutex> guard(pool.lock);
+    if (--pool.tracers == 0) pool.arenas.clear();
 }
 
 HDCX_API const char* hdcx_last_error(const hdcx_tracer* t) { return t ? t->lastError.c_str() : ""; }
@@ -696,6 +815,7 @@ namespace {
 // kernels overlap on the GPU.
 struct RenderCall {
     FrameConst frame{};
+    PathBuffers paths;  // the buffers this call renders with: the tracer's own, or a batch lane's
     uint64_t pathsNeeded = 0;
     StageTimes times;
     uint64_t launches = 0;
@@ -706,7 +826,7 @@ struct RenderCall {
 
 void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, uint32_t height, uint32_t sampleIndex,
                    uint32_t maxBounces, uint32_t sampleCount, uint64_t waveCap, bool allowStageTiming,
-                   RenderCall& call)
+                   RenderCall& call, PathArena* arena = nullptr, bool fixedArena = false)
 {
     ensureOutput(t, width, height);
     if (!t->fallbackAxisInitialized) {
@@ -715,23 +835,28 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
     }
     call.frame = makeFrame(t, camera, width, height, sampleIndex, maxBounces, sampleCount);
     call.pathsNeeded = uint64_t(width) * height * 3u * call.frame.sampleCount;
-    const uint32_t shadowPerPath = t->scene.lightCount > 0u ? (t->scene.hasMeshLights ? 2u : 1u)
-                                                            : (t->scene.hasMeshLights ? 2u : 3u);
-    ensurePaths(t, call.pathsNeeded, std::max(shadowPerPath, 3u), waveCap);
-    t->paths.traceBlocksPerSm = t->traceBlocksPerSm;
-    t->paths.shadeBlocksPerSm = t->shadeBlocksPerSm;
-    check(cudaMemsetAsync(t->paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
-    t->paths.cache = CacheDevice{};
+    // Radiance-cache renders keep path state of their own; the others use the
+    // arena checked out for the call (a batch lane's arena is `fixed`).
+    PathStore& store = (t->radianceCache || !arena) ? t->own : arena->store;
+    const bool fixed = fixedArena && &store != &t->own;
+    const uint64_t wave = ensureStore(t, store, call.pathsNeeded, waveCap, fixed);
+    call.paths = store.paths;
+    call.paths.wavePaths = wave;
+    call.paths.stats = tracerStats(t);
+    call.paths.traceBlocksPerSm = t->traceBlocksPerSm;
+    call.paths.shadeBlocksPerSm = t->shadeBlocksPerSm;
+    check(cudaMemsetAsync(call.paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
+    call.paths.cache = CacheDevice{};
     if (t->radianceCache) {
-        ensureCacheBuffers(t, t->paths.capacity);
+        ensureCacheBuffers(t, call.paths.capacity);
         CacheDevice c = t->cacheDevice;
         c.enabled = 1u;
         c.prefixBounces = t->cachePrefix;
-        const double wave = static_cast<double>(std::min<uint64_t>(call.pathsNeeded, t->paths.wavePaths));
+        const double wave = static_cast<double>(std::min<uint64_t>(call.pathsNeeded, call.paths.wavePaths));
         c.trainThreshold = static_cast<uint32_t>(std::min(4294967295.0, double(t->cacheTrainingPaths) / wave * 4294967296.0));
         c.sceneMin = t->sceneMin;
         c.sceneScale = t->sceneScale;
-        t->paths.cache = c;
+        call.paths.cache = c;
         t->cacheRun.cache = t->radianceCache->cache;
     }
     call.stageTiming = allowStageTiming && (t->profiling & HDCX_PROFILE_STAGE_TIMES) != 0u;
@@ -739,12 +864,16 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
     call.active = true;
 }
 
-void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut, bool timeEvents = true)
+// `pathsDone` (optional) is recorded once the kernels no longer use the path
+// buffers, before the read-back: the next job of a batch lane waits on it.
+void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut, bool timeEvents = true,
+                   cudaEvent_t pathsDone = nullptr)
 {
     if (timeEvents) check(cudaEventRecord(t->start, t->stream), "cudaEventRecord");
-    renderFrame(t->scene, call.frame, t->paths, t->fb, t->stream, call.stageTiming ? &call.times : nullptr,
+    renderFrame(t->scene, call.frame, call.paths, t->fb, t->stream, call.stageTiming ? &call.times : nullptr,
                 call.counting, &call.launches, t->radianceCache ? &t->cacheRun : nullptr);
     if (timeEvents) check(cudaEventRecord(t->stop, t->stream), "cudaEventRecord");
+    if (pathsDone) check(cudaEventRecord(pathsDone, t->stream), "cudaEventRecord");
     if (rgbaOut) {
         check(cudaMemcpyAsync(rgbaOut, t->fb.rgba, size_t(call.frame.width) * call.frame.height * sizeof(float4),
                               cudaMemcpyDeviceToHost, t->stream),
@@ -758,7 +887,7 @@ void finishRender(hdcx_tracer* t, RenderCall& call, float graphMs = -1.0F)
     check(cudaStreamSynchronize(t->stream), "render");
     t->xyzSamples = (call.frame.sampleIndex == 0 ? 0 : t->xyzSamples) + call.frame.sampleCount;
     unsigned long long counters[8];
-    check(cudaMemcpy(counters, t->paths.stats, sizeof counters, cudaMemcpyDeviceToHost), "read stats");
+    check(cudaMemcpy(counters, call.paths.stats, sizeof counters, cudaMemcpyDeviceToHost), "read stats");
     float ms = graphMs;
     if (graphMs < 0.0F) check(cudaEventElapsedTime(&ms, t->start, t->stop), "cudaEventElapsedTime");
     t->stats = hdcx_render_stats{};
@@ -792,8 +921,11 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint
     if (!t->geometryReady || width == 0 || height == 0) return HDCX_OK;
     if (uint64_t(width) * height > (1ull << 28)) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels");
     return guarded(t, [&] {
+        // The arena stays checked out until the render's work has finished.
+        ArenaLease lease;
+        if (!t->radianceCache) lease = checkoutArena(t->device, true);
         RenderCall call;
-        prepareRender(t, *camera, width, height, sampleIndex, maxBounces, sampleCount, 0, true, call);
+        prepareRender(t, *camera, width, height, sampleIndex, maxBounces, sampleCount, 0, true, call, lease.arena);
         enqueueRender(t, call, rgbaOut);
         finishRender(t, call);
         if (written) *written = 1;
@@ -809,13 +941,135 @@ HDCX_API hdcx_status hdcx_render_batch(hdcx_batch_job* jobs, uint32_t count, uin
 
 namespace {
 
+// A batch renders the jobs of each device in up to kBatchLanes lanes that run
+// concurrently. The jobs of a lane run one after another on the lane's path
+// buffers, which belong to the lane's first tracer and hold up to
+// kBatchLaneWave paths: waves as large as a single render's, where one set of
+// buffers per job would split the device memory among all the jobs.
+constexpr uint32_t kBatchLanes = 4;
+constexpr uint64_t kBatchLaneWave = 48ull << 20;
+
+struct BatchPlan {
+    std::vector<uint32_t> order;     // jobs in enqueue order, lane by lane
+    std::vector<int> lane;           // per job: its lane, or -1 (the tracer's own path state)
+    std::vector<ArenaLease> leases;  // per lane: its arena, held until the batch's work has finished
+};
+
+// Deals the jobs that can share path state (geometry, a non-empty image, no
+// radiance cache) to lanes, largest first onto the lane with the fewest paths,
+// and sizes each lane's arena: its largest job's paths, at most kBatchLaneWave
+// and at most an equal share of the budget (`pathBudget` paths per device, 0:
+// half the device's free memory), never below 1,048,576 paths. Lanes take the
+// arenas that are free; only a batch that holds none yet waits for one, so
+// concurrent batches cannot wait on each other. Jobs left without a lane (no
+// arena, or its buffers could not be allocated) render on their own path state.
+BatchPlan planBatch(hdcx_batch_job* jobs, uint32_t count, uint64_t pathBudget)
+{
+    BatchPlan plan;
+    plan.lane.assign(count, -1);
+    auto need = [&](uint32_t j) {
+        const hdcx_batch_job& b = jobs[j];
+        return uint64_t(b.width) * b.height * 3u * std::max(b.sample_count, 1u);
+    };
+    std::vector<int> devices;
+    for (uint32_t j = 0; j < count; ++j) {
+        if (std::find(devices.begin(), devices.end(), jobs[j].tracer->device) == devices.end())
+            devices.push_back(jobs[j].tracer->device);
+    }
+    for (int device : devices) {
+        std::vector<uint32_t> eligible;
+        for (uint32_t j = 0; j < count; ++j) {
+            const hdcx_batch_job& b = jobs[j];
+            const hdcx_tracer* t = b.tracer;
+            if (t->device == device && t->geometryReady && !t->radianceCache && b.width > 0 && b.height > 0 &&
+                uint64_t(b.width) * b.height <= (1ull << 28))
+                eligible.push_back(j);
+        }
+        if (eligible.empty() || cudaSetDevice(device) != cudaSuccess) continue;
+        std::stable_sort(eligible.begin(), eligible.end(), [&](uint32_t a, uint32_t b) { return need(a) > need(b); });
+        std::vector<ArenaLease> leases;
+        const size_t wanted = std::min<size_t>(kBatchLanes, eligible.size());
+        try {
+            while (leases.size() < wanted) {
+                ArenaLease lease = checkoutArena(device, false);
+                if (!lease.arena) break;
+                leases.push_back(std::move(lease));
+            }
+            if (leases.empty() && plan.leases.empty()) leases.push_back(checkoutArena(device, true));
+        } catch (const std::exception&) {
+        }
+        if (leases.empty()) continue;
+        const uint32_t lanes = static_cast<uint32_t>(leases.size());
+        uint64_t budget = pathBudget;
+        if (budget == 0) {
+            size_t freeBytes = 0, totalBytes = 0;
+            if (cudaMemGetInfo(&freeBytes, &totalBytes) != cudaSuccess) freeBytes = 0;
+            uint64_t held = 0;
+            for (const ArenaLease& l : leases) held += l.arena->store.paths.capacity * kPathStateBytes;
+            budget = (freeBytes + held) / 2 / kPathStateBytes;
+        }
+        std::vector<std::vector<uint32_t>> members(lanes);
+        std::vector<uint64_t> total(lanes, 0);
+        for (uint32_t j : eligible) {
+            const uint32_t l = static_cast<uint32_t>(std::min_element(total.begin(), total.end()) - total.begin());
+            members[l].push_back(j);
+            total[l] += need(j);
+        }
+        for (uint32_t l = 0; l < lanes; ++l) {
+            uint64_t capacity = std::min(need(members[l].front()), kBatchLaneWave);
+            capacity = std::max<uint64_t>(3, std::min(capacity, std::max<uint64_t>(budget / lanes, 1ull << 20)));
+            PathStore& store = leases[l].arena->store;
+            bool ready = true;
+            try {
+                if (store.paths.capacity < capacity || store.paths.shadowPerPath < 3u) store.allocate(capacity, 3u);
+            } catch (const std::exception&) {
+                store.release();
+                cudaGetLastError();
+                ready = false;
+            }
+            if (!ready) {
+                for (uint32_t j : members[l]) plan.order.push_back(j);
+                continue;
+            }
+            const int index = static_cast<int>(plan.leases.size());
+            plan.leases.push_back(std::move(leases[l]));
+            for (uint32_t j : members[l]) {
+                plan.lane[j] = index;
+                plan.order.push_back(j);
+            }
+        }
+    }
+    for (uint32_t j = 0; j < count; ++j) {
+        if (std::find(plan.order.begin(), plan.order.end(), j) == plan.order.end()) plan.order.push_back(j);
+    }
+    return plan;
+}
+
+// Events of one batch call, destroyed with it.
+struct BatchEvents {
+    std::vector<cudaEvent_t> events;
+    explicit BatchEvents(uint32_t count) : events(count, nullptr) {}
+    BatchEvents(const BatchEvents&) = delete;
+    BatchEvents& operator=(const BatchEvents&) = delete;
+    ~BatchEvents()
+    {
+        for (cudaEvent_t e : events)
+            if (e) cudaEventDestroy(e);
+    }
+    cudaEvent_t make(uint32_t j)
+    {
+        if (!events[j]) check(cudaEventCreateWithFlags(&events[j], cudaEventDisableTiming), "cudaEventCreate");
+        return events[j];
+    }
+};
+
 // Captures the kernels of every active job (each on its own tracer's stream,
 // forked from and joined into one capture stream) into a single CUDA graph,
 // launches it once, then queues the read-backs. Returns the graph's device
 // time, or a negative value (nothing launched) when the batch cannot be
 // captured: jobs on several devices, a job in radiance-cache mode (it
 // synchronises with the host per wave) or a capture error.
-float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<RenderCall>& calls)
+float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<RenderCall>& calls, const BatchPlan& plan)
 {
     int device = -1;
     for (uint32_t j = 0; j < count; ++j) {
@@ -855,16 +1109,21 @@ float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<Render
     try {
         if (captured) {
             check(cudaEventRecord(fork, batch), "fork");
-            for (uint32_t j = 0; j < count; ++j) {
+            // A job starts after the fork, or after the previous job of its lane.
+            std::vector<cudaEvent_t> laneDone(plan.leases.size(), nullptr);
+            for (uint32_t j : plan.order) {
                 if (!calls[j].active) continue;
                 hdcx_tracer* t = jobs[j].tracer;
-                check(cudaStreamWaitEvent(t->stream, fork, 0), "join the capture");
+                const int lane = plan.lane[j];
+                check(cudaStreamWaitEvent(t->stream, lane >= 0 && laneDone[lane] ? laneDone[lane] : fork, 0),
+                      "join the capture");
                 enqueueRender(t, calls[j], nullptr, false);
                 cudaEvent_t join = nullptr;
                 check(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), "cudaEventCreate");
                 joins.push_back(join);
                 check(cudaEventRecord(join, t->stream), "join");
                 check(cudaStreamWaitEvent(batch, join, 0), "join");
+                if (lane >= 0) laneDone[lane] = join;
             }
         }
     } catch (const std::exception&) {
@@ -913,50 +1172,14 @@ HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, 
         }
     }
     std::vector<RenderCall> calls(count);
-    // Wave sizes: every job gets min(its paths, the automatic wave) unless the
-    // jobs on one device would then hold more path state than the budget
-    // (default: half of the device's free memory), in which case the waves
-    // shrink in proportion (never below 1M paths).
-    std::vector<uint64_t> caps(count, 0);
-    {
-        std::vector<int> devices;
-        for (uint32_t j = 0; j < count; ++j) {
-            if (std::find(devices.begin(), devices.end(), jobs[j].tracer->device) == devices.end())
-                devices.push_back(jobs[j].tracer->device);
-        }
-        for (int device : devices) {
-            uint64_t budget = pathBudget;
-            if (budget == 0) {
-                size_t freeBytes = 0, totalBytes = 0;
-                if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&freeBytes, &totalBytes) != cudaSuccess)
-                    freeBytes = 0;
-                budget = freeBytes / 2 / kPathStateBytes;
-            }
-            uint64_t wanted = 0;
-            for (uint32_t j = 0; j < count; ++j) {
-                if (jobs[j].tracer->device != device) continue;
-                const hdcx_batch_job& b = jobs[j];
-                const uint64_t need = uint64_t(b.width) * b.height * 3u * std::max(b.sample_count, 1u);
-                caps[j] = std::max<uint64_t>(3, std::min(need, kAutomaticWavePaths));
-                wanted += caps[j];
-            }
-            if (budget > 0 && wanted > budget) {
-                for (uint32_t j = 0; j < count; ++j) {
-                    if (jobs[j].tracer->device != device) continue;
-                    const double share = static_cast<double>(caps[j]) / static_cast<double>(wanted);
-                    caps[j] = std::max<uint64_t>(std::min<uint64_t>(caps[j], 1ull << 20),
-                                                 static_cast<uint64_t>(share * static_cast<double>(budget)));
-                }
-            }
-        }
-    }
     auto record = [&](uint32_t j, hdcx_status status) {
         if (status != HDCX_OK) {
             jobs[j].status = status;
             calls[j].active = false;
         }
     };
-    for (uint32_t j = 0; j < count; ++j) {
+    const BatchPlan plan = planBatch(jobs, count, pathBudget);
+    for (uint32_t j : plan.order) {
         hdcx_batch_job& b = jobs[j];
         hdcx_tracer* t = b.tracer;
         if (!t->geometryReady || b.width == 0 || b.height == 0) continue;
@@ -964,16 +1187,32 @@ HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, 
             record(j, fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels"));
             continue;
         }
+        PathArena* arena = plan.lane[j] >= 0 ? plan.leases[plan.lane[j]].arena : nullptr;
+        const uint64_t laneWave = arena ? arena->store.paths.capacity : 0;
         record(j, guarded(t, [&] {
-            prepareRender(t, b.camera, b.width, b.height, b.sample_index, b.max_bounces, b.sample_count, caps[j], false,
-                          calls[j]);
+            prepareRender(t, b.camera, b.width, b.height, b.sample_index, b.max_bounces, b.sample_count, laneWave,
+                          false, calls[j], arena, true);
         }));
     }
-    const float graphMs = (flags & HDCX_BATCH_CUDA_GRAPH) ? enqueueBatchGraph(jobs, count, calls) : -1.0F;
+    BatchEvents events(count);
+    const float graphMs = (flags & HDCX_BATCH_CUDA_GRAPH) ? enqueueBatchGraph(jobs, count, calls, plan) : -1.0F;
     if (graphMs < 0.0F) {
-        for (uint32_t j = 0; j < count; ++j) {
+        // Lane by lane: a job waits until the previous job of its lane no
+        // longer uses the lane's path buffers.
+        std::vector<cudaEvent_t> laneDone(plan.leases.size(), nullptr);
+        for (uint32_t j : plan.order) {
             if (!calls[j].active) continue;
-            record(j, guarded(jobs[j].tracer, [&] { enqueueRender(jobs[j].tracer, calls[j], jobs[j].rgba_out); }));
+            hdcx_tracer* t = jobs[j].tracer;
+            const int lane = plan.lane[j];
+            record(j, guarded(t, [&] {
+                cudaEvent_t done = nullptr;
+                if (lane >= 0) {
+                    if (laneDone[lane]) check(cudaStreamWaitEvent(t->stream, laneDone[lane], 0), "lane order");
+                    done = events.make(j);
+                }
+                enqueueRender(t, calls[j], jobs[j].rgba_out, true, done);
+                if (lane >= 0) laneDone[lane] = done;
+            }));
         }
     }
     hdcx_status overall = HDCX_OK;
@@ -1286,6 +1525,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
     return guarded(t, [&] {
         const uint32_t savedProfiling = t->profiling;
         t->profiling = 0;
+        ArenaLease lease = checkoutArena(t->device, true);  // one arena for every timed render
         // Best of two device-timed renders of one configuration.
         auto measure = [&](uint64_t wave, uint32_t trace, uint32_t shade) {
             t->wavePaths = wave;
@@ -1294,7 +1534,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
             double ms = 1e30;
             for (int rep = 0; rep < 2; ++rep) {
                 RenderCall call;
-                prepareRender(t, *camera, width, height, 0, maxBounces, sampleCount, 0, false, call);
+                prepareRender(t, *camera, width, height, 0, maxBounces, sampleCount, 0, false, call, lease.arena);
                 enqueueRender(t, call, nullptr);
                 finishRender(t, call);
                 ms = std::min(ms, t->stats.render_ms);
@@ -1320,10 +1560,10 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         };
         // Waves above the automatic size shorten the launches' tails; they are
         // tried while their path state stays within half the device memory
-        // that is free or already held by this tracer's path buffers.
+        // that is free or already held by the arena.
         size_t freeBytes = 0, totalBytes = 0;
         check(cudaMemGetInfo(&freeBytes, &totalBytes), "cudaMemGetInfo");
-        const uint64_t pathBytesLimit = (freeBytes + t->paths.capacity * kPathStateBytes) / 2;
+        const uint64_t pathBytesLimit = (freeBytes + lease.arena->store.paths.capacity * kPathStateBytes) / 2;
         for (uint64_t wave : {48ull << 20, 32ull << 20, 24ull << 20, 16ull << 20, 8ull << 20, 4ull << 20, 2ull << 20,
                               1ull << 20}) {
             if (wave < needed && wave * kPathStateBytes <= pathBytesLimit)
@@ -1331,12 +1571,12 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         }
         for (uint32_t trace : {8u, 32u, 64u}) consider(best.wave_paths, trace, best.shade_blocks_per_sm);
         for (uint32_t shade : {2u, 4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade);
-        // Buffers grown for a larger candidate than the one chosen are released;
-        // the next render allocates the chosen wave.
+        // Arena buffers grown for a larger candidate than the one chosen are
+        // released; the next render allocates the chosen wave.
         const uint64_t chosen = std::max<uint64_t>(3, std::min(needed, best.wave_paths ? best.wave_paths : kAutomaticWavePaths));
-        if (t->paths.capacity > chosen) {
+        if (lease.arena->store.paths.capacity > chosen) {
             check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
-            t->clearPaths();
+            lease.arena->store.release();
         }
         t->wavePaths = best.wave_paths;
         t->traceBlocksPerSm = best.trace_blocks_per_sm;

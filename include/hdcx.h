@@ -412,7 +412,15 @@ HDCX_API int32_t hdcx_get_shading_mode(const hdcx_tracer* tracer);
  * max_bounces is clamped to [1, 12]. When rgba_out is not NULL the whole
  * RGBA32F image (width*height*4 floats, row 0 = bottom) is copied into it.
  * With no geometry or a zero size nothing is traced and *written = 0
- * (the reference returns an empty vector, :3235); otherwise *written = 1. */
+ * (the reference returns an empty vector, :3235); otherwise *written = 1.
+ * Device memory: the path state of a wave (about 307 bytes per path) lives in
+ * a per-device pool of arenas, not in the tracer: a call checks out a free
+ * arena (at most eight per device; when all are busy it waits for one) and
+ * grows it to its wave, and the arenas are freed with the device's last
+ * tracer. Tracers that render one after another therefore share one arena.
+ * Automatic waves take at most three quarters of the free device memory plus
+ * what the arena holds. A tracer in radiance-cache mode keeps path state of
+ * its own. */
 HDCX_API hdcx_status hdcx_render(hdcx_tracer* tracer, const hdcx_camera* camera,
                                  uint32_t width, uint32_t height,
                                  uint32_t sample_index, uint32_t max_bounces,
@@ -463,13 +471,18 @@ HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* tracer, const hdcx_camera* 
  * scenes (a farm of small shots, turntables, look-development variants).
  * Each tracer appears in at most one job (HDCX_ERROR_INVALID_ARGUMENT
  * otherwise). Tracers may live on different devices. Per-stage times are not
- * recorded for batched jobs. Path state: every job gets waves of
- * min(its paths, the automatic wave) unless the jobs on a device would then
- * hold more than `path_budget` paths of path state (0: half of the device's
- * free memory at the call), in which case the waves shrink in proportion
- * (never below 1,048,576 paths); a wave size set with hdcx_set_wave_size
- * wins. Returns HDCX_OK when every job succeeded, else the first failing
- * job's status; each job's own status is in its `status`. */
+ * recorded for batched jobs. Path state: the jobs of a device are dealt,
+ * largest first, to up to four lanes that run concurrently, one path arena
+ * (see hdcx_render) per lane; the jobs of a lane run one after another on its
+ * arena. A lane holds waves of its largest job's paths, at most 50,331,648
+ * paths and at most an equal share of `path_budget` paths of path state per
+ * device (0: half of the device's free memory at the call), never below
+ * 1,048,576 paths; a wave size set with hdcx_set_wave_size bounds its own
+ * job's waves. A batch takes the arenas that are free and waits only while it
+ * holds none. Jobs in radiance-cache mode render on their own tracers' path
+ * state. Returns HDCX_OK when every job
+ * succeeded, else the first failing job's status; each job's own status is in
+ * its `status`. */
 HDCX_API hdcx_status hdcx_render_batch(hdcx_batch_job* jobs, uint32_t count, uint64_t path_budget);
 
 /* hdcx_render_batch with options. HDCX_BATCH_CUDA_GRAPH: the kernels of all
@@ -521,8 +534,8 @@ HDCX_API hdcx_status hdcx_set_tuning(hdcx_tracer* tracer, const hdcx_tuning* tun
  * grid sizes, one knob at a time from the defaults, keeps the fastest on the
  * tracer and returns it. Wave sizes of 1M to 48M paths are tried, the larger
  * ones while their path state (about 307 bytes per path) fits half of the free
- * device memory; path buffers grown for a candidate larger than the one kept
- * are released before it returns. Results are cached per device and workload shape
+ * device memory; a path arena grown for a candidate larger than the one kept
+ * is released before it returns. Results are cached per device and workload shape
  * (triangles, pixels, samples, bounces, shading variant) for the process, so
  * a repeated call times nothing. The tuning renders overwrite the tracer's
  * accumulation: render with sample_index 0 afterwards. */

@@ -99,3 +99,35 @@ def test_batch_job_without_geometry_writes_nothing():
         assert results[0]["written"] == 0 and results[0]["status"] == 0
         assert results[1]["written"] == 1
         assert not a.any() and b[..., 3].min() == 1.0
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_jobs_sharing_lane_buffers_equal_sequential(graph):
+    """Eleven jobs: more than the batch's lanes, so several jobs render one
+    after another on one lane's path buffers. Each job's image and counters
+    equal its own hdcx_render call."""
+    spec = [(workloads.closed_box(width=w, height=h, spp=spp), w, h, spp)
+            for w, h, spp in [(96, 64, 3), (64, 64, 2), (128, 72, 1), (80, 80, 4), (32, 48, 5), (72, 40, 2),
+                              (100, 60, 2), (48, 48, 6), (120, 90, 1), (56, 72, 3), (64, 32, 7)]]
+    expected = []
+    for wl, w, h, spp in spec:
+        with PathTracer(0) as t:
+            t.set_scene(wl.scene)
+            expected.append((t.render(wl.camera, w, h, 0, 8, spp), t.stats()))
+    tracers = [PathTracer(0) for _ in spec]
+    try:
+        for t, (wl, *_rest) in zip(tracers, spec):
+            t.set_scene(wl.scene)
+        images = [np.zeros((h, w, 4), np.float32) for _, w, h, _ in spec]
+        jobs = [(t, wl.camera, w, h, 0, 8, spp, img) for t, (wl, w, h, spp), img in zip(tracers, spec, images)]
+        results = render_batch(jobs, 0, graph=graph)
+        assert all(r["written"] == 1 and r["status"] == 0 for r in results)
+        for k, (img, t) in enumerate(zip(images, tracers)):
+            ref, stats = expected[k]
+            assert np.array_equal(img, ref), k
+            got = t.stats()
+            for key in ("spectral_paths", "extension_rays", "shadow_rays"):
+                assert got[key] == stats[key], (k, key)
+    finally:
+        for t in tracers:
+            t.close()
