@@ -292,11 +292,12 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
 // sampling (:1670-1731) can run; both are compiled out.
 // kCache: radiance-cache mode (PathBuffers::cache): queries and training
 // records at surface vertices; the plain kernels compile without it.
-// The lit, non-full variants wait on memory most of the time (long-scoreboard
-// stalls): they are capped at 80 registers so that six blocks fit an SM
-// instead of four, which costs a few spilled values and gains 6% of their time.
+// The lit variants wait on memory most of the time (long-scoreboard stalls):
+// the non-full ones are capped at 80 registers so that six blocks fit an SM
+// instead of four, the full ones at 128 registers for four blocks instead of
+// three; each costs a few spilled values and gains 4-6% of the kernel's time.
 template <bool kFull, bool kLit, bool kCache>
-__global__ void __launch_bounds__(128, (!kFull && kLit) ? 6 : 1)
+__global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
     shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce, const uint32_t* queue,
                 const uint32_t* count, uint32_t* nextQueue, uint32_t* nextCount)
 {
