@@ -1204,15 +1204,21 @@ HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, 
             if (!calls[j].active) continue;
             hdcx_tracer* t = jobs[j].tracer;
             const int lane = plan.lane[j];
-            record(j, guarded(t, [&] {
-                cudaEvent_t done = nullptr;
+            cudaEvent_t done = nullptr;
+            const hdcx_status st = guarded(t, [&] {
                 if (lane >= 0) {
-                    if (laneDone[lane]) check(cudaStreamWaitEvent(t->stream, laneDone[lane], 0), "lane order");
                     done = events.make(j);
+                    if (laneDone[lane]) check(cudaStreamWaitEvent(t->stream, laneDone[lane], 0), "lane order");
                 }
                 enqueueRender(t, calls[j], jobs[j].rgba_out, true, done);
-                if (lane >= 0) laneDone[lane] = done;
-            }));
+            });
+            if (lane >= 0 && done) {
+                // A job that failed part-way may have launched kernels on the
+                // arena: the lane's next job waits for its stream all the same.
+                if (st != HDCX_OK) cudaEventRecord(done, t->stream);
+                laneDone[lane] = done;
+            }
+            record(j, st);
         }
     }
     hdcx_status overall = HDCX_OK;
