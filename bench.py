@@ -68,8 +68,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default="",
-                    help="wave_paths,trace_blocks_per_sm,shade_blocks_per_sm to use instead of autotuning "
-                         "(to repeat a tuned run, e.g. under a profiler)")
+                    help="wave_paths,trace_blocks_per_sm,shade_blocks_per_sm[,sort_hits] to use instead of "
+                         "autotuning (to repeat a tuned run, e.g. under a profiler)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip hdcx_autotune (by default it picks wave and grid sizes before the warm-up; setup, "
                          "not timed)")
@@ -537,8 +537,9 @@ def run_hdcx(args):
     tracer.set_scene(wl.scene)
     tuning = None
     if args.tuning:
-        wave, trace, shade = (int(x) for x in args.tuning.split(","))
-        tracer.set_tuning(wave_paths=wave, trace_blocks_per_sm=trace, shade_blocks_per_sm=shade)
+        knobs = [int(x) for x in args.tuning.split(",")] + [0]
+        tracer.set_tuning(wave_paths=knobs[0], trace_blocks_per_sm=knobs[1], shade_blocks_per_sm=knobs[2],
+                          sort_hits=knobs[3])
     elif args.autotune and not args.profile:
         tuning = tracer.autotune(wl.camera, wl.width, wl.height, wl.max_bounces, wl.spp)
     if args.profile:

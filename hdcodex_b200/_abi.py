@@ -267,7 +267,7 @@ class Tuning(C.Structure):
         ("milliseconds", C.c_double),
         ("default_milliseconds", C.c_double),
         ("candidates", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("sort_hits", C.c_uint32),
     ]
 
 

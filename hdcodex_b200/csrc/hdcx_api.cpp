@@ -123,13 +123,15 @@ struct PathStore {
         p.shadowSlot = alloc<uint32_t>(ns);
         p.shadowInfo = alloc<uint32_t>(ns);
         p.counters = alloc<uint32_t>(8);
+        p.sortedHits = alloc<uint32_t>(n);
+        p.hitBins = alloc<uint32_t>(2 * kHitBins);
     }
 };
 
 // ---------------------------------------------------------------------------
 // Path arenas
 //
-// A render needs the path state of its waves (about 307 bytes per path) only
+// A render needs the path state of its waves (about 311 bytes per path) only
 // while it runs, so path state belongs to a per-device pool of arenas rather
 // than to tracers: hdcx_render and hdcx_autotune check an arena out for the
 // call, hdcx_render_batch one per lane until the batch's work has finished.
@@ -219,6 +221,7 @@ struct hdcx_tracer {
     uint64_t wavePaths = 0;  // 0 = automatic
     uint32_t traceBlocksPerSm = 16;
     uint32_t shadeBlocksPerSm = 8;
+    uint32_t sortHits = 0;   // shade hits in material order
     uint32_t profiling = 0;  // HDCX_PROFILE_* bits
     // Scene.
     std::vector<DeviceBuffer*> sceneBuffers;
@@ -497,7 +500,7 @@ void ensureOutput(hdcx_tracer* t, uint32_t w, uint32_t h)
 
 constexpr uint64_t kAutomaticWavePaths = 12ull << 20;  // ~12.6M paths per wave
 // Device bytes of path state per path (PathBuffers with three shadow slots).
-constexpr uint64_t kPathStateBytes = 139 + 3 * 56;
+constexpr uint64_t kPathStateBytes = 143 + 3 * 56;
 
 // Smallest wave an automatic wave is shrunk to when device memory is short.
 constexpr uint64_t kMinimumAutomaticWave = 1ull << 16;
@@ -519,8 +522,8 @@ uint64_t ensureStore(hdcx_tracer* t, PathStore& store, uint64_t needed, uint64_t
     if (t->wavePaths == 0) {
         size_t freeBytes = 0, totalBytes = 0;
         check(cudaMemGetInfo(&freeBytes, &totalBytes), "cudaMemGetInfo");
-        const uint64_t held = store.paths.capacity * (139ull + 56ull * store.paths.shadowPerPath);
-        uint64_t fit = (static_cast<uint64_t>(freeBytes) + held) / 4 * 3 / (139ull + 56ull * kShadowSlots);
+        const uint64_t held = store.paths.capacity * (143ull + 56ull * store.paths.shadowPerPath);
+        uint64_t fit = (static_cast<uint64_t>(freeBytes) + held) / 4 * 3 / (143ull + 56ull * kShadowSlots);
         if (store.paths.shadowPerPath >= kShadowSlots) fit = std::max(fit, store.paths.capacity);  // held buffers serve as is
         capacity = std::min(capacity, std::max(fit, std::min(capacity, kMinimumAutomaticWave)));
     }
@@ -845,6 +848,7 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
     call.paths.stats = tracerStats(t);
     call.paths.traceBlocksPerSm = t->traceBlocksPerSm;
     call.paths.shadeBlocksPerSm = t->shadeBlocksPerSm;
+    call.paths.sortHits = t->sortHits;
     check(cudaMemsetAsync(call.paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
     call.paths.cache = CacheDevice{};
     if (t->radianceCache) {
@@ -1468,6 +1472,7 @@ HDCX_API hdcx_status hdcx_get_tuning(const hdcx_tracer* t, hdcx_tuning* out)
     out->wave_paths = t->wavePaths;
     out->trace_blocks_per_sm = t->traceBlocksPerSm;
     out->shade_blocks_per_sm = t->shadeBlocksPerSm;
+    out->sort_hits = t->sortHits;
     return HDCX_OK;
 }
 
@@ -1475,11 +1480,13 @@ HDCX_API hdcx_status hdcx_set_tuning(hdcx_tracer* t, const hdcx_tuning* in)
 {
     if (!t || !in) return HDCX_ERROR_INVALID_ARGUMENT;
     if ((in->wave_paths != 0 && in->wave_paths < 3) || in->trace_blocks_per_sm < 1 || in->trace_blocks_per_sm > 64 ||
-        in->shade_blocks_per_sm < 1 || in->shade_blocks_per_sm > 64)
-        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "tuning out of range (wave >= 3 paths or 0, 1..64 blocks per SM)");
+        in->shade_blocks_per_sm < 1 || in->shade_blocks_per_sm > 64 || in->sort_hits > 1)
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT,
+                    "tuning out of range (wave >= 3 paths or 0, 1..64 blocks per SM, sort_hits 0 or 1)");
     t->wavePaths = in->wave_paths;
     t->traceBlocksPerSm = in->trace_blocks_per_sm;
     t->shadeBlocksPerSm = in->shade_blocks_per_sm;
+    t->sortHits = in->sort_hits;
     return HDCX_OK;
 }
 
@@ -1522,6 +1529,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
                 t->wavePaths = cached.wave_paths;
                 t->traceBlocksPerSm = cached.trace_blocks_per_sm;
                 t->shadeBlocksPerSm = cached.shade_blocks_per_sm;
+                t->sortHits = cached.sort_hits;
                 if (result) *result = cached;
                 return HDCX_OK;
             }
@@ -1533,10 +1541,11 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         t->profiling = 0;
         ArenaLease lease = checkoutArena(t->device, true);  // one arena for every timed render
         // Best of two device-timed renders of one configuration.
-        auto measure = [&](uint64_t wave, uint32_t trace, uint32_t shade) {
+        auto measure = [&](uint64_t wave, uint32_t trace, uint32_t shade, uint32_t sort = 0) {
             t->wavePaths = wave;
             t->traceBlocksPerSm = trace;
             t->shadeBlocksPerSm = shade;
+            t->sortHits = sort;
             double ms = 1e30;
             for (int rep = 0; rep < 2; ++rep) {
                 RenderCall call;
@@ -1554,14 +1563,15 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         best.default_milliseconds = measure(0, 16, 8);
         best.milliseconds = best.default_milliseconds;
         best.candidates = 1;
-        auto consider = [&](uint64_t wave, uint32_t trace, uint32_t shade) {
-            const double ms = measure(wave, trace, shade);
+        auto consider = [&](uint64_t wave, uint32_t trace, uint32_t shade, uint32_t sort = 0) {
+            const double ms = measure(wave, trace, shade, sort);
             ++best.candidates;
             if (ms < best.milliseconds) {
                 best.milliseconds = ms;
                 best.wave_paths = wave;
                 best.trace_blocks_per_sm = trace;
                 best.shade_blocks_per_sm = shade;
+                best.sort_hits = sort;
             }
         };
         // Waves above the automatic size shorten the launches' tails; they are
@@ -1577,6 +1587,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         }
         for (uint32_t trace : {8u, 32u, 64u}) consider(best.wave_paths, trace, best.shade_blocks_per_sm);
         for (uint32_t shade : {2u, 4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade);
+        consider(best.wave_paths, best.trace_blocks_per_sm, best.shade_blocks_per_sm, 1u);
         // Arena buffers grown for a larger candidate than the one chosen are
         // released; the next render allocates the chosen wave.
         const uint64_t chosen = std::max<uint64_t>(3, std::min(needed, best.wave_paths ? best.wave_paths : kAutomaticWavePaths));
@@ -1587,6 +1598,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         t->wavePaths = best.wave_paths;
         t->traceBlocksPerSm = best.trace_blocks_per_sm;
         t->shadeBlocksPerSm = best.shade_blocks_per_sm;
+        t->sortHits = best.sort_hits;
         t->profiling = savedProfiling;
         {
             std::lock_guard<std::mutex> lock(gTuningLock);

@@ -1132,6 +1132,80 @@ void uploadSrgbTable(const float* table256, cudaStream_t stream)
     CUDA_OK(cudaMemcpyToSymbolAsync(cSrgbToLinear, table256, 256 * sizeof(float), 0, cudaMemcpyHostToDevice, stream));
 }
 
+// ---------------------------------------------------------------------------
+// hit sort: the hit queue in material order, so that a shading warp's lanes
+// run the same material's code (scenes whose materials take very different
+// paths: glass, subsurface walks, cut-out leaves). A counting sort over
+// material bins: per-block shared histograms, one global reservation per bin
+// and block iteration. Order within a bin is arbitrary; every path's result
+// is independent of queue order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t hitMaterialBin(const DeviceScene& s, const PathBuffers& p, uint32_t slot)
+{
+    const uint32_t primitive = __float_as_uint(p.hit[slot].y);
+    return __ldg(s.triangleMaterials + primitive) % kHitBins;
+}
+
+__global__ void __launch_bounds__(256) countHitBinsKernel(DeviceScene s, PathBuffers p)
+{
+    __shared__ uint32_t histogram[kHitBins];
+    for (uint32_t b = threadIdx.x; b < kHitBins; b += blockDim.x) histogram[b] = 0u;
+    __syncthreads();
+    const uint32_t n = p.counters[4];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(&histogram[hitMaterialBin(s, p, p.hitQueue[i])], 1u);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < kHitBins; b += blockDim.x)
+        if (histogram[b] != 0u) atomicAdd(p.hitBins + b, histogram[b]);
+}
+
+// Exclusive prefix sum of the bin counts into the cursors (one warp).
+__global__ void scanHitBinsKernel(PathBuffers p)
+{
+    constexpr uint32_t kPerLane = kHitBins / 32u;
+    const uint32_t lane = threadIdx.x;
+    uint32_t counts[kPerLane];
+    uint32_t local = 0u;
+    for (uint32_t k = 0; k < kPerLane; ++k) {
+        counts[k] = p.hitBins[lane * kPerLane + k];
+        local += counts[k];
+    }
+    uint32_t inclusive = local;
+    for (uint32_t d = 1; d < 32u; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, inclusive, d);
+        if (lane >= d) inclusive += v;
+    }
+    uint32_t offset = inclusive - local;
+    for (uint32_t k = 0; k < kPerLane; ++k) {
+        p.hitBins[kHitBins + lane * kPerLane + k] = offset;
+        offset += counts[k];
+    }
+}
+
+__global__ void __launch_bounds__(256) scatterHitsKernel(DeviceScene s, PathBuffers p)
+{
+    __shared__ uint32_t histogram[kHitBins];
+    __shared__ uint32_t start[kHitBins];
+    const uint32_t n = p.counters[4];
+    // The loop bound is the same for every thread of the block (base is
+    // per block), so the barriers inside are reached by all of them.
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        for (uint32_t b = threadIdx.x; b < kHitBins; b += blockDim.x) histogram[b] = 0u;
+        __syncthreads();
+        const uint32_t i = base + threadIdx.x;
+        const bool valid = i < n;
+        const uint32_t slot = valid ? p.hitQueue[i] : 0u;
+        const uint32_t bin = valid ? hitMaterialBin(s, p, slot) : 0u;
+        const uint32_t rank = valid ? atomicAdd(&histogram[bin], 1u) : 0u;
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < kHitBins; b += blockDim.x)
+            if (histogram[b] != 0u) start[b] = atomicAdd(p.hitBins + kHitBins + b, histogram[b]);
+        __syncthreads();
+        if (valid) p.sortedHits[start[bin] + rank] = slot;
+        __syncthreads();
+    }
+}
+
 template <bool kCache>
 void launchShade(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, uint32_t bounce, const uint32_t* inQueue,
                  const uint32_t* inCount, uint32_t* outQueue, uint32_t* outCount, int grid, cudaStream_t stream)
@@ -1160,6 +1234,8 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
     const int traceGrid = gridFor(static_cast<uint32_t>(wavePaths), static_cast<int>(std::max(paths.traceBlocksPerSm, 1u)));
     const int shadeGrid = gridFor(static_cast<uint32_t>(wavePaths), static_cast<int>(std::max(paths.shadeBlocksPerSm, 1u)));
     const int missGrid = gridFor(static_cast<uint32_t>(wavePaths), 8);
+    const bool sortHits = paths.sortHits != 0u && paths.sortedHits != nullptr && paths.hitBins != nullptr;
+    const int sortGrid = std::max(1, gridFor(static_cast<uint32_t>(wavePaths), 8) / 2);  // 256-thread blocks
     std::vector<EventPair> events;
     auto timed = [&](int stage, auto&& launch) {
         if (!timing) {
@@ -1198,8 +1274,16 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
             CUDA_OK(cudaMemsetAsync(outCount, 0, sizeof(uint32_t), stream));
             CUDA_OK(cudaMemsetAsync(paths.counters + 2, 0, sizeof(uint32_t), stream));
             timed(1, [&] {
-                if (cacheMode) launchShade<true>(scene, frame, paths, bounce, paths.hitQueue, paths.counters + 4, outQueue, outCount, shadeGrid, stream);
-                else launchShade<false>(scene, frame, paths, bounce, paths.hitQueue, paths.counters + 4, outQueue, outCount, shadeGrid, stream);
+                const uint32_t* hits = paths.hitQueue;
+                if (sortHits) {
+                    CUDA_OK(cudaMemsetAsync(paths.hitBins, 0, 2 * kHitBins * sizeof(uint32_t), stream));
+                    countHitBinsKernel<<<sortGrid, 256, 0, stream>>>(scene, paths);
+                    scanHitBinsKernel<<<1, 32, 0, stream>>>(paths);
+                    scatterHitsKernel<<<sortGrid, 256, 0, stream>>>(scene, paths);
+                    hits = paths.sortedHits;
+                }
+                if (cacheMode) launchShade<true>(scene, frame, paths, bounce, hits, paths.counters + 4, outQueue, outCount, shadeGrid, stream);
+                else launchShade<false>(scene, frame, paths, bounce, hits, paths.counters + 4, outQueue, outCount, shadeGrid, stream);
                 missKernel<<<missGrid, 128, 0, stream>>>(scene, frame, paths);
             });
             CUDA_OK(cudaGetLastError());
@@ -1213,7 +1297,7 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
                 }
             });
             CUDA_OK(cudaGetLastError());
-            launched += 4;
+            launched += sortHits ? 7 : 4;
         }
         if (cacheMode) {
             // Predictions for the terminated paths, then one training round on

@@ -34,6 +34,9 @@ struct CacheDevice {
     uint32_t* counters = nullptr;      // [0] queries, [1] training paths, [2] training samples
 };
 
+// Material bins of the hit sort (material index modulo kHitBins).
+constexpr uint32_t kHitBins = 256;
+
 // Device buffers of one wave of paths (structure of arrays, 16-byte records).
 struct PathBuffers {
     uint64_t capacity = 0;          // paths the buffers hold (the stride of the per-slot arrays)
@@ -69,6 +72,12 @@ struct PathBuffers {
     // and shade kernels (the autotuner's knobs; results do not depend on them).
     uint32_t traceBlocksPerSm = 16;
     uint32_t shadeBlocksPerSm = 8;
+    // Hits shaded in material order (sortHits = 1): the hit queue is counted
+    // and scattered into sortedHits by material bin; hitBins holds the bins'
+    // counts, then their cursors (2 x kHitBins).
+    uint32_t sortHits = 0;
+    uint32_t* sortedHits = nullptr;
+    uint32_t* hitBins = nullptr;
 };
 
 // Per-pixel accumulation buffers of the current output size.

@@ -231,9 +231,9 @@ class PathTracer:
         self._check(lib().hdcx_get_tuning(self._h, C.byref(r)), "get_tuning")
         return {name: getattr(r, name) for name, _ in _abi.Tuning._fields_}
 
-    def set_tuning(self, wave_paths=0, trace_blocks_per_sm=16, shade_blocks_per_sm=8):
+    def set_tuning(self, wave_paths=0, trace_blocks_per_sm=16, shade_blocks_per_sm=8, sort_hits=0):
         r = _abi.Tuning(wave_paths=wave_paths, trace_blocks_per_sm=trace_blocks_per_sm,
-                        shade_blocks_per_sm=shade_blocks_per_sm)
+                        shade_blocks_per_sm=shade_blocks_per_sm, sort_hits=sort_hits)
         self._check(lib().hdcx_set_tuning(self._h, C.byref(r)), "set_tuning")
 
     def radiance_cache_stats(self) -> dict:

@@ -333,7 +333,7 @@ typedef struct hdcx_tuning {
     double milliseconds;           /* hdcx_autotune: device time of the best configuration */
     double default_milliseconds;   /* hdcx_autotune: device time of the defaults */
     uint32_t candidates;           /* hdcx_autotune: configurations timed (0: taken from the cache) */
-    uint32_t reserved;
+    uint32_t sort_hits;            /* 1: hits are shaded in material order (a counting sort per bounce); default 0 */
 } hdcx_tuning;
 
 /* Profiling switches for hdcx_set_profiling. */
@@ -413,7 +413,7 @@ HDCX_API int32_t hdcx_get_shading_mode(const hdcx_tracer* tracer);
  * RGBA32F image (width*height*4 floats, row 0 = bottom) is copied into it.
  * With no geometry or a zero size nothing is traced and *written = 0
  * (the reference returns an empty vector, :3235); otherwise *written = 1.
- * Device memory: the path state of a wave (about 307 bytes per path) lives in
+ * Device memory: the path state of a wave (about 311 bytes per path) lives in
  * a per-device pool of arenas, not in the tracer: a call checks out a free
  * arena (at most eight per device; when all are busy it waits for one) and
  * grows it to its wave, and the arenas are freed with the device's last
@@ -531,9 +531,9 @@ HDCX_API hdcx_status hdcx_get_tuning(const hdcx_tracer* tracer, hdcx_tuning* tun
 HDCX_API hdcx_status hdcx_set_tuning(hdcx_tracer* tracer, const hdcx_tuning* tuning);
 /* Autotuner (no counterpart in the reference): times renders of this camera,
  * size, bounce budget and sample count over wave sizes and traversal/shade
- * grid sizes, one knob at a time from the defaults, keeps the fastest on the
+ * grid sizes and the hit sort, one knob at a time from the defaults, keeps the fastest on the
  * tracer and returns it. Wave sizes of 1M to 48M paths are tried, the larger
- * ones while their path state (about 307 bytes per path) fits half of the free
+ * ones while their path state (about 311 bytes per path) fits half of the free
  * device memory; a path arena grown for a candidate larger than the one kept
  * is released before it returns. Results are cached per device and workload shape
  * (triangles, pixels, samples, bounces, shading variant) for the process, so

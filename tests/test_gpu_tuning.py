@@ -52,3 +52,26 @@ def test_wave_size_follows_the_tuning_after_larger_buffers():
         launches_many = t.stats()["kernel_launches"]
     assert np.array_equal(one_wave, many_waves)
     assert launches_many > 8 * launches_one, (launches_one, launches_many)
+
+
+@pytest.mark.parametrize("make", [
+    lambda: workloads.spectral_stress(width=96, height=54, spp=2, dome_size=(128, 64)),
+    lambda: workloads.heavy_geometry(width=96, height=54, spp=2, dome_size=(128, 64)),
+], ids=["stress", "heavy"])
+def test_material_sorted_hits_render_the_same_image(make):
+    """sort_hits shades each bounce's hits in material order (a counting sort
+    of the hit queue); per-path results do not depend on the order."""
+    wl = make()
+    with PathTracer(0) as t:
+        t.set_scene(wl.scene)
+        t.set_tuning(wave_paths=8192)  # several waves per frame
+        plain = t.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
+        plain_stats = t.stats()
+        t.set_tuning(wave_paths=8192, sort_hits=1)
+        assert t.tuning()["sort_hits"] == 1
+        sorted_ = t.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
+        sorted_stats = t.stats()
+    assert np.array_equal(plain, sorted_)
+    for key in ("extension_rays", "shadow_rays", "subsurface_rays"):
+        assert plain_stats[key] == sorted_stats[key], key
+    assert sorted_stats["kernel_launches"] > plain_stats["kernel_launches"]
