@@ -396,8 +396,22 @@ def run_nrc(args):
         total, samples = t.read_xyz()
         return total / max(samples, 1)
 
+    # One launch tuning for every tracer (reference, plain and cache arms):
+    # --tuning, or the autotuner's pick for a plain render call of the arms'
+    # shape (a tracer with a radiance cache attached cannot be autotuned).
+    if args.tuning:
+        knobs = [int(x) for x in args.tuning.split(",")] + [0]
+        tuning = {"wave_paths": knobs[0], "trace_blocks_per_sm": knobs[1], "shade_blocks_per_sm": knobs[2],
+                  "sort_hits": knobs[3]}
+    else:
+        with PathTracer(0) as t:
+            t.set_scene(wl.scene)
+            tuned = t.autotune(wl.camera, w, h, wl.max_bounces, args.chunk_spp)
+        tuning = {k: tuned[k] for k in ("wave_paths", "trace_blocks_per_sm", "shade_blocks_per_sm", "sort_hits")}
+
     with PathTracer(0) as t:
         t.set_scene(wl.scene)
+        t.set_tuning(**tuning)
         t0 = time.perf_counter()
         done = 0
         # Sample indices disjoint from the measured arms' (which start at 0).
@@ -421,6 +435,7 @@ def run_nrc(args):
         curve = []
         with PathTracer(0) as t:
             t.set_scene(wl.scene)
+            t.set_tuning(**tuning)
             if cache is not None:
                 t.set_radiance_cache(cache, prefix_bounces=prefix, training_paths=1 << 14, train_steps=4)
             elapsed, spp, err = 0.0, 0, float("inf")
@@ -458,7 +473,8 @@ def run_nrc(args):
                    "reference_seconds": ref_s, "reference_rel_noise": reference_noise,
                    "target_rel_rmse": args.target_rmse, "chunk_spp": args.chunk_spp,
                    "cache": "16 levels x 2 features, 2^19 entries/level fp16; MLP 64x4 ReLU bf16; "
-                            f"prefix {prefixes[0]} bounces; 2^14 training paths per wave, 4 Adam steps per wave"},
+                            f"prefix {prefixes[0]} bounces; 2^14 training paths per wave, 4 Adam steps per wave",
+                   "tuning": tuning},
         "plain": plain, "cache": cached,
         "cache_by_prefix": {str(k): {"seconds": v["seconds"], "spp": v["spp"], "final_rel_rmse": v["final_rel_rmse"],
                                      "ratio_to_plain": (v["seconds"] / plain["seconds"])

@@ -1563,7 +1563,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         best.default_milliseconds = measure(0, 16, 8);
         best.milliseconds = best.default_milliseconds;
         best.candidates = 1;
-        auto consider = [&](uint64_t wave, uint32_t trace, uint32_t shade, uint32_t sort = 0) {
+        auto consider = [&](uint64_t wave, uint32_t trace, uint32_t shade, uint32_t sort) {
             const double ms = measure(wave, trace, shade, sort);
             ++best.candidates;
             if (ms < best.milliseconds) {
@@ -1574,6 +1574,10 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
                 best.sort_hits = sort;
             }
         };
+        // The hit sort first: whether it pays depends on how differently the
+        // scene's materials shade, which the other knobs hardly change.
+        consider(0, 16, 8, 1u);
+        const uint32_t sort = best.sort_hits;
         // Waves above the automatic size shorten the launches' tails; they are
         // tried while their path state stays within half the device memory
         // that is free or already held by the arena.
@@ -1583,11 +1587,12 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         for (uint64_t wave : {48ull << 20, 32ull << 20, 24ull << 20, 16ull << 20, 8ull << 20, 4ull << 20, 2ull << 20,
                               1ull << 20}) {
             if (wave < needed && wave * kPathStateBytes <= pathBytesLimit)
-                consider(wave, best.trace_blocks_per_sm, best.shade_blocks_per_sm);
+                consider(wave, best.trace_blocks_per_sm, best.shade_blocks_per_sm, sort);
         }
-        for (uint32_t trace : {8u, 32u, 64u}) consider(best.wave_paths, trace, best.shade_blocks_per_sm);
-        for (uint32_t shade : {2u, 4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade);
-        consider(best.wave_paths, best.trace_blocks_per_sm, best.shade_blocks_per_sm, 1u);
+        for (uint32_t trace : {8u, 32u, 64u}) consider(best.wave_paths, trace, best.shade_blocks_per_sm, sort);
+        for (uint32_t shade : {2u, 4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade, sort);
+        // The sort again, the other way, at the chosen launch shape.
+        consider(best.wave_paths, best.trace_blocks_per_sm, best.shade_blocks_per_sm, best.sort_hits ^ 1u);
         // Arena buffers grown for a larger candidate than the one chosen are
         // released; the next render allocates the chosen wave.
         const uint64_t chosen = std::max<uint64_t>(3, std::min(needed, best.wave_paths ? best.wave_paths : kAutomaticWavePaths));
