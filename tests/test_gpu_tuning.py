@@ -36,6 +36,8 @@ def test_tuning_rejects_out_of_range_values():
             t.set_tuning(trace_blocks_per_sm=0)
         with pytest.raises(RuntimeError, match="tuning out of range"):
             t.set_tuning(wave_paths=2)
+        with pytest.raises(RuntimeError, match="tuning out of range"):
+            t.set_tuning(sort_hits=2)
 
 
 def test_wave_size_follows_the_tuning_after_larger_buffers():
