@@ -19,6 +19,7 @@
 #include <string>
 #include <vector>
 
+#include "batch_plan.h"
 #include "bvh_build.h"
 #include "integrator.h"
 #include "nrc.h"
@@ -963,7 +964,8 @@ struct BatchPlan {
 // radiance cache) to lanes, largest first onto the lane with the fewest paths,
 // and sizes each lane's arena: its largest job's paths, at most kBatchLaneWave
 // and at most an equal share of the budget (`pathBudget` paths per device, 0:
-// half the device's free memory), never below 1,048,576 paths. Lanes take the
+// half the device's free memory), never below 1,048,576 paths (planLanes,
+// batch_plan.h, holds these rules). Lanes take the
 // arenas that are free; only a batch that holds none yet waits for one, so
 // concurrent batches cannot wait on each other. Jobs left without a lane (no
 // arena, or its buffers could not be allocated) render on their own path state.
@@ -990,7 +992,6 @@ BatchPlan planBatch(hdcx_batch_job* jobs, uint32_t count, uint64_t pathBudget)
                 eligible.push_back(j);
         }
         if (eligible.empty() || cudaSetDevice(device) != cudaSuccess) continue;
-        std::stable_sort(eligible.begin(), eligible.end(), [&](uint32_t a, uint32_t b) { return need(a) > need(b); });
         std::vector<ArenaLease> leases;
         const size_t wanted = std::min<size_t>(kBatchLanes, eligible.size());
         try {
@@ -1012,16 +1013,13 @@ BatchPlan planBatch(hdcx_batch_job* jobs, uint32_t count, uint64_t pathBudget)
             for (const ArenaLease& l : leases) held += l.arena->store.paths.capacity * kPathStateBytes;
             budget = (freeBytes + held) / 2 / kPathStateBytes;
         }
-        std::vector<std::vector<uint32_t>> members(lanes);
-        std::vector<uint64_t> total(lanes, 0);
-        for (uint32_t j : eligible) {
-            const uint32_t l = static_cast<uint32_t>(std::min_element(total.begin(), total.end()) - total.begin());
-            members[l].push_back(j);
-            total[l] += need(j);
-        }
+        std::vector<uint64_t> paths;
+        for (uint32_t j : eligible) paths.push_back(need(j));
+        const LanePlan lanePlan = planLanes(paths, lanes, budget, kBatchLaneWave, 1ull << 20);
         for (uint32_t l = 0; l < lanes; ++l) {
-            uint64_t capacity = std::min(need(members[l].front()), kBatchLaneWave);
-            capacity = std::max<uint64_t>(3, std::min(capacity, std::max<uint64_t>(budget / lanes, 1ull << 20)));
+            std::vector<uint32_t> members;
+            for (uint32_t k : lanePlan.members[l]) members.push_back(eligible[k]);
+            const uint64_t capacity = lanePlan.capacity[l];
             PathStore& store = leases[l].arena->store;
             bool ready = true;
             try {
@@ -1032,12 +1030,12 @@ BatchPlan planBatch(hdcx_batch_job* jobs, uint32_t count, uint64_t pathBudget)
                 ready = false;
             }
             if (!ready) {
-                for (uint32_t j : members[l]) plan.order.push_back(j);
+                for (uint32_t j : members) plan.order.push_back(j);
                 continue;
             }
             const int index = static_cast<int>(plan.leases.size());
             plan.leases.push_back(std::move(leases[l]));
-            for (uint32_t j : members[l]) {
+            for (uint32_t j : members) {
                 plan.lane[j] = index;
                 plan.order.push_back(j);
             }
