@@ -86,3 +86,34 @@ def test_raster_preview_is_rejected_without_a_device(hdcx_lib):
     tracer._h = None
     with pytest.raises(ValueError):
         hdcx_lib.PathTracer.set_shading_mode(tracer, hdcx_lib.RASTER_PREVIEW)
+
+
+C_STRUCT_NAMES = ["hdcx_camera", "hdcx_mesh_desc", "hdcx_material_desc", "hdcx_texture_desc", "hdcx_light_desc",
+                  "hdcx_scene_desc", "hdcx_packed_texture", "hdcx_packed_scene", "hdcx_render_stats",
+                  "hdcx_batch_job", "hdcx_nrc_config", "hdcx_tuning"]
+
+
+def test_struct_fields_match_the_header(tmp_path):
+    """Every field of every Python mirror has the header's name and offset:
+    gcc compiles offsetof() of each field against include/hdcx.h."""
+    import subprocess
+    assert len(C_STRUCT_NAMES) == len(_abi.STRUCTS_IN_ABI_ORDER)
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "hdcx.h"', "int main(void) {"]
+    expected = []
+    for cname, struct in zip(C_STRUCT_NAMES, _abi.STRUCTS_IN_ABI_ORDER):
+        for field, _ctype in struct._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {field}));')
+            expected.append((cname, field, getattr(struct, field).offset))
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        expected.append((cname, "sizeof", C.sizeof(struct)))
+    lines.append("  return 0;\n}")
+    src = tmp_path / "offsets.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "offsets"
+    build = subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                           capture_output=True, text=True)
+    assert build.returncode == 0, build.stderr
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert len(got) == len(expected)
+    mismatched = [(c, f, e, g) for (c, f, e), g in zip(expected, got) if e != g]
+    assert not mismatched, mismatched
