@@ -174,3 +174,80 @@ def variant(name: str) -> Scene:
     else:
         raise KeyError(name)
     return s
+
+
+def fuzz_material(rng, material_id: str) -> Material:
+    """A seeded random material over the closure ABI: every diffuse model,
+    anisotropic GGX, coat, sheen (both modes), translucency, subsurface,
+    transmission (dispersive, scattering, thin-walled) and emission; opacity 1
+    (cut-outs agree with the reference only in expectation)."""
+    m = Material(id=material_id)
+    m.base_color = rng.uniform(0.02, 0.95, 3).tolist()
+    m.diffuse_model = int(rng.integers(0, 4))
+    m.diffuse_roughness = float(rng.uniform(0, 1))
+    m.diffuse_weight = float(rng.choice([1.0, rng.uniform(0, 1)]))
+    m.metalness = float(rng.choice([0.0, rng.uniform(0, 1), 1.0]))
+    m.roughness = float(rng.uniform(0.02, 1))
+    m.roughness_v = float(rng.choice([m.roughness, rng.uniform(0.02, 1)]))
+    m.specular_weight = float(rng.choice([0.0, 1.0, rng.uniform(0, 1)]))
+    m.specular_color = rng.uniform(0.3, 1, 3).tolist()
+    m.index_of_refraction = float(rng.uniform(1.1, 2.2))
+    if rng.random() < 0.4:
+        m.coat = float(rng.uniform(0, 1))
+        m.coat_roughness = float(rng.uniform(0.01, 0.6))
+        m.coat_roughness_v = float(rng.choice([m.coat_roughness, rng.uniform(0.01, 0.6)]))
+        m.coat_color = rng.uniform(0.5, 1, 3).tolist()
+        m.coat_index_of_refraction = float(rng.uniform(1.2, 2.0))
+    if rng.random() < 0.4:
+        m.sheen = float(rng.uniform(0, 1))
+        m.sheen_roughness = float(rng.uniform(0.05, 1))
+        m.sheen_mode = int(rng.integers(0, 2))
+        m.sheen_color = rng.uniform(0.2, 1, 3).tolist()
+    if rng.random() < 0.3:
+        m.translucent_weight = float(rng.uniform(0, 1))
+        m.translucent_color = rng.uniform(0.1, 1, 3).tolist()
+    if rng.random() < 0.3:
+        m.subsurface = float(rng.uniform(0, 1))
+        m.subsurface_color = rng.uniform(0.1, 0.99, 3).tolist()
+        m.subsurface_radius = rng.uniform(0.01, 0.5, 3).tolist()
+        m.subsurface_scale = float(rng.uniform(0.05, 1))
+        m.subsurface_scatter_anisotropy = float(rng.uniform(-0.8, 0.8))
+    if rng.random() < 0.3:
+        m.transmission = float(rng.uniform(0.3, 1))
+        m.transmission_color = rng.uniform(0.3, 1, 3).tolist()
+        m.transmission_depth = float(rng.choice([0.0, rng.uniform(0.05, 1)]))
+        m.transmission_scatter = (rng.uniform(0, 2, 3) if rng.random() < 0.5 else [0.0, 0.0, 0.0])
+        m.transmission_scatter = [float(x) for x in m.transmission_scatter]
+        m.transmission_scatter_anisotropy = float(rng.uniform(-0.8, 0.8))
+        if rng.random() < 0.5:
+            m.transmission_dispersion_scale = float(rng.uniform(0.2, 1))
+            m.transmission_dispersion_abbe_number = float(rng.uniform(9, 60))
+        m.thin_walled = bool(rng.random() < 0.3)
+    if rng.random() < 0.15:
+        m.emission = rng.uniform(0.5, 5, 3).tolist()
+        m.emission_weight = float(rng.uniform(0.2, 1))
+    return m
+
+
+def fuzz_box(seed: int, size: int = 40):
+    """The closed box (5 walls, 2 boxes, a rect light) with seeded random
+    materials on walls and boxes, and at random a dome and a sphere light."""
+    import numpy as np
+
+    from hdcodex_b200 import workloads
+    rng = np.random.default_rng(seed)
+    wl = workloads.closed_box(width=size, height=size, spp=4)
+    s = wl.scene
+    s.materials = [fuzz_material(rng, i) for i in ("/white", "/red", "/green", "/tallBox", "/shortBox")]
+    for mesh in s.meshes:
+        if mesh.id == "/tall":
+            mesh.material_id = "/tallBox"
+        elif mesh.id == "/short":
+            mesh.material_id = "/shortBox"
+    if rng.random() < 0.5:
+        s.lights.append(Light(id="/dome", type=DOME, color=rng.uniform(0.1, 1, 3).tolist(),
+                              intensity=float(rng.uniform(0.1, 1))))
+    if rng.random() < 0.4:
+        s.lights.append(Light(id="/sphere", type=SPHERE, intensity=float(rng.uniform(1, 10)),
+                              position=[0.5, 0.7, 0.6], radius=0.05, area=0.0314159))
+    return wl

@@ -134,3 +134,18 @@ def test_spectral_stress_agrees_with_reference_shader_in_expectation(ref_oracle)
     ma, mb = a[..., :3].mean(axis=(0, 1)), b[..., :3].mean(axis=(0, 1))
     assert np.allclose(ma, mb, rtol=0.02), (ma, mb)
     assert np.isfinite(a).all() and np.isfinite(b).all()
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_materials_match_reference_shader(ref_oracle, seed):
+    """Seeded random materials and lights in the closed box (ref_scenes.fuzz_box):
+    the oracle equals the reference shader bit for bit."""
+    wl = R.fuzz_box(seed)
+    o = ref_oracle.OracleTracer()
+    o.set_scene(wl.scene)
+    r = ref_oracle.ReferenceTracer()
+    r.set_scene(wl.scene)
+    a = o.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
+    b = r.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
+    assert float(a[..., :3].mean()) > 0.0
+    assert np.array_equal(a, b), f"seed {seed}: identical={np.all(a == b, axis=-1).mean():.4f}"
