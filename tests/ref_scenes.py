@@ -251,3 +251,69 @@ def fuzz_box(seed: int, size: int = 40):
         s.lights.append(Light(id="/sphere", type=SPHERE, intensity=float(rng.uniform(1, 10)),
                               position=[0.5, 0.7, 0.6], radius=0.05, area=0.0314159))
     return wl
+
+
+def _fuzz_frame(rng):
+    import numpy as np
+    z = rng.normal(size=3)
+    z /= np.linalg.norm(z)
+    a = np.array([1.0, 0.0, 0.0]) if abs(z[0]) < 0.9 else np.array([0.0, 1.0, 0.0])
+    x = np.cross(a, z)
+    x /= np.linalg.norm(x)
+    return x, np.cross(z, x), z
+
+
+def fuzz_light(rng, light_id: str, textures) -> Light:
+    """A seeded random light of any type: placement and frame, colour,
+    temperature tint, exposure, diffuse/specular factors, normalisation,
+    visibility, shaping cone and focus, shadow controls, and (rect and dome)
+    a texture from `textures`."""
+    kind = int(rng.choice([RECT, DISK, SPHERE, CYLINDER, DISTANT, DOME]))
+    x, y, z = _fuzz_frame(rng)
+    l = Light(id=light_id, type=kind)
+    l.color = rng.uniform(0.2, 1, 3).tolist()
+    l.temperature_color = rng.uniform(0.6, 1, 3).tolist()
+    l.intensity = float(rng.uniform(0.5, 8))
+    l.exposure = float(rng.uniform(-1, 1))
+    l.diffuse = float(rng.choice([1.0, rng.uniform(0, 1)]))
+    l.specular = float(rng.choice([1.0, rng.uniform(0, 1)]))
+    l.normalize = bool(rng.random() < 0.5)
+    l.visible = bool(rng.random() < 0.7)
+    l.basis_x, l.basis_y, l.basis_z = x.tolist(), y.tolist(), z.tolist()
+    l.position = rng.uniform(0.15, 0.85, 3).tolist()
+    l.width, l.height = float(rng.uniform(0.05, 0.4)), float(rng.uniform(0.05, 0.4))
+    l.axis_u = (x * l.width / 2).tolist()
+    l.axis_v = (y * l.height / 2).tolist()
+    l.radius = float(rng.uniform(0.02, 0.15))
+    l.length = float(rng.uniform(0.05, 0.4))
+    l.angle = float(rng.uniform(0.2, 8.0))
+    l.area = float(rng.uniform(0.01, 0.2))
+    if rng.random() < 0.5:
+        l.shaping_focus = float(rng.uniform(0, 2))
+        l.shaping_focus_tint = rng.uniform(0, 1, 3).tolist()
+        l.shaping_cone_angle = float(rng.uniform(20, 180))
+        l.shaping_cone_softness = float(rng.uniform(0, 1))
+    l.shadow_enable = bool(rng.random() < 0.85)
+    if rng.random() < 0.4:
+        l.shadow_color = rng.uniform(0, 0.5, 3).tolist()
+        l.shadow_distance = float(rng.choice([-1.0, rng.uniform(0.1, 1.5)]))
+        l.shadow_falloff = float(rng.choice([-1.0, rng.uniform(0.1, 1.5)]))
+        l.shadow_falloff_gamma = float(rng.uniform(0.5, 2))
+    if kind in (RECT, DOME) and rng.random() < 0.5:
+        l.texture = str(rng.choice(textures))
+    return l
+
+
+def fuzz_lights_box(seed: int, size: int = 40):
+    """The closed box (its own or random materials) lit by one to six seeded
+    random lights instead of its rect light."""
+    import numpy as np
+
+    from hdcodex_b200 import workloads
+    rng = np.random.default_rng(10_000 + seed)
+    wl = fuzz_box(seed, size) if rng.random() < 0.5 else workloads.closed_box(width=size, height=size, spp=4)
+    s = wl.scene
+    hdr = ("rect#hdr", "spectral-gradient#hdr")
+    s.textures += [t for t in base_scene().textures if t.id in hdr]
+    s.lights = [fuzz_light(rng, f"/light{i}", hdr) for i in range(int(rng.integers(1, 7)))]
+    return wl

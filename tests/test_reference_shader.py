@@ -149,3 +149,18 @@ def test_random_materials_match_reference_shader(ref_oracle, seed):
     b = r.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
     assert float(a[..., :3].mean()) > 0.0
     assert np.array_equal(a, b), f"seed {seed}: identical={np.all(a == b, axis=-1).mean():.4f}"
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_lights_match_reference_shader(ref_oracle, seed):
+    """One to six seeded random lights of every type (ref_scenes.fuzz_lights_box):
+    the oracle equals the reference shader bit for bit."""
+    wl = R.fuzz_lights_box(seed)
+    o = ref_oracle.OracleTracer()
+    o.set_scene(wl.scene)
+    r = ref_oracle.ReferenceTracer()
+    r.set_scene(wl.scene)
+    a = o.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
+    b = r.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
+    assert np.isfinite(a).all()
+    assert np.array_equal(a, b), f"seed {seed}: identical={np.all(a == b, axis=-1).mean():.4f}"
