@@ -317,3 +317,69 @@ def fuzz_lights_box(seed: int, size: int = 40):
     s.textures += [t for t in base_scene().textures if t.id in hdr]
     s.lights = [fuzz_light(rng, f"/light{i}", hdr) for i in range(int(rng.integers(1, 7)))]
     return wl
+
+
+def _fuzz_texture(rng, texture_id: str) -> Texture:
+    import numpy as np
+    w, h = int(rng.integers(1, 9)), int(rng.integers(1, 9))
+    kind = int(rng.integers(0, 3))  # sRGB8, linear RGBA8, RGBA32F
+    if kind == 2:
+        return Texture(id=texture_id, source_path="synthetic", width=w, height=h,
+                       rgba_float=rng.uniform(0, 1.5, w * h * 4).astype(np.float32).tolist())
+    return Texture(id=texture_id, source_path="synthetic", width=w, height=h, srgb=kind == 0,
+                   rgba=rng.integers(0, 256, w * h * 4).tolist())
+
+
+def _fuzz_normal_map(rng, texture_id: str) -> Texture:
+    import numpy as np
+    w, h = int(rng.integers(1, 6)), int(rng.integers(1, 6))
+    n = rng.normal(size=(w * h, 3)) * 0.3 + np.array([0.0, 0.0, 1.0])
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    rgb = np.clip((n * 0.5 + 0.5) * 255, 0, 255).astype(int)
+    return Texture(id=texture_id, source_path="synthetic", width=w, height=h,
+                   rgba=np.concatenate([rgb, np.full((w * h, 1), 255)], axis=1).ravel().tolist())
+
+
+def fuzz_textured(seed: int) -> Scene:
+    """The reference's textured triangle with random UVs above a UV-tiled
+    ground quad, both with random materials whose texture slots (all but
+    opacity) bind seeded random textures (sRGB8, linear RGBA8, RGBA32F, at
+    random a UDIM set of three tiles), a random normal map, and random
+    base-colour scale, bias and channel."""
+    import numpy as np
+
+    from hdcodex_b200 import _abi
+    rng = np.random.default_rng(20_000 + seed)
+    s = base_scene()
+    s.meshes.append(Mesh(id="/ground", positions=[-4, -1.0, -1, 4, -1.0, -1, 4, -1.0, -6, -4, -1.0, -6],
+                         indices=[0, 1, 2, 0, 2, 3],
+                         texcoords=[0.0, 0.0, 3.0, 0.0, 3.0, 2.5, 0.0, 0.0, 3.0, 2.5, 0.0, 2.5],
+                         material_id="/groundMat"))
+    s.meshes[0].texcoords = rng.uniform(-0.5, 2.5, 6).tolist()
+    textures = [_fuzz_texture(rng, f"fuzz{i}") for i in range(4)] + [_fuzz_normal_map(rng, "fuzzNormal")]
+    bindable = [t.id for t in textures if t.id != "fuzzNormal"]
+    if rng.random() < 0.4:
+        for tile in (1001, 1002, 1011):
+            t = _fuzz_texture(rng, f"fuzzUdim#udim={tile}")
+            t.udim_set_id, t.udim_tile, t.source_path = "fuzzUdim", tile, f"fuzzUdim.{tile}"
+            textures.append(t)
+        bindable.append("fuzzUdim")
+    s.textures += textures
+    slots = [n for n, _t, _d in _abi.MATERIAL_FIELDS if n.endswith("_texture") and n != "opacity_texture"]
+    s.materials = []
+    for material_id in ("/red", "/groundMat"):
+        m = fuzz_material(rng, material_id)
+        for slot in slots:
+            if slot == "normal_texture":
+                if rng.random() < 0.4:
+                    m.normal_texture = "fuzzNormal"
+                    m.normal_texture_scale = float(rng.uniform(0.2, 1.5))
+                    m.normal_texture_flip_y = bool(rng.random() < 0.5)
+            elif rng.random() < 0.3:
+                setattr(m, slot, str(rng.choice(bindable)))
+        if rng.random() < 0.5:
+            m.base_color_texture_scale = rng.uniform(0.5, 1.5, 3).tolist()
+            m.base_color_texture_bias = rng.uniform(-0.1, 0.2, 3).tolist()
+            m.base_color_texture_channel = int(rng.integers(-1, 4))
+        s.materials.append(m)
+    return s
