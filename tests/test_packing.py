@@ -102,3 +102,12 @@ def test_dome_importance_map(oracle_lib, hdcx_lib):
     v1 = (np.arange(h) + 1) / h
     solid = (2 * np.pi / w) * np.abs(np.cos(np.pi * (1 - v1)) - np.cos(np.pi * (1 - v0)))
     assert (m[:, :, 2] * solid[:, None]).sum() == pytest.approx(1.0, rel=1e-5)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_scene_packing_matches_oracle(oracle_lib, hdcx_lib, seed):
+    """The random material, light and texture scenes of the shader fuzz tests
+    (ref_scenes.fuzz_box, fuzz_lights_box, fuzz_textured) pack byte for byte
+    as the oracle's restatement of BuildScene packs them."""
+    for scene in (R.fuzz_box(seed).scene, R.fuzz_lights_box(seed).scene, R.fuzz_textured(seed)):
+        assert_same_packing(pack_scene(scene), oracle_packing(oracle_lib, scene))
