@@ -4,7 +4,7 @@
   and, where the reference checkout exists, against the reference's own
   include/hdcodex/core/versioned_scene.h (HDCX_USE_EXTERNAL_SCENE_ABI), which
   is what a Hydra delegate does.
-* On the GPU box, tests/cpp/path_tracer_tests.cpp (the reference's GPU test
+* On a B200, tests/cpp/path_tracer_tests.cpp (the reference's GPU test
   flow through CudaPathTracer) runs and passes.
 """
 import os
@@ -34,7 +34,8 @@ def test_shim_compiles_and_links(hdcx_lib):
 
 
 def test_shim_compiles_against_reference_scene_abi(hdcx_lib, tmp_path):
-    ref_include = "/root/reference/include"
+    import ref_build
+    ref_include = os.path.join(ref_build.REFERENCE, "include")
     if not os.path.isdir(ref_include):
         pytest.skip("the reference checkout is not present")
     src = tmp_path / "with_reference_abi.cpp"
