@@ -118,6 +118,23 @@ def test_spectral_stress_without_cutouts_matches_reference_shader(ref_oracle):
     assert np.array_equal(a, b), f"identical={np.all(a == b, axis=-1).mean():.4f}"
 
 
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
+def test_spectral_stress_generator_seeds_match_reference_shader(ref_oracle, seed):
+    # Other seeds of the stress-scene generator (glass Abbe numbers, leaf
+    # placement, dome), cutouts removed: bit for bit.
+    wl = workloads.spectral_stress(width=48, height=27, seed=seed)
+    for m in wl.scene.materials:
+        if m.id == "/leaf":
+            m.opacity_texture = ""
+    o = ref_oracle.OracleTracer()
+    o.set_scene(wl.scene)
+    r = ref_oracle.ReferenceTracer()
+    r.set_scene(wl.scene)
+    a = o.render(wl.camera, 48, 27, 0, 8, 8)
+    b = r.render(wl.camera, 48, 27, 0, 8, 8)
+    assert np.array_equal(a, b), f"seed {seed}: identical={np.all(a == b, axis=-1).mean():.4f}"
+
+
 def test_spectral_stress_agrees_with_reference_shader_in_expectation(ref_oracle):
     # With the opacity-cutout leaves the reference draws one random number per
     # candidate; the oracle's any-hit threshold draws none. The images then
