@@ -220,7 +220,8 @@ class PathTracer:
                                                   training_paths, train_steps), "set_radiance_cache")
 
     def autotune(self, camera, width, height, max_bounces=8, sample_count=1) -> dict:
-        """hdcx_autotune: picks wave size and grid sizes for this workload shape."""
+        """hdcx_autotune: picks the hit sort, wave size and grid sizes for this
+        workload shape (cached per device and shape); returns the tuning."""
         r = _abi.Tuning()
         self._check(lib().hdcx_autotune(self._h, C.byref(camera), width, height, max_bounces, sample_count,
                                         C.byref(r)), "autotune")
@@ -232,6 +233,9 @@ class PathTracer:
         return {name: getattr(r, name) for name, _ in _abi.Tuning._fields_}
 
     def set_tuning(self, wave_paths=0, trace_blocks_per_sm=16, shade_blocks_per_sm=8, sort_hits=0):
+        """hdcx_set_tuning: paths per wave (0: automatic), blocks of 128 threads
+        per SM for traversal and shading (1-64), sort_hits 1 to shade each
+        bounce's hits in material order. Images do not depend on these."""
         r = _abi.Tuning(wave_paths=wave_paths, trace_blocks_per_sm=trace_blocks_per_sm,
                         shade_blocks_per_sm=shade_blocks_per_sm, sort_hits=sort_hits)
         self._check(lib().hdcx_set_tuning(self._h, C.byref(r)), "set_tuning")
