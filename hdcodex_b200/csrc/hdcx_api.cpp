@@ -1070,7 +1070,9 @@ struct BatchEvents {
 // launches it once, then queues the read-backs. Returns the graph's device
 // time, or a negative value (nothing launched) when the batch cannot be
 // captured: jobs on several devices, a job in radiance-cache mode (it
-// synchronises with the host per wave) or a capture error.
+// synchronises with the host per wave) or a capture error. A launch,
+// synchronisation or read-back error after instantiation sets the affected
+// jobs' status to HDCX_ERROR_CUDA and takes them out of the batch.
 float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<RenderCall>& calls, const BatchPlan& plan)
 {
     int device = -1;
@@ -1139,16 +1141,30 @@ float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<Render
         cleanup();
         return -1.0F;
     }
-    if (cudaEventRecord(start, batch) == cudaSuccess && cudaGraphLaunch(exec, batch) == cudaSuccess &&
-        cudaEventRecord(stop, batch) == cudaSuccess && cudaStreamSynchronize(batch) == cudaSuccess) {
-        cudaEventElapsedTime(&ms, start, stop);
-        for (uint32_t j = 0; j < count; ++j) {
-            if (!calls[j].active || !jobs[j].rgba_out) continue;
-            hdcx_tracer* t = jobs[j].tracer;
-            cudaMemcpyAsync(jobs[j].rgba_out, t->fb.rgba, size_t(calls[j].frame.width) * calls[j].frame.height * sizeof(float4),
-                            cudaMemcpyDeviceToHost, t->stream);
+    // Once the graph is instantiated the jobs' work is committed to it: a
+    // failure from here on fails every job of the graph (its images are not
+    // valid), and is not retried on the streams.
+    cudaError_t err = cudaEventRecord(start, batch);
+    if (err == cudaSuccess) err = cudaGraphLaunch(exec, batch);
+    if (err == cudaSuccess) err = cudaEventRecord(stop, batch);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(batch);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, start, stop);
+    for (uint32_t j = 0; j < count; ++j) {
+        if (!calls[j].active) continue;
+        hdcx_tracer* t = jobs[j].tracer;
+        cudaError_t jobErr = err;
+        if (jobErr == cudaSuccess && jobs[j].rgba_out) {
+            jobErr = cudaMemcpyAsync(jobs[j].rgba_out, t->fb.rgba,
+                                     size_t(calls[j].frame.width) * calls[j].frame.height * sizeof(float4),
+                                     cudaMemcpyDeviceToHost, t->stream);
+        }
+        if (jobErr != cudaSuccess) {
+            jobs[j].status = fail(t, HDCX_ERROR_CUDA, std::string("hdcx_render_batch (CUDA graph): ") +
+                                                           cudaGetErrorString(jobErr));
+            calls[j].active = false;
         }
     }
+    if (err != cudaSuccess) cudaGetLastError();
     cleanup();
     return ms < 0.0F ? 0.0F : ms;
 }
@@ -1251,6 +1267,11 @@ HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* t, const hdcx_camera* camer
     }
     if (reinterpret_cast<uintptr_t>(rgbaDevice) % 16u != 0u)
         return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_render_static: rgba_device must be 16-byte aligned");
+    if (t->radianceCache) {
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT,
+                    "hdcx_render_static: the tracer has a radiance cache attached; the static render has no cache "
+                    "mode (detach it with hdcx_set_radiance_cache(tracer, NULL, ...) or use hdcx_render)");
+    }
     return guarded(t, [&] {
         if (!t->fallbackAxisInitialized) {
             t->fallbackZUp = std::fabs(camera->vertical[2]) > std::fabs(camera->vertical[1]);

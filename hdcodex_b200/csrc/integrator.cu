@@ -1019,7 +1019,9 @@ __global__ void finalizeKernel(FrameConst f, FrameBuffers fb)
 {
     const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
     if (pixel >= f.width * f.height) return;
-    const float4 prev = fb.rgba[pixel];
+    // A restart (sampleIndex 0) gives the previous mean weight 0; it is not
+    // read, so whatever the output buffer held (NaN included) cannot leak in.
+    const float4 prev = f.sampleIndex == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : fb.rgba[pixel];
     const float4 b = fb.batch[pixel];
     const float previousWeight = u2f(f.sampleIndex);
     const float totalWeight = previousWeight + u2f(f.sampleCount);

@@ -51,6 +51,11 @@ namespace {
     } while (0)
 
 constexpr uint32_t kErrorTimeout = 1u;
+// The drain wait after a timeout also ran out: an MMA may still have been in
+// flight when the kernel freed its tensor memory. Freeing is still the lesser
+// hazard: a CTA that exits holding tensor memory leaves the next CTA's
+// tcgen05.alloc on that SM waiting for columns that never come back.
+constexpr uint32_t kErrorDrain = 2u;
 constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before a wait gives up
 
 struct DeviceParams {
@@ -289,8 +294,9 @@ __global__ void __launch_bounds__(128) queryKernel(DeviceParams p, const float* 
         }
     }
     if (failed) {
-        if (threadIdx.x == 0) atomicOr(error, kErrorTimeout);
-        barrierWait(bar, phase);  // bounded: lets an MMA still in flight finish before the memory is freed
+        // Bounded: lets an MMA still in flight finish before the memory is freed.
+        const bool drained = barrierWait(bar, phase);
+        if (threadIdx.x == 0) atomicOr(error, drained ? kErrorTimeout : (kErrorTimeout | kErrorDrain));
     }
     __syncthreads();
     fenceAfterSync();
@@ -443,8 +449,9 @@ __global__ void __launch_bounds__(128) trainKernel(DeviceParams p, const float* 
         accumulated = true;
     }
     if (failed) {
-        if (threadIdx.x == 0) atomicOr(error, kErrorTimeout);
-        barrierWait(bar, phase);  // bounded: lets an MMA still in flight finish before the memory is freed
+        // Bounded: lets an MMA still in flight finish before the memory is freed.
+        const bool drained = barrierWait(bar, phase);
+        if (threadIdx.x == 0) atomicOr(error, drained ? kErrorTimeout : (kErrorTimeout | kErrorDrain));
     }
     fenceBeforeSync();
     __syncthreads();
@@ -566,7 +573,10 @@ void checkError(Cache* c, cudaStream_t stream)
     NRC_OK(cudaStreamSynchronize(stream));
     if (e != 0u) {
         NRC_OK(cudaMemsetAsync(c->error, 0, sizeof(uint32_t), stream));
-        throw std::runtime_error("nrc: a tensor-core wait timed out");
+        throw std::runtime_error((e & kErrorDrain) != 0u
+                                     ? "nrc: a tensor-core wait timed out, and so did the wait for the MMA in flight "
+                                       "before tensor memory was freed"
+                                     : "nrc: a tensor-core wait timed out");
     }
 }
 

@@ -450,7 +450,9 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* tracer, const hdcx_camera* camera,
  * sums of one frame) is one static device array of 62,063,104 bytes inside
  * the library, which every GPU that loads the library keeps until the process
  * exits. Images above 1,048,576 pixels (width*height) are rejected with
- * HDCX_ERROR_INVALID_ARGUMENT and a message. The first call on a device looks
+ * HDCX_ERROR_INVALID_ARGUMENT and a message, and so is a tracer with a
+ * radiance cache attached (this entry point has no cache mode, whose training
+ * buffers it would have to allocate). The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) with that device
  * current; make that first call before any stream capture. All calls on a
  * device share the array, which keeps the last call's contents, so calls whose

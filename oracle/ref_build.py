@@ -30,7 +30,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REFERENCE = os.environ.get("HDCX_REFERENCE_ROOT", "/root/reference")
+# The hdCodex checkout: $HDCX_REFERENCE_ROOT, else a checkout named
+# "reference" beside this repository's root directory.
+REFERENCE = os.environ.get("HDCX_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 SOURCE = os.path.join(REFERENCE, "src", "gpu", "vulkan_path_tracer.cpp")
 LIB = os.path.join(OUT, "libhdcx_ref.so")
 

@@ -67,6 +67,66 @@ def test_static_render_matches_render_two_calls(hdcx_lib, case):
             assert frac >= MIN_IDENTICAL and rel <= MAX_REL_L1, (case, sample_index, frac, rel)
 
 
+def test_static_render_allocates_no_device_memory(hdcx_lib):
+    """The property the entry point exists for: after the first call on the
+    device (which looks up the static array's address and loads the kernels),
+    further calls leave the device's free memory unchanged, including a call
+    at a new, larger image size, where hdcx_render would grow its buffers."""
+    import torch
+    camera = R.base_camera()
+    small = torch.zeros((48, 48, 4), dtype=torch.float32, device="cuda:0")
+    large = torch.zeros((300, 400, 4), dtype=torch.float32, device="cuda:0")
+    with PathTracer(0) as tracer:
+        tracer.set_scene(R.base_scene())
+        status, _ = render_static(tracer, camera, 48, 48, 0, 8, 1, small.data_ptr())
+        assert status == 0, tracer_error(tracer)
+        torch.cuda.synchronize()
+        free_before, _ = torch.cuda.mem_get_info(0)
+        for w, h, image in ((48, 48, small), (400, 300, large), (48, 48, small)):
+            for sample_index, spp in ((0, 2), (2, 1)):
+                status, written = render_static(tracer, camera, w, h, sample_index, 8, spp, image.data_ptr())
+                assert status == 0 and written == 1, tracer_error(tracer)
+        torch.cuda.synchronize()
+        free_after, _ = torch.cuda.mem_get_info(0)
+        assert free_after == free_before, (free_before, free_after)
+        assert torch.isfinite(large).all().item()
+
+
+def test_static_render_restart_ignores_buffer_contents(hdcx_lib):
+    """sample_index 0 does not read the caller's buffer: NaN left in it (a
+    recycled or uninitialised allocation) does not reach the image."""
+    import torch
+    camera = R.base_camera()
+    with PathTracer(0) as tracer:
+        tracer.set_scene(R.base_scene())
+        ref = tracer.render(camera, 32, 32, 0, 8, 2).copy()
+        torch.cuda.synchronize()
+        image = torch.full((32, 32, 4), float("nan"), dtype=torch.float32, device="cuda:0")
+        status, written = render_static(tracer, camera, 32, 32, 0, 8, 2, image.data_ptr())
+        assert status == 0 and written == 1, tracer_error(tracer)
+        img = image.cpu().numpy()
+        assert np.isfinite(img).all()
+        frac, rel = compare(img, ref)
+        assert frac >= MIN_IDENTICAL and rel <= MAX_REL_L1, (frac, rel)
+
+
+def test_static_render_rejects_a_tracer_with_a_radiance_cache(hdcx_lib):
+    """The static render has no cache mode; a tracer with a cache attached is
+    refused with a message instead of silently rendering plain paths."""
+    import torch
+    from hdcodex_b200 import RadianceCache
+    image = torch.zeros((16, 16, 4), dtype=torch.float32, device="cuda:0")
+    with PathTracer(0) as tracer, RadianceCache(0, log2_table_size=12) as cache:
+        tracer.set_scene(R.base_scene())
+        tracer.set_radiance_cache(cache)
+        status, written = render_static(tracer, R.base_camera(), 16, 16, 0, 8, 1, image.data_ptr())
+        assert status == INVALID_ARGUMENT and written == 0
+        assert "radiance cache" in tracer_error(tracer)
+        tracer.set_radiance_cache(None)
+        status, written = render_static(tracer, R.base_camera(), 16, 16, 0, 8, 1, image.data_ptr())
+        assert status == 0 and written == 1, tracer_error(tracer)
+
+
 def test_static_render_rejects_images_above_its_maximum(hdcx_lib):
     import torch
     device_image = torch.zeros((4,), dtype=torch.float32, device="cuda:0")
