@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default="",
-                    help="wave_paths,trace_blocks_per_sm,shade_blocks_per_sm[,sort_hits] to use instead of "
+                    help="wave_paths,trace_blocks_per_sm,shade_blocks_per_sm[,sort_hits[,sort_rays]] to use instead of "
                          "autotuning (to repeat a tuned run, e.g. under a profiler)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip hdcx_autotune (by default it picks wave and grid sizes before the warm-up; setup, "
@@ -400,14 +400,15 @@ def run_nrc(args):
     # --tuning, or the autotuner's pick for a plain render call of the arms'
     # shape (a tracer with a radiance cache attached cannot be autotuned).
     if args.tuning:
-        knobs = [int(x) for x in args.tuning.split(",")] + [0]
+        knobs = [int(x) for x in args.tuning.split(",")] + [0, 0]
         tuning = {"wave_paths": knobs[0], "trace_blocks_per_sm": knobs[1], "shade_blocks_per_sm": knobs[2],
-                  "sort_hits": knobs[3]}
+                  "sort_hits": knobs[3], "sort_rays": knobs[4]}
     else:
         with PathTracer(0) as t:
             t.set_scene(wl.scene)
             tuned = t.autotune(wl.camera, w, h, wl.max_bounces, args.chunk_spp)
-        tuning = {k: tuned[k] for k in ("wave_paths", "trace_blocks_per_sm", "shade_blocks_per_sm", "sort_hits")}
+        tuning = {k: tuned[k] for k in ("wave_paths", "trace_blocks_per_sm", "shade_blocks_per_sm", "sort_hits",
+                                        "sort_rays")}
 
     with PathTracer(0) as t:
         t.set_scene(wl.scene)
@@ -553,9 +554,9 @@ def run_hdcx(args):
     tracer.set_scene(wl.scene)
     tuning = None
     if args.tuning:
-        knobs = [int(x) for x in args.tuning.split(",")] + [0]
+        knobs = [int(x) for x in args.tuning.split(",")] + [0, 0]
         tracer.set_tuning(wave_paths=knobs[0], trace_blocks_per_sm=knobs[1], shade_blocks_per_sm=knobs[2],
-                          sort_hits=knobs[3])
+                          sort_hits=knobs[3], sort_rays=knobs[4])
     elif args.autotune and not args.profile:
         tuning = tracer.autotune(wl.camera, wl.width, wl.height, wl.max_bounces, wl.spp)
     if args.profile:

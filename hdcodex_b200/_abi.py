@@ -268,6 +268,7 @@ class Tuning(C.Structure):
         ("default_milliseconds", C.c_double),
         ("candidates", C.c_uint32),
         ("sort_hits", C.c_uint32),
+        ("sort_rays", C.c_uint32),
     ]
 
 

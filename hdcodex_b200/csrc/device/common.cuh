@@ -112,6 +112,10 @@ struct __align__(16) WideNode {
 };
 static_assert(sizeof(WideNode) == 80, "wide node is 80 bytes");
 
+// DeviceScene::status bits.
+constexpr unsigned int kTraversalOverflow = 1u;  // a pending node group found the stack full and was dropped
+constexpr unsigned int kTraversalBudget = 2u;    // a traversal visited more nodes than the BVH holds
+
 // Scene as the kernels see it (device pointers).
 struct DeviceScene {
     const float4* vertices;
@@ -132,6 +136,10 @@ struct DeviceScene {
     uint32_t hasMeshLights;
     uint32_t nodeCount;
     uint32_t fullShading;    // 0: no material uses textures or layered lobes (see shadeKernel)
+    // Traversal faults of the current render (kTraversalOverflow,
+    // kTraversalBudget; null: not recorded). Set per render to a word the
+    // host reads back with the render's counters.
+    unsigned int* status;
 };
 
 // Per-render constants: the reference's CameraBlock (vulkan_path_tracer.cpp:91-98)

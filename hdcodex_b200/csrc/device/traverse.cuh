@@ -17,7 +17,20 @@
 //   octant first, leaf triangles of the node are tested before descending,
 //   and pending node groups go on a per-thread stack. Child boxes are padded
 //   by one quantisation step on every side at build time, which keeps the
-//   binary32 slab test conservative.
+//   binary32 slab test conservative. The 48 plane distances of a node are
+//   evaluated two children at a time with the packed binary32 instructions
+//   of sm_100 (__fadd2_rn, __ffma2_rn): each half is the same IEEE operation
+//   as the scalar form, so the node test's results are unchanged, in fewer
+//   instructions.
+// * Triangle postponing (Ylitie et al., section 4.2): while fewer than
+//   kPostponeLanes lanes of the warp would test triangles, a lane that also
+//   has a node to visit pushes its triangle group on the stack and visits
+//   the node; the group is tested when it is popped. Closest-hit results do
+//   not depend on the order of the tests.
+// * Faults: a node group that finds the stack full, or a traversal that
+//   visits more nodes than the BVH holds (a malformed node array), sets a
+//   bit in DeviceScene::status, which the host reports as an error of the
+//   render.
 #pragma once
 
 #include "common.cuh"
@@ -26,6 +39,20 @@
 namespace hdcx {
 
 constexpr int kTraversalStack = 64;
+// Triangle groups are postponed while fewer than this many lanes of the warp
+// would test triangles in a step ...
+#ifndef HDCX_POSTPONE_LANES
+#define HDCX_POSTPONE_LANES 6
+#endif
+constexpr uint32_t kPostponeLanes = HDCX_POSTPONE_LANES;
+// ... and while the stack holds fewer than this many entries (node groups
+// need at most one entry per BVH level, which the build caps at 64).
+constexpr int kPostponeDepth = 32;
+
+HDCX_D void traversalFault(const DeviceScene& s, unsigned int code)
+{
+    if (s.status != nullptr) atomicOr(s.status, code);
+}
 
 enum class Accept : int {
     Opaque = 0,      // every candidate is confirmed
@@ -110,14 +137,23 @@ HDCX_D bool intersectTriangle(const RayPre& r, float3 v0, float3 v1, float3 v2, 
     return true;
 }
 
-// Byte `index` of `word` as a float: the byte is placed in the low mantissa
-// bits of 2^23 (bit pattern 0x4B0000bb) and 2^23 is subtracted, which is exact.
-// A byte permute and an add run on full-rate pipes, where an integer-to-float
-// conversion would queue on the quarter-rate conversion pipe (eight children
-// x six planes per node).
-HDCX_D float byteToFloat(uint32_t word, int index)
+// Byte `index` of `word` as the float 2^23 + byte: the byte is placed in the
+// low mantissa bits of 2^23 (bit pattern 0x4B0000bb). Subtracting 2^23 then
+// gives the byte's value exactly. A byte permute and an add run on full-rate
+// pipes, where an integer-to-float conversion would queue on the
+// quarter-rate conversion pipe (eight children x six planes per node).
+HDCX_D float biasedByte(uint32_t word, int index)
 {
-    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u + static_cast<uint32_t>(index))) - 8388608.0f;
+    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u + static_cast<uint32_t>(index)));
+}
+
+// Quantised planes of children 2j and 2j+1 (bytes k and k+1 of `word`, k
+// even) as distances t = q * a + b, two lanes per packed instruction.
+HDCX_D float2 planePair(uint32_t word, int k, float2 a, float2 b)
+{
+    const float2 q = __fadd2_rn(make_float2(biasedByte(word, k), biasedByte(word, k + 1)),
+                                make_float2(-8388608.0f, -8388608.0f));
+    return __ffma2_rn(q, a, b);
 }
 
 // State of one ray's traversal: the ray, the closest confirmed hit so far,
@@ -170,6 +206,18 @@ HDCX_D void beginTraversal(Traversal& st, const DeviceScene& s, float3 o, float3
 template <Accept kMode, bool kAny, bool kCount = false>
 HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint2* work)
 {
+    // Postponing: a triangle group on the stack has no hit bits in 24..31
+    // (a node group always has some), which tells the two apart on a pop.
+    // Only a lane with a node group in hand postpones, so the step still
+    // visits a node and the postponed group is not popped straight back.
+    if (kPostponeLanes > 0u) {
+        const uint32_t testing = __ballot_sync(__activemask(), st.triGroup.y != 0u);
+        if (st.triGroup.y != 0u && static_cast<uint32_t>(__popc(testing)) < kPostponeLanes &&
+            (st.nodeGroup.y & 0xff000000u) != 0u && st.sp < kPostponeDepth) {
+            stack[st.sp++] = st.triGroup;
+            st.triGroup.y = 0u;
+        }
+    }
     while (st.triGroup.y != 0u) {
         const int bit = __ffs(st.triGroup.y) - 1;
         st.triGroup.y &= st.triGroup.y - 1u;
@@ -200,9 +248,17 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
     }
     if ((st.nodeGroup.y & 0xff000000u) == 0u) {
         if (st.sp == 0) return kStepDone;
-        st.nodeGroup = stack[--st.sp];
+        const uint2 entry = stack[--st.sp];
+        if ((entry.y & 0xff000000u) == 0u) {  // a postponed triangle group
+            st.triGroup = entry;
+            return kStepContinue;
+        }
+        st.nodeGroup = entry;
     }
-    if (st.budget-- == 0u) return kStepDone;
+    if (st.budget-- == 0u) {
+        traversalFault(s, kTraversalBudget);
+        return kStepDone;
+    }
     // Next child of the current group, nearest octant first.
     const uint32_t hitBits = st.nodeGroup.y >> 24;
     const uint32_t pos = 31u - __clz(hitBits);
@@ -210,7 +266,10 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
     const uint32_t childSlot = pos ^ st.octInv;
     const uint32_t parentMask = st.nodeGroup.y & 0xffu;
     const uint32_t nodeIndex = st.nodeGroup.x + __popc(parentMask & ((1u << childSlot) - 1u));
-    if ((st.nodeGroup.y & 0xff000000u) != 0u && st.sp < kTraversalStack) stack[st.sp++] = st.nodeGroup;
+    if ((st.nodeGroup.y & 0xff000000u) != 0u) {
+        if (st.sp < kTraversalStack) stack[st.sp++] = st.nodeGroup;
+        else traversalFault(s, kTraversalOverflow);
+    }
 
     if (kCount) work->x++;
     const uint4* np = reinterpret_cast<const uint4*>(s.nodes + nodeIndex);
@@ -226,6 +285,8 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
     // t = q * (scale * invd) + (p - o) * invd per plane.
     const float ax = scx * idx, ay = scy * idy, az = scz * idz;
     const float bx = (px - o.x) * idx, by = (py - o.y) * idy, bz = (pz - o.z) * idz;
+    const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
+    const float2 bx2 = make_float2(bx, bx), by2 = make_float2(by, by), bz2 = make_float2(bz, bz);
     // Near/far planes by direction sign: words of qlo (n2.x..n3.y) and qhi (n3.z..n4.w).
     const uint32_t loX0 = n2.x, loX1 = n2.y, loY0 = n2.z, loY1 = n2.w, loZ0 = n3.x, loZ1 = n3.y;
     const uint32_t hiX0 = n3.z, hiX1 = n3.w, hiY0 = n4.x, hiY1 = n4.y, hiZ0 = n4.z, hiZ1 = n4.w;
@@ -237,21 +298,28 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
     const uint32_t octInv = st.octInv;
     const float bestT = st.bestT;
     uint32_t nodeHits = 0u, triHits = 0u;
+    // Children 2j and 2j+1 share a word per plane (bytes k and k+1). An
+    // empty slot has meta 0 and is not internal, so it adds no bits.
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int k = i & 3;
-        const uint32_t meta = ((i < 4 ? meta0 : meta1) >> (8 * k)) & 0xffu;
-        const float tnx = fmaf(byteToFloat(i < 4 ? nearX0 : nearX1, k), ax, bx);
-        const float tny = fmaf(byteToFloat(i < 4 ? nearY0 : nearY1, k), ay, by);
-        const float tnz = fmaf(byteToFloat(i < 4 ? nearZ0 : nearZ1, k), az, bz);
-        const float tfx = fmaf(byteToFloat(i < 4 ? farX0 : farX1, k), ax, bx);
-        const float tfy = fmaf(byteToFloat(i < 4 ? farY0 : farY1, k), ay, by);
-        const float tfz = fmaf(byteToFloat(i < 4 ? farZ0 : farZ1, k), az, bz);
-        const float tNear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-        const float tFar = fminf(fminf(tfx, tfy), fminf(tfz, bestT));
-        if (meta != 0u && tNear <= tFar) {
-            if ((imask >> i) & 1u) nodeHits |= 1u << (static_cast<uint32_t>(i) ^ octInv);
-            else triHits |= (meta >> 5) << (meta & 31u);
+    for (int j = 0; j < 4; ++j) {
+        const int k = (2 * j) & 3;
+        const bool low = j < 2;
+        const float2 tnx = planePair(low ? nearX0 : nearX1, k, ax2, bx2);
+        const float2 tny = planePair(low ? nearY0 : nearY1, k, ay2, by2);
+        const float2 tnz = planePair(low ? nearZ0 : nearZ1, k, az2, bz2);
+        const float2 tfx = planePair(low ? farX0 : farX1, k, ax2, bx2);
+        const float2 tfy = planePair(low ? farY0 : farY1, k, ay2, by2);
+        const float2 tfz = planePair(low ? farZ0 : farZ1, k, az2, bz2);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = 2 * j + h;
+            const uint32_t meta = ((low ? meta0 : meta1) >> (8 * (k + h))) & 0xffu;
+            const float tNear = fmaxf(fmaxf(h ? tnx.y : tnx.x, h ? tny.y : tny.x), fmaxf(h ? tnz.y : tnz.x, 0.0f));
+            const float tFar = fminf(fminf(h ? tfx.y : tfx.x, h ? tfy.y : tfy.x), fminf(h ? tfz.y : tfz.x, bestT));
+            if (tNear <= tFar) {
+                if ((imask >> i) & 1u) nodeHits |= 1u << (static_cast<uint32_t>(i) ^ octInv);
+                else triHits |= (meta >> 5) << (meta & 31u);
+            }
         }
     }
     st.nodeGroup = make_uint2(n1.x, (nodeHits << 24) | imask);

@@ -223,6 +223,7 @@ struct hdcx_tracer {
     uint32_t traceBlocksPerSm = 16;
     uint32_t shadeBlocksPerSm = 8;
     uint32_t sortHits = 0;   // shade hits in material order
+    uint32_t sortRays = 0;   // trace secondary rays in direction order
     uint32_t profiling = 0;  // HDCX_PROFILE_* bits
     // Scene.
     std::vector<DeviceBuffer*> sceneBuffers;
@@ -850,6 +851,7 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
     call.paths.traceBlocksPerSm = t->traceBlocksPerSm;
     call.paths.shadeBlocksPerSm = t->shadeBlocksPerSm;
     call.paths.sortHits = t->sortHits;
+    call.paths.sortRays = t->sortRays;
     check(cudaMemsetAsync(call.paths.stats, 0, 8 * sizeof(unsigned long long), t->stream), "clear stats");
     call.paths.cache = CacheDevice{};
     if (t->radianceCache) {
@@ -886,6 +888,20 @@ void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut, bool timeEv
     }
 }
 
+// The render's traversal fault word (DeviceScene::status): a dropped node
+// group or an exhausted node budget means hits may have been lost, so the
+// image is not trusted.
+void throwOnTraversalFault(unsigned long long word)
+{
+    const unsigned int bits = static_cast<unsigned int>(word);
+    if (bits == 0u) return;
+    std::string what = "render: traversal fault:";
+    if (bits & kTraversalOverflow) what += " a pending node group found the traversal stack full;";
+    if (bits & kTraversalBudget) what += " a ray visited more nodes than the BVH holds (malformed node array);";
+    what += " the image may have lost hits";
+    throw StatusError(HDCX_ERROR_INTERNAL, what);
+}
+
 // `graphMs` >= 0: the render ran inside a batch graph, whose device time it reports.
 void finishRender(hdcx_tracer* t, RenderCall& call, float graphMs = -1.0F)
 {
@@ -893,6 +909,7 @@ void finishRender(hdcx_tracer* t, RenderCall& call, float graphMs = -1.0F)
     t->xyzSamples = (call.frame.sampleIndex == 0 ? 0 : t->xyzSamples) + call.frame.sampleCount;
     unsigned long long counters[8];
     check(cudaMemcpy(counters, call.paths.stats, sizeof counters, cudaMemcpyDeviceToHost), "read stats");
+    throwOnTraversalFault(counters[7]);
     float ms = graphMs;
     if (graphMs < 0.0F) check(cudaEventElapsedTime(&ms, t->start, t->stop), "cudaEventElapsedTime");
     t->stats = hdcx_render_stats{};
@@ -1278,7 +1295,7 @@ HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* t, const hdcx_camera* camer
             t->fallbackAxisInitialized = true;
         }
         const FrameConst f = makeFrame(t, *camera, width, height, sampleIndex, maxBounces, sampleCount);
-        renderStatic(t->scene, f, reinterpret_cast<float4*>(rgbaDevice), t->stream);
+        throwOnTraversalFault(renderStatic(t->scene, f, reinterpret_cast<float4*>(rgbaDevice), t->stream));
         if (written) *written = 1;
     });
 }
@@ -1492,6 +1509,7 @@ HDCX_API hdcx_status hdcx_get_tuning(const hdcx_tracer* t, hdcx_tuning* out)
     out->trace_blocks_per_sm = t->traceBlocksPerSm;
     out->shade_blocks_per_sm = t->shadeBlocksPerSm;
     out->sort_hits = t->sortHits;
+    out->sort_rays = t->sortRays;
     return HDCX_OK;
 }
 
@@ -1499,13 +1517,14 @@ HDCX_API hdcx_status hdcx_set_tuning(hdcx_tracer* t, const hdcx_tuning* in)
 {
     if (!t || !in) return HDCX_ERROR_INVALID_ARGUMENT;
     if ((in->wave_paths != 0 && in->wave_paths < 3) || in->trace_blocks_per_sm < 1 || in->trace_blocks_per_sm > 64 ||
-        in->shade_blocks_per_sm < 1 || in->shade_blocks_per_sm > 64 || in->sort_hits > 1)
+        in->shade_blocks_per_sm < 1 || in->shade_blocks_per_sm > 64 || in->sort_hits > 1 || in->sort_rays > 1)
         return fail(t, HDCX_ERROR_INVALID_ARGUMENT,
-                    "tuning out of range (wave >= 3 paths or 0, 1..64 blocks per SM, sort_hits 0 or 1)");
+                    "tuning out of range (wave >= 3 paths or 0, 1..64 blocks per SM, sort_hits and sort_rays 0 or 1)");
     t->wavePaths = in->wave_paths;
     t->traceBlocksPerSm = in->trace_blocks_per_sm;
     t->shadeBlocksPerSm = in->shade_blocks_per_sm;
     t->sortHits = in->sort_hits;
+    t->sortRays = in->sort_rays;
     return HDCX_OK;
 }
 
@@ -1549,6 +1568,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
                 t->traceBlocksPerSm = cached.trace_blocks_per_sm;
                 t->shadeBlocksPerSm = cached.shade_blocks_per_sm;
                 t->sortHits = cached.sort_hits;
+                t->sortRays = cached.sort_rays;
                 if (result) *result = cached;
                 return HDCX_OK;
             }
@@ -1560,11 +1580,12 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         t->profiling = 0;
         ArenaLease lease = checkoutArena(t->device, true);  // one arena for every timed render
         // Best of two device-timed renders of one configuration.
-        auto measure = [&](uint64_t wave, uint32_t trace, uint32_t shade, uint32_t sort = 0) {
+        auto measure = [&](uint64_t wave, uint32_t trace, uint32_t shade, uint32_t sort = 0, uint32_t rays = 0) {
             t->wavePaths = wave;
             t->traceBlocksPerSm = trace;
             t->shadeBlocksPerSm = shade;
             t->sortHits = sort;
+            t->sortRays = rays;
             double ms = 1e30;
             for (int rep = 0; rep < 2; ++rep) {
                 RenderCall call;
@@ -1582,8 +1603,8 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         best.default_milliseconds = measure(0, 16, 8);
         best.milliseconds = best.default_milliseconds;
         best.candidates = 1;
-        auto consider = [&](uint64_t wave, uint32_t trace, uint32_t shade, uint32_t sort) {
-            const double ms = measure(wave, trace, shade, sort);
+        auto consider = [&](uint64_t wave, uint32_t trace, uint32_t shade, uint32_t sort, uint32_t rays = 0) {
+            const double ms = measure(wave, trace, shade, sort, rays);
             ++best.candidates;
             if (ms < best.milliseconds) {
                 best.milliseconds = ms;
@@ -1591,6 +1612,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
                 best.trace_blocks_per_sm = trace;
                 best.shade_blocks_per_sm = shade;
                 best.sort_hits = sort;
+                best.sort_rays = rays;
             }
         };
         // The hit sort first: whether it pays depends on how differently the
@@ -1612,6 +1634,8 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         for (uint32_t shade : {2u, 4u, 16u}) consider(best.wave_paths, best.trace_blocks_per_sm, shade, sort);
         // The sort again, the other way, at the chosen launch shape.
         consider(best.wave_paths, best.trace_blocks_per_sm, best.shade_blocks_per_sm, best.sort_hits ^ 1u);
+        // The ray sort, at the chosen launch shape and hit sort.
+        consider(best.wave_paths, best.trace_blocks_per_sm, best.shade_blocks_per_sm, best.sort_hits, 1u);
         // Arena buffers grown for a larger candidate than the one chosen are
         // released; the next render allocates the chosen wave.
         const uint64_t chosen = std::max<uint64_t>(3, std::min(needed, best.wave_paths ? best.wave_paths : kAutomaticWavePaths));
@@ -1623,6 +1647,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
         t->traceBlocksPerSm = best.trace_blocks_per_sm;
         t->shadeBlocksPerSm = best.shade_blocks_per_sm;
         t->sortHits = best.sort_hits;
+        t->sortRays = best.sort_rays;
         t->profiling = savedProfiling;
         {
             std::lock_guard<std::mutex> lock(gTuningLock);

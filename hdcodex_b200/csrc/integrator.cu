@@ -137,8 +137,14 @@ __global__ void generateKernel(FrameConst f, WaveDesc w, PathBuffers p)
 // ---------------------------------------------------------------------------
 // extend: closest hit of every queued ray (vulkan_path_tracer.cpp:1228-1243)
 // ---------------------------------------------------------------------------
+// Resident blocks of 128 threads per SM the traversal kernels are compiled
+// for (8: 64 registers per thread).
+#ifndef HDCX_TRACE_MIN_BLOCKS
+#define HDCX_TRACE_MIN_BLOCKS 8
+#endif
+
 template <Accept kMode, bool kCount>
-__global__ void __launch_bounds__(128, 8) extendKernel(DeviceScene s, PathBuffers p, const uint32_t* queue,
+__global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) extendKernel(DeviceScene s, PathBuffers p, const uint32_t* queue,
                                                     const uint32_t* count)
 {
     const uint32_t n = *count;
@@ -923,7 +929,7 @@ __global__ void __launch_bounds__(128) missKernel(DeviceScene s, FrameConst f, P
 // shadow: visibility of light samples (vulkan_path_tracer.cpp:855-912)
 // ---------------------------------------------------------------------------
 template <bool kOpaque, bool kCount>
-__global__ void __launch_bounds__(128, 8) shadowKernel(DeviceScene s, PathBuffers p)
+__global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(DeviceScene s, PathBuffers p)
 {
     const uint32_t n = p.counters[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(p.stats + 1, static_cast<unsigned long long>(n));
@@ -1208,6 +1214,102 @@ __global__ void __launch_bounds__(256) scatterHitsKernel(DeviceScene s, PathBuff
     }
 }
 
+// ---------------------------------------------------------------------------
+// ray sort (tuning knob sort_rays): secondary extension rays are reordered
+// within chunks of kRayChunk queue entries by a direction cell, so that a
+// warp traces rays of similar direction. The queue's own order already keeps
+// rays of nearby pixels, and so of nearby origins, close together: sorting
+// within a chunk keeps that and adds directional coherence, with no global
+// pass. Order within a cell is arbitrary; every path's result is independent
+// of queue order.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kRayChunk = 1024;  // queue entries per block iteration (256 threads x 4)
+constexpr uint32_t kRayCells = 128;   // 6 cube faces x 4 x 4 cells (96 used)
+
+__device__ __forceinline__ uint32_t directionCell(float4 d)
+{
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    uint32_t face;
+    float u, v, m;
+    if (ax >= ay && ax >= az) {
+        face = d.x < 0.0f ? 1u : 0u;
+        u = d.y;
+        v = d.z;
+        m = ax;
+    } else if (ay >= az) {
+        face = d.y < 0.0f ? 3u : 2u;
+        u = d.x;
+        v = d.z;
+        m = ay;
+    } else {
+        face = d.z < 0.0f ? 5u : 4u;
+        u = d.x;
+        v = d.y;
+        m = az;
+    }
+    const float inv = m > 0.0f ? 2.0f / m : 0.0f;  // (u/m + 1) * 2 in [0, 4]
+    const uint32_t cu = min(static_cast<uint32_t>(fmaxf(fmaf(u, inv, 2.0f), 0.0f)), 3u);
+    const uint32_t cv = min(static_cast<uint32_t>(fmaxf(fmaf(v, inv, 2.0f), 0.0f)), 3u);
+    return face * 16u + cu * 4u + cv;
+}
+
+__global__ void __launch_bounds__(256) sortRaysKernel(PathBuffers p, uint32_t* queue, const uint32_t* count)
+{
+    __shared__ uint32_t cursor[kRayCells];
+    __shared__ uint32_t sorted[kRayChunk];
+    const uint32_t n = *count;
+    constexpr uint32_t kPer = kRayChunk / 256u;
+    // The loop bound is the same for every thread of the block, so the
+    // barriers inside are reached by all of them.
+    for (uint32_t base = blockIdx.x * kRayChunk; base < n; base += gridDim.x * kRayChunk) {
+        if (threadIdx.x < kRayCells) cursor[threadIdx.x] = 0u;
+        __syncthreads();
+        uint32_t slot[kPer], cell[kPer], rank[kPer];
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) {
+            const uint32_t i = base + k * 256u + threadIdx.x;
+            slot[k] = i < n ? queue[i] : 0u;
+            cell[k] = i < n ? directionCell(p.rayDirection[slot[k]]) : 0u;
+            rank[k] = i < n ? atomicAdd(&cursor[cell[k]], 1u) : 0u;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32u) {
+            // Exclusive prefix sum of the cell counts, four cells per lane.
+            const uint32_t lane = threadIdx.x;
+            uint32_t c[4], local = 0u;
+#pragma unroll
+            for (uint32_t k = 0; k < 4u; ++k) {
+                c[k] = cursor[lane * 4u + k];
+                local += c[k];
+            }
+            uint32_t inclusive = local;
+#pragma unroll
+            for (uint32_t d = 1; d < 32u; d <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, inclusive, d);
+                if (lane >= d) inclusive += v;
+            }
+            uint32_t offset = inclusive - local;
+#pragma unroll
+            for (uint32_t k = 0; k < 4u; ++k) {
+                cursor[lane * 4u + k] = offset;
+                offset += c[k];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) {
+            if (base + k * 256u + threadIdx.x < n) sorted[cursor[cell[k]] + rank[k]] = slot[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) {
+            const uint32_t i = base + k * 256u + threadIdx.x;
+            if (i < n) queue[i] = sorted[k * 256u + threadIdx.x];
+        }
+        __syncthreads();
+    }
+}
+
 template <bool kCache>
 void launchShade(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, uint32_t bounce, const uint32_t* inQueue,
                  const uint32_t* inCount, uint32_t* outQueue, uint32_t* outCount, int grid, cudaStream_t stream)
@@ -1222,9 +1324,12 @@ void launchShade(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
     }
 }
 
-void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, FrameBuffers& fb,
+void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffers& paths, FrameBuffers& fb,
                  cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches, CacheRun* cacheRun)
 {
+    // Traversal faults go to the last word of the render's counters.
+    DeviceScene scene = sceneIn;
+    scene.status = reinterpret_cast<unsigned int*>(paths.stats + 7);
     const bool cacheMode = cacheRun != nullptr && cacheRun->cache != nullptr && paths.cache.enabled != 0u;
     if (!cacheMode) paths.cache.enabled = 0u;
     uint64_t launched = 0;
@@ -1237,6 +1342,7 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
     const int shadeGrid = gridFor(static_cast<uint32_t>(wavePaths), static_cast<int>(std::max(paths.shadeBlocksPerSm, 1u)));
     const int missGrid = gridFor(static_cast<uint32_t>(wavePaths), 8);
     const bool sortHits = paths.sortHits != 0u && paths.sortedHits != nullptr && paths.hitBins != nullptr;
+    const bool sortRays = paths.sortRays != 0u;
     const int sortGrid = std::max(1, gridFor(static_cast<uint32_t>(wavePaths), 8) / 2);  // 256-thread blocks
     std::vector<EventPair> events;
     auto timed = [&](int stage, auto&& launch) {
@@ -1263,6 +1369,10 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
             uint32_t* inCount = paths.counters + (bounce & 1u);
             uint32_t* outCount = paths.counters + ((bounce + 1u) & 1u);
             CUDA_OK(cudaMemsetAsync(paths.counters + 4, 0, 2 * sizeof(uint32_t), stream));
+            if (sortRays && bounce > 0u) {
+                sortRaysKernel<<<sortGrid, 256, 0, stream>>>(paths, inQueue, inCount);
+                launched += 1;
+            }
             timed(0, [&] {
                 if (countTraversal) {
                     if (scene.opaque) extendKernel<Accept::Opaque, true><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);

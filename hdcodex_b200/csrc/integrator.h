@@ -78,6 +78,9 @@ struct PathBuffers {
     uint32_t sortHits = 0;
     uint32_t* sortedHits = nullptr;
     uint32_t* hitBins = nullptr;
+    // Secondary extension rays traced in direction order (sortRays = 1): each
+    // chunk of 1024 queue entries is sorted in place by a direction cell.
+    uint32_t sortRays = 0;
 };
 
 // Per-pixel accumulation buffers of the current output size.

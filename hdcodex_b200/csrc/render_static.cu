@@ -107,7 +107,7 @@ void ok(cudaError_t e, const char* what)
 
 }  // namespace
 
-void renderStatic(const DeviceScene& scene, const FrameConst& frame, float4* rgba, cudaStream_t stream)
+unsigned int renderStatic(const DeviceScene& scene, const FrameConst& frame, float4* rgba, cudaStream_t stream)
 {
     const uint64_t pixels = static_cast<uint64_t>(frame.width) * frame.height;
     if (pixels > kStaticMaxPixels) throw std::invalid_argument("image larger than the static scratch maximum");
@@ -170,6 +170,9 @@ void renderStatic(const DeviceScene& scene, const FrameConst& frame, float4* rgb
     renderFrame(scene, frame, p, fb, stream, nullptr, false, nullptr);
     // The lock covers the GPU work too: the next call may reuse the array.
     ok(cudaStreamSynchronize(stream), "render");
+    unsigned long long faults = 0;  // renderFrame's traversal fault word
+    ok(cudaMemcpy(&faults, p.stats + 7, sizeof faults, cudaMemcpyDeviceToHost), "read the traversal fault word");
+    return static_cast<unsigned int>(faults);
 }
 
 }  // namespace hdcx

@@ -232,12 +232,13 @@ class PathTracer:
         self._check(lib().hdcx_get_tuning(self._h, C.byref(r)), "get_tuning")
         return {name: getattr(r, name) for name, _ in _abi.Tuning._fields_}
 
-    def set_tuning(self, wave_paths=0, trace_blocks_per_sm=16, shade_blocks_per_sm=8, sort_hits=0):
+    def set_tuning(self, wave_paths=0, trace_blocks_per_sm=16, shade_blocks_per_sm=8, sort_hits=0, sort_rays=0):
         """hdcx_set_tuning: paths per wave (0: automatic), blocks of 128 threads
         per SM for traversal and shading (1-64), sort_hits 1 to shade each
-        bounce's hits in material order. Images do not depend on these."""
+        bounce's hits in material order, sort_rays 1 to trace secondary rays
+        in direction order. Images do not depend on these."""
         r = _abi.Tuning(wave_paths=wave_paths, trace_blocks_per_sm=trace_blocks_per_sm,
-                        shade_blocks_per_sm=shade_blocks_per_sm, sort_hits=sort_hits)
+                        shade_blocks_per_sm=shade_blocks_per_sm, sort_hits=sort_hits, sort_rays=sort_rays)
         self._check(lib().hdcx_set_tuning(self._h, C.byref(r)), "set_tuning")
 
     def radiance_cache_stats(self) -> dict:

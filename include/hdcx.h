@@ -334,6 +334,8 @@ typedef struct hdcx_tuning {
     double default_milliseconds;   /* hdcx_autotune: device time of the defaults */
     uint32_t candidates;           /* hdcx_autotune: configurations timed (0: taken from the cache) */
     uint32_t sort_hits;            /* 1: hits are shaded in material order (a counting sort per bounce); default 0 */
+    uint32_t sort_rays;            /* 1: secondary rays are traced in direction order (a sort within chunks of
+                                      1024 queue entries per bounce); default 0 */
 } hdcx_tuning;
 
 /* Profiling switches for hdcx_set_profiling. */

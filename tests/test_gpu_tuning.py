@@ -77,3 +77,29 @@ def test_material_sorted_hits_render_the_same_image(make):
     for key in ("extension_rays", "shadow_rays", "subsurface_rays"):
         assert plain_stats[key] == sorted_stats[key], key
     assert sorted_stats["kernel_launches"] > plain_stats["kernel_launches"]
+
+
+@pytest.mark.parametrize("make", [
+    lambda: workloads.spectral_stress(width=96, height=54, spp=2, dome_size=(128, 64)),
+    lambda: workloads.heavy_geometry(width=96, height=54, spp=2, dome_size=(128, 64)),
+], ids=["stress", "heavy"])
+def test_direction_sorted_rays_render_the_same_image(make):
+    """sort_rays reorders each secondary extension queue by direction cell
+    within chunks of 1024 entries; per-path results do not depend on the
+    order, with or without the hit sort."""
+    wl = make()
+    with PathTracer(0) as t:
+        t.set_scene(wl.scene)
+        t.set_tuning(wave_paths=8192)
+        plain = t.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
+        plain_stats = t.stats()
+        for sort_hits in (0, 1):
+            t.set_tuning(wave_paths=8192, sort_hits=sort_hits, sort_rays=1)
+            assert t.tuning()["sort_rays"] == 1
+            img = t.render(wl.camera, wl.width, wl.height, 0, 8, wl.spp)
+            st = t.stats()
+            assert np.array_equal(plain, img), sort_hits
+            for key in ("extension_rays", "shadow_rays", "subsurface_rays"):
+                assert plain_stats[key] == st[key], key
+        with pytest.raises(RuntimeError, match="tuning out of range"):
+            t.set_tuning(sort_rays=2)
