@@ -136,6 +136,7 @@ struct DeviceScene {
     uint32_t hasMeshLights;
     uint32_t nodeCount;
     uint32_t fullShading;    // 0: no material uses textures or layered lobes (see shadeKernel)
+    uint32_t hasSubsurface;  // some material can take the subsurface random walk
     // Traversal faults of the current render (kTraversalOverflow,
     // kTraversalBudget; null: not recorded). Set per render to a word the
     // host reads back with the render's counters.

@@ -126,13 +126,16 @@ struct PathStore {
         p.counters = alloc<uint32_t>(8);
         p.sortedHits = alloc<uint32_t>(n);
         p.hitBins = alloc<uint32_t>(2 * kHitBins);
+        p.walkEntry = alloc<float4>(n);
+        p.walkNormal = alloc<float4>(n);
+        p.walkState = alloc<float4>(n);
     }
 };
 
 // ---------------------------------------------------------------------------
 // Path arenas
 //
-// A render needs the path state of its waves (about 311 bytes per path) only
+// A render needs the path state of its waves (about 359 bytes per path) only
 // while it runs, so path state belongs to a per-device pool of arenas rather
 // than to tracers: hdcx_render and hdcx_autotune check an arena out for the
 // call, hdcx_render_batch one per lane until the batch's work has finished.
@@ -353,6 +356,19 @@ bool needsFullShading(const PackedSceneData& d)
     return false;
 }
 
+// Whether any material can take the subsurface walk: a subsurface weight
+// above zero (or NaN) or a subsurface-weight texture.
+bool hasSubsurfaceMaterial(const PackedSceneData& d)
+{
+    const size_t n = d.materials.size() / HDCX_GPU_MATERIAL_BYTES;
+    for (size_t i = 0; i < n; ++i) {
+        GpuMaterial m;
+        std::memcpy(&m, d.materials.data() + i * HDCX_GPU_MATERIAL_BYTES, sizeof m);
+        if (!(m.subsurfaceWeightScale.x <= 0.0F) || m.textureIndices2.x != HDCX_MISSING_TEXTURE) return true;
+    }
+    return false;
+}
+
 // The arrays behind TexDesc::cdf for a dome importance texture (R: the
 // row's conditional CDF, G at column 0: the marginal CDF). Returns false, and
 // the device keeps the plain binary search, unless every CDF is finite and
@@ -431,6 +447,7 @@ void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
     s.lightCount = std::min(d.lightCount, static_cast<uint32_t>(HDCX_MAX_LIGHTS));
     s.opaque = d.opaque ? 1u : 0u;
     s.fullShading = needsFullShading(d) ? 1u : 0u;
+    s.hasSubsurface = hasSubsurfaceMaterial(d) ? 1u : 0u;
     s.hasMeshLights = (d.triangleCount() > 0 && d.emissive[(size_t(d.triangleCount()) - 1) * 4u] > 0.0F) ? 1u : 0u;
     {
         // Scene box (padded by 0.1% per side) for the radiance-cache positions.
@@ -501,8 +518,9 @@ void ensureOutput(hdcx_tracer* t, uint32_t w, uint32_t h)
 }
 
 constexpr uint64_t kAutomaticWavePaths = 12ull << 20;  // ~12.6M paths per wave
-// Device bytes of path state per path (PathBuffers with three shadow slots).
-constexpr uint64_t kPathStateBytes = 143 + 3 * 56;
+// Device bytes of path state per path (PathBuffers with three shadow slots
+// and the deferred subsurface-walk records).
+constexpr uint64_t kPathStateBytes = 143 + 48 + 3 * 56;
 
 // Smallest wave an automatic wave is shrunk to when device memory is short.
 constexpr uint64_t kMinimumAutomaticWave = 1ull << 16;

@@ -302,18 +302,40 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
 // the non-full ones are capped at 80 registers so that six blocks fit an SM
 // instead of four, the full ones at 128 registers for four blocks instead of
 // three; each costs a few spilled values and gains 4-6% of the kernel's time.
-template <bool kFull, bool kLit, bool kCache>
+//
+// kWalk: how a subsurface random walk (:1153-1186) runs.
+//   kWalkInline - inside this kernel, nested in shading (the radiance-cache
+//                 mode and renders without walk buffers);
+//   kWalkDefer  - the walk's start (entry, normal, mean free path, albedo,
+//                 anisotropy, RNG state, throughput) is recorded and the path
+//                 handed to walkKernel, a traversal kernel; everything before
+//                 it in the bounce (emission, the light sample, the radiance
+//                 so far) is done. On the last bounce the walk cannot change
+//                 the image and is not run;
+//   kWalkReplay - re-shades a path whose deferred walk failed (a boundary ray
+//                 escaped): the same bounce from its stored start, with the
+//                 light sample and radiance writes of the first pass
+//                 suppressed, taking the walk's RNG state after the failed
+//                 walk at the walk's place and continuing with the diffuse
+//                 lobe as the inline form does.
+// All three give the same bits.
+enum : int { kWalkInline = 0, kWalkDefer = 1, kWalkReplay = 2 };
+
+template <bool kFull, bool kLit, bool kCache, int kWalk = kWalkInline>
 __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
     shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce, const uint32_t* queue,
                 const uint32_t* count, uint32_t* nextQueue, uint32_t* nextCount)
 {
+    constexpr bool kReplay = kWalk == kWalkReplay;
+    static_assert(kWalk == kWalkInline || (kFull && !kCache), "deferred walks are for the full plain kernel");
     const uint32_t n = *count;
     const bool lastBounce = bounce + 1u >= f.maxBounces;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t slot = queue[i];
         float radiance = p.radiance[slot];
         // Light-sample contributions of the previous bounce, in slot order.
-        for (uint32_t k = 0; k < 3u; ++k) {
+        // (A replay finds this bounce's own samples in the slots: they stay.)
+        for (uint32_t k = 0; k < 3u && !kReplay; ++k) {
             uint8_t& valid = p.contributionValid[k * p.capacity + slot];
             if (valid) {
                 radiance += p.contribution[k * p.capacity + slot];
@@ -338,6 +360,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
         const float4 hitRec = p.hit[slot];
         const uint32_t primitive = __float_as_uint(hitRec.y);
         bool alive = true;
+        bool deferred = false;  // kWalkDefer: walkKernel finishes this bounce
 
         if (primitive == kInvalidPrimitive) {
             // :1245-1255
@@ -658,7 +681,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                                                                              translucentProbability))
                                        : 1.0f;
                         const float a = throughput * direct * spectralLight;
-                        traceSurfaceLightSample(p, s, spec, slot, 0u, kShadowAnalytic, lightIndex, light,
+                        if (!kReplay) traceSurfaceLightSample(p, s, spec, slot, 0u, kShadowAnalytic, lightIndex, light,
                                                 offsetSurfaceOrigin(hit, orientedGeometricNormal, lightDirection), lightDirection,
                                                 maximumShadowDistance, a, inversePdf, misWeight, gmax(lightSelectionPdf, 1e-8f));
                     }
@@ -673,7 +696,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                 const float direct = evaluateDirectSurface(normal, tangent, viewDirection, sunDirection, sp, 1.0f, 1.0f);
                 if (direct > 0.0f) {
                     const float spectralSun = illuminantSpectrum(f3(3.45575f, 3.14159f, 2.82743f), spec);
-                    traceSurfaceLightSample(p, s, spec, slot, 0u, kShadowSun, 0u, dummy,
+                    if (!kReplay) traceSurfaceLightSample(p, s, spec, slot, 0u, kShadowSun, 0u, dummy,
                                             offsetSurfaceOrigin(hit, orientedGeometricNormal, sunDirection), sunDirection,
                                             10000.0f, throughput * direct * spectralSun, 0.0f, 0.0f, 0.0f);
                 }
@@ -681,7 +704,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                 const float skyDirect = evaluateDirectSurface(normal, tangent, viewDirection, skyDirection, sp, 1.0f, 0.0f);
                 if (skyDirect > 0.0f) {
                     const float spectralSky = illuminantSpectrum(environment(s, f, skyDirection), spec);
-                    traceSurfaceLightSample(p, s, spec, slot, 1u, kShadowSky, 0u, dummy,
+                    if (!kReplay) traceSurfaceLightSample(p, s, spec, slot, 1u, kShadowSky, 0u, dummy,
                                             offsetSurfaceOrigin(hit, orientedGeometricNormal, skyDirection), skyDirection,
                                             10000.0f, throughput * skyDirect * spectralSky,
                                             kPi / gmax(dot(normal, skyDirection), 1e-4f), 0.0f, 0.0f);
@@ -692,7 +715,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                         evaluateDirectSurface(normal, tangent, viewDirection, backSkyDirection, sp, 1.0f, 0.0f);
                     if (backSkyDirect > 0.0f) {
                         const float spectralSky = illuminantSpectrum(environment(s, f, backSkyDirection), spec);
-                        traceSurfaceLightSample(p, s, spec, slot, 2u, kShadowSky, 0u, dummy,
+                        if (!kReplay) traceSurfaceLightSample(p, s, spec, slot, 2u, kShadowSky, 0u, dummy,
                                                 offsetSurfaceOrigin(hit, orientedGeometricNormal, backSkyDirection),
                                                 backSkyDirection, 10000.0f, throughput * backSkyDirect * spectralSky,
                                                 kPi / gmax(dot(-normal, backSkyDirection), 1e-4f), 0.0f, 0.0f);
@@ -741,7 +764,8 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                             const float a = throughput * direct * spectralLight;
                             const float maxDistance = gmax(lightDistance - 0.003f, 0.001f);
                             const float f1 = misWeight / lightPdf;
-                            if (maxDistance <= 0.001f) {
+                            if (kReplay) {
+                            } else if (maxDistance <= 0.001f) {
                                 setContribution(p, slot, 1u, a * f1);
                             } else {
                                 emitShadow(p, slot, 1u, kShadowMesh, 0u,
@@ -835,9 +859,26 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                                 const float albedo = reflectanceSpectrum(subsurfaceColorRgb, spec);
                                 float3 exitOrigin, exitDirection;
                                 float attenuation;
-                                if (randomWalkSubsurface(s, p, hit, orientedGeometricNormal, radius, albedo,
-                                                         material->subsurfaceWeightScale.z, rng, exitOrigin, exitDirection,
-                                                         attenuation)) {
+                                if (kWalk == kWalkDefer) {
+                                    if (!lastBounce) {
+                                        p.walkEntry[slot] = make_float4(hit.x, hit.y, hit.z, radius);
+                                        p.walkNormal[slot] = make_float4(orientedGeometricNormal.x, orientedGeometricNormal.y,
+                                                                         orientedGeometricNormal.z, albedo);
+                                        p.walkState[slot] = make_float4(material->subsurfaceWeightScale.z,
+                                                                        __uint_as_float(rng), throughput, 0.0f);
+                                        // This bounce's extension queue has been traced: it holds the walks.
+                                        uint32_t* walks = (bounce & 1u) ? p.queue[1] : p.queue[0];
+                                        walks[appendIndex(p.counters + 6)] = slot;
+                                    }
+                                    deferred = true;
+                                    break;
+                                }
+                                if (kWalk == kWalkReplay) {
+                                    // The deferred walk failed; its RNG state after the walk.
+                                    rng = __float_as_uint(p.walkState[slot].y);
+                                } else if (randomWalkSubsurface(s, p, hit, orientedGeometricNormal, radius, albedo,
+                                                                material->subsurfaceWeightScale.z, rng, exitOrigin,
+                                                                exitDirection, attenuation)) {
                                     throughput = throughput * attenuation;
                                     rayOrigin = exitOrigin;
                                     rayDirection = exitDirection;
@@ -881,8 +922,8 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             }
         } while (false);
 
-        p.radiance[slot] = radiance;
-        if (!alive || lastBounce) continue;
+        if (!kReplay) p.radiance[slot] = radiance;
+        if (deferred || !alive || lastBounce) continue;
         p.rng[slot] = rng;
         p.throughput[slot] = throughput;
         p.flags[slot] = (environmentOnMiss ? kFlagEnvironmentOnMiss : 0u) | (previousWasDelta ? kFlagPreviousWasDelta : 0u) |
@@ -892,6 +933,43 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
         p.rayOrigin[slot] = make_float4(rayOrigin.x, rayOrigin.y, rayOrigin.z, 0.0f);
         p.rayDirection[slot] = make_float4(rayDirection.x, rayDirection.y, rayDirection.z, 0.0f);
         nextQueue[appendIndex(nextCount)] = slot;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// walk: the deferred subsurface random walks of one bounce (:1153-1186), a
+// traversal kernel of its own instead of up to eight traversals nested in the
+// full shade kernel. A walk that exits finishes the bounce as the inline form
+// does (the exit ray is the path's next ray; no MIS bookkeeping, no roulette);
+// a walk whose boundary ray escapes stores its RNG state and queues the path
+// for shadeKernel<..., kWalkReplay>, which finishes the bounce the inline way.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS)
+    walkKernel(DeviceScene s, PathBuffers p, const uint32_t* walks, uint32_t* nextQueue, uint32_t* nextCount,
+               uint32_t* replayQueue)
+{
+    const uint32_t n = p.counters[6];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = walks[i];
+        const float4 entry = p.walkEntry[slot];
+        const float4 outward = p.walkNormal[slot];
+        const float4 state = p.walkState[slot];
+        uint32_t rng = __float_as_uint(state.y);
+        float3 exitOrigin, exitDirection;
+        float attenuation;
+        if (randomWalkSubsurface(s, p, xyz(entry), xyz(outward), entry.w, outward.w, state.x, rng, exitOrigin,
+                                 exitDirection, attenuation)) {
+            p.rng[slot] = rng;
+            p.throughput[slot] = state.z * attenuation;
+            p.flags[slot] = kFlagEnvironmentOnMiss | kFlagPreviousWasDelta | (p.flags[slot] & kFlagInsideMedium);
+            p.previousPdf[slot] = make_float2(0.0f, p.previousPdf[slot].y);
+            p.rayOrigin[slot] = make_float4(exitOrigin.x, exitOrigin.y, exitOrigin.z, 0.0f);
+            p.rayDirection[slot] = make_float4(exitDirection.x, exitDirection.y, exitDirection.z, 0.0f);
+            nextQueue[appendIndex(nextCount)] = slot;
+        } else {
+            p.walkState[slot] = make_float4(state.x, __uint_as_float(rng), state.z, 0.0f);
+            replayQueue[appendIndex(p.counters + 7)] = slot;
+        }
     }
 }
 
@@ -1310,14 +1388,27 @@ __global__ void __launch_bounds__(256) sortRaysKernel(PathBuffers p, uint32_t* q
     }
 }
 
+// Whether the full shade kernel defers subsurface walks to walkKernel: the
+// plain (non-cache) mode with walk buffers.
+bool deferWalks(const PathBuffers& paths, bool cacheMode)
+{
+    return !cacheMode && paths.walkEntry != nullptr && paths.walkNormal != nullptr && paths.walkState != nullptr;
+}
+
 template <bool kCache>
 void launchShade(const DeviceScene& scene, const FrameConst& frame, PathBuffers& paths, uint32_t bounce, const uint32_t* inQueue,
                  const uint32_t* inCount, uint32_t* outQueue, uint32_t* outCount, int grid, cudaStream_t stream)
 {
     const bool lit = scene.lightCount > 0u && !scene.hasMeshLights;
     if (scene.fullShading) {
-        if (lit) shadeKernel<true, true, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
-        else shadeKernel<true, false, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+        if (!kCache && deferWalks(paths, kCache)) {
+            if (lit) shadeKernel<true, true, false, kWalkDefer><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+            else shadeKernel<true, false, false, kWalkDefer><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+        } else if (lit) {
+            shadeKernel<true, true, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+        } else {
+            shadeKernel<true, false, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+        }
     } else {
         if (lit) shadeKernel<false, true, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
         else shadeKernel<false, false, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
@@ -1343,6 +1434,8 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
     const int missGrid = gridFor(static_cast<uint32_t>(wavePaths), 8);
     const bool sortHits = paths.sortHits != 0u && paths.sortedHits != nullptr && paths.hitBins != nullptr;
     const bool sortRays = paths.sortRays != 0u;
+    // Subsurface walks in walkKernel (scenes that can take them, plain mode).
+    const bool walks = scene.fullShading && scene.hasSubsurface && deferWalks(paths, cacheMode);
     const int sortGrid = std::max(1, gridFor(static_cast<uint32_t>(wavePaths), 8) / 2);  // 256-thread blocks
     std::vector<EventPair> events;
     auto timed = [&](int stage, auto&& launch) {
@@ -1368,7 +1461,7 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
             uint32_t* outQueue = paths.queue[(bounce + 1u) & 1u];
             uint32_t* inCount = paths.counters + (bounce & 1u);
             uint32_t* outCount = paths.counters + ((bounce + 1u) & 1u);
-            CUDA_OK(cudaMemsetAsync(paths.counters + 4, 0, 2 * sizeof(uint32_t), stream));
+            CUDA_OK(cudaMemsetAsync(paths.counters + 4, 0, 4 * sizeof(uint32_t), stream));
             if (sortRays && bounce > 0u) {
                 sortRaysKernel<<<sortGrid, 256, 0, stream>>>(paths, inQueue, inCount);
                 launched += 1;
@@ -1397,6 +1490,20 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
                 if (cacheMode) launchShade<true>(scene, frame, paths, bounce, hits, paths.counters + 4, outQueue, outCount, shadeGrid, stream);
                 else launchShade<false>(scene, frame, paths, bounce, hits, paths.counters + 4, outQueue, outCount, shadeGrid, stream);
                 missKernel<<<missGrid, 128, 0, stream>>>(scene, frame, paths);
+                if (walks) {
+                    // The deferred walks (in this bounce's traced extension
+                    // queue), then the failed ones re-shaded (queued in the
+                    // miss queue, which missKernel has consumed).
+                    walkKernel<<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, outQueue, outCount, paths.missQueue);
+                    const bool lit = scene.lightCount > 0u && !scene.hasMeshLights;
+                    if (lit) {
+                        shadeKernel<true, true, false, kWalkReplay><<<missGrid, 128, 0, stream>>>(
+                            scene, frame, paths, bounce, paths.missQueue, paths.counters + 7, outQueue, outCount);
+                    } else {
+                        shadeKernel<true, false, false, kWalkReplay><<<missGrid, 128, 0, stream>>>(
+                            scene, frame, paths, bounce, paths.missQueue, paths.counters + 7, outQueue, outCount);
+                    }
+                }
             });
             CUDA_OK(cudaGetLastError());
             timed(2, [&] {
@@ -1409,7 +1516,7 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
                 }
             });
             CUDA_OK(cudaGetLastError());
-            launched += sortHits ? 7 : 4;
+            launched += (sortHits ? 7 : 4) + (walks ? 2 : 0);
         }
         if (cacheMode) {
             // Predictions for the terminated paths, then one training round on

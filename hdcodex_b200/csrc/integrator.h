@@ -63,7 +63,9 @@ struct PathBuffers {
     float4* shadowFactors = nullptr;    // f1, f2, f3
     uint32_t* shadowSlot = nullptr;     // path slot * 4 + k
     uint32_t* shadowInfo = nullptr;     // kind | light << 8
-    uint32_t* counters = nullptr;       // [0], [1] extension queues, [2] shadow queue, [4] hits, [5] misses (8 entries)
+    // [0], [1] extension queues, [2] shadow queue, [4] hits, [5] misses,
+    // [6] deferred subsurface walks, [7] failed walks to re-shade (8 entries)
+    uint32_t* counters = nullptr;
     // extension, shadow, subsurface rays; extension node visits and triangle
     // tests; shadow node visits and triangle tests (counting mode)
     unsigned long long* stats = nullptr;
@@ -81,6 +83,12 @@ struct PathBuffers {
     // Secondary extension rays traced in direction order (sortRays = 1): each
     // chunk of 1024 queue entries is sorted in place by a direction cell.
     uint32_t sortRays = 0;
+    // Deferred subsurface walks (all three set, else walks run inside the
+    // shade kernel): per path slot, the walk's entry point and mean free path,
+    // outward normal and albedo, and (anisotropy, RNG state, throughput).
+    float4* walkEntry = nullptr;
+    float4* walkNormal = nullptr;
+    float4* walkState = nullptr;
 };
 
 // Per-pixel accumulation buffers of the current output size.

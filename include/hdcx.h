@@ -415,7 +415,7 @@ HDCX_API int32_t hdcx_get_shading_mode(const hdcx_tracer* tracer);
  * RGBA32F image (width*height*4 floats, row 0 = bottom) is copied into it.
  * With no geometry or a zero size nothing is traced and *written = 0
  * (the reference returns an empty vector, :3235); otherwise *written = 1.
- * Device memory: the path state of a wave (about 311 bytes per path) lives in
+ * Device memory: the path state of a wave (about 359 bytes per path) lives in
  * a per-device pool of arenas, not in the tracer: a call checks out a free
  * arena (at most eight per device; when all are busy it waits for one) and
  * grows it to its wave, and the arenas are freed with the device's last
@@ -537,7 +537,7 @@ HDCX_API hdcx_status hdcx_set_tuning(hdcx_tracer* tracer, const hdcx_tuning* tun
  * size, bounce budget and sample count over wave sizes and traversal/shade
  * grid sizes and the hit sort, one knob at a time from the defaults, keeps the fastest on the
  * tracer and returns it. Wave sizes of 1M to 48M paths are tried, the larger
- * ones while their path state (about 311 bytes per path) fits half of the free
+ * ones while their path state (about 359 bytes per path) fits half of the free
  * device memory; a path arena grown for a candidate larger than the one kept
  * is released before it returns. Results are cached per device and workload shape
  * (triangles, pixels, samples, bounces, shading variant) for the process, so
