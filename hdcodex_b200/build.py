@@ -27,6 +27,7 @@ SOURCES = [
     "nrc.cu",
     "render_static.cu",
     "scene_pack.cpp",
+    "device_memory.cpp",
     "hdcx_api.cpp",
 ]
 

@@ -14,6 +14,7 @@
 //      8 bits per plane against a power-of-two step, padded by one step on
 //      every side; leaf triangles are copied in leaf order.
 #include "bvh_build.h"
+#include "device_memory.h"
 
 #include <cub/cub.cuh>
 
@@ -418,9 +419,7 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
 template <typename T>
 T* deviceAlloc(size_t count)
 {
-    void* p = nullptr;
-    CUDA_OK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-    return static_cast<T*>(p);
+    return static_cast<T*>(deviceMalloc(std::max<size_t>(count, 1) * sizeof(T)));
 }
 
 }  // namespace
@@ -434,8 +433,7 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
     const int blocks = (n + kBlock - 1) / kBlock;
     std::vector<void*> temps;
     auto tmp = [&](size_t bytes) {
-        void* p = nullptr;
-        CUDA_OK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+        void* p = deviceMalloc(std::max<size_t>(bytes, 16));
         temps.push_back(p);
         return p;
     };
@@ -520,19 +518,19 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
         out.depth = depth;
         out.triangleCount = triangleCount;
     } catch (...) {
-        for (void* p : temps) cudaFree(p);
-        if (out.nodes) cudaFree(out.nodes);
-        if (out.triVerts) cudaFree(out.triVerts);
+        for (void* p : temps) deviceFree(p);
+        deviceFree(out.nodes);
+        deviceFree(out.triVerts);
         throw;
     }
-    for (void* p : temps) cudaFree(p);
+    for (void* p : temps) deviceFree(p);
     return out;
 }
 
 void freeWideBvh(WideBvh& bvh)
 {
-    if (bvh.nodes) cudaFree(bvh.nodes);
-    if (bvh.triVerts) cudaFree(bvh.triVerts);
+    deviceFree(bvh.nodes);
+    deviceFree(bvh.triVerts);
     bvh = WideBvh{};
 }
 

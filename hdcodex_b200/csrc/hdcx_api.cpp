@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <memory>
 #include <mutex>
 #include <cmath>
@@ -21,6 +22,7 @@
 
 #include "batch_plan.h"
 #include "bvh_build.h"
+#include "device_memory.h"
 #include "integrator.h"
 #include "nrc.h"
 #include "render_static.h"
@@ -52,14 +54,14 @@ struct DeviceBuffer {
     ~DeviceBuffer() { reset(); }
     void reset()
     {
-        if (ptr) cudaFree(ptr);
+        deviceFree(ptr);
         ptr = nullptr;
         bytes = 0;
     }
     void allocate(size_t n)
     {
         reset();
-        check(cudaMalloc(&ptr, std::max<size_t>(n, 16)), "cudaMalloc");
+        ptr = deviceMalloc(n);
         bytes = n;
     }
     template <typename T>
@@ -322,6 +324,8 @@ hdcx_status guarded(hdcx_tracer* t, F&& body)
         return HDCX_OK;
     } catch (const StatusError& e) {
         return fail(t, e.status, e.what());
+    } catch (const OutOfDeviceMemory& e) {
+        return fail(t, HDCX_ERROR_OUT_OF_MEMORY, e.what());
     } catch (const std::invalid_argument& e) {
         return fail(t, HDCX_ERROR_INVALID_ARGUMENT, e.what());
     } catch (const std::bad_alloc&) {
@@ -696,6 +700,36 @@ HDCX_API hdcx_status hdcx_probe_devices(int32_t* supported, int32_t* deviceCount
     if (supported) *supported = ok;
     if (deviceCount) *deviceCount = count;
     return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_set_device_memory_limit(int32_t device, uint64_t bytes)
+{
+    if (device < 0 || device >= 64) return HDCX_ERROR_INVALID_ARGUMENT;
+    setDeviceMemoryLimit(device, bytes);
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_get_device_memory_usage(int32_t device, uint64_t* inUse, uint64_t* limit)
+{
+    if (device < 0 || device >= 64) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (inUse) *inUse = deviceMemoryInUse(device);
+    if (limit) *limit = deviceMemoryLimit(device);
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_test_break_bvh(hdcx_tracer* t)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (!t->geometryReady || t->scene.nodes == nullptr || t->scene.nodeCount < 8u)
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_test_break_bvh: needs a BVH of at least 8 nodes");
+    return guarded(t, [&] {
+        // WideNode::childBase of node 0: the root's internal children become nodes 0..7.
+        static_assert(offsetof(WideNode, childBase) == 16, "WideNode layout");
+        const uint32_t zero = 0;
+        auto* field = reinterpret_cast<char*>(const_cast<WideNode*>(t->scene.nodes)) + offsetof(WideNode, childBase);
+        check(cudaMemcpyAsync(field, &zero, sizeof zero, cudaMemcpyHostToDevice, t->stream), "break BVH");
+        check(cudaStreamSynchronize(t->stream), "break BVH");
+    });
 }
 
 HDCX_API hdcx_status hdcx_create(int32_t device, hdcx_tracer** out)

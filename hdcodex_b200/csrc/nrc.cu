@@ -28,6 +28,8 @@
 // waits (bounded) for the MMA in flight, frees its tensor memory and returns.
 #include "nrc.h"
 
+#include "device_memory.h"
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -525,9 +527,7 @@ __global__ void refreshKernel(const float* params, uint32_t n, __nv_bfloat16* ti
 template <typename T>
 T* deviceAlloc(size_t count)
 {
-    void* p = nullptr;
-    NRC_OK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-    return static_cast<T*>(p);
+    return static_cast<T*>(deviceMalloc(std::max<size_t>(count, 1) * sizeof(T)));
 }
 
 }  // namespace
@@ -647,7 +647,7 @@ void destroy(Cache* c)
                     static_cast<void*>(c->mlpV), static_cast<void*>(c->mlpTiled), static_cast<void*>(c->grid),
                     static_cast<void*>(c->gridGrad), static_cast<void*>(c->gridM), static_cast<void*>(c->gridV),
                     static_cast<void*>(c->gridHalf), static_cast<void*>(c->loss), static_cast<void*>(c->error)})
-        cudaFree(p);
+        deviceFree(p);
     delete c;
 }
 

@@ -85,6 +85,9 @@ SIGNATURES = {
     "hdcx_get_stats": (C.c_int, [_P, C.POINTER(_abi.RenderStats)]),
     "hdcx_set_wave_size": (C.c_int, [_P, C.c_uint64]),
     "hdcx_set_profiling": (C.c_int, [_P, C.c_uint32]),
+    "hdcx_set_device_memory_limit": (C.c_int, [C.c_int32, C.c_uint64]),
+    "hdcx_get_device_memory_usage": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "hdcx_test_break_bvh": (C.c_int, [_P]),
 }
 
 PROFILE_STAGE_TIMES = 1
@@ -107,6 +110,23 @@ def lib():
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def set_device_memory_limit(device: int, limit_bytes: int):
+    """hdcx_set_device_memory_limit: the library's device-memory budget on
+    `device` (0 removes it)."""
+    status = lib().hdcx_set_device_memory_limit(device, limit_bytes)
+    if status != 0:
+        raise RuntimeError(f"hdcx_set_device_memory_limit failed: {STATUS.get(status, status)}")
+
+
+def device_memory_usage(device: int):
+    """(bytes the library holds on `device`, its budget or 0)."""
+    used, limit = C.c_uint64(0), C.c_uint64(0)
+    status = lib().hdcx_get_device_memory_usage(device, C.byref(used), C.byref(limit))
+    if status != 0:
+        raise RuntimeError(f"hdcx_get_device_memory_usage failed: {STATUS.get(status, status)}")
+    return int(used.value), int(limit.value)
 
 
 def probe_devices():

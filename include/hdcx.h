@@ -366,6 +366,19 @@ HDCX_API void hdcx_mesh_defaults(hdcx_mesh_desc* mesh);
  * CUDA device of compute capability 10.x is present. */
 HDCX_API hdcx_status hdcx_probe_devices(int32_t* supported, int32_t* device_count);
 
+/* Budget of the device memory the library may hold on `device`, in bytes (0:
+ * no budget, the default). No counterpart in the reference, whose Vulkan
+ * allocations are bounded only by the device. Every allocation of the
+ * library (path arenas, scene and BVH buffers, the BVH build's temporaries,
+ * radiance caches; not hdcx_render_static's static array) counts against it;
+ * one that would exceed it fails like an exhausted device: the call returns
+ * HDCX_ERROR_OUT_OF_MEMORY with a message, launches nothing for that call,
+ * and the tracer stays usable. Allocations already made are kept when the
+ * budget is lowered. Device ordinals 0..63. */
+HDCX_API hdcx_status hdcx_set_device_memory_limit(int32_t device, uint64_t bytes);
+/* Bytes the library holds on `device`, and its budget (0: none). */
+HDCX_API hdcx_status hdcx_get_device_memory_usage(int32_t device, uint64_t* in_use, uint64_t* limit);
+
 /* ---------------------------------------------------------------------------
  * Tracer lifetime (VulkanPathTracer constructor/destructor,
  * vulkan_path_tracer.cpp:3348-3350; render_delegate.cpp:113-132 constructs it)
@@ -618,6 +631,20 @@ HDCX_API hdcx_status hdcx_set_radiance_cache(hdcx_tracer* tracer, hdcx_nrc* cach
  * used, and the mean loss of the last training step. */
 HDCX_API hdcx_status hdcx_get_radiance_cache_stats(const hdcx_tracer* tracer, uint64_t* queries, uint64_t* samples,
                                                    float* last_loss);
+
+/* ---------------------------------------------------------------------------
+ * Test support (failure detection). No counterpart in the reference.
+ * ------------------------------------------------------------------------- */
+
+/* Makes the tracer's BVH cyclic for a test of traversal-fault reporting: the
+ * root node's internal children are redirected to the root itself and the
+ * seven nodes after it (all in bounds, so nothing is read outside the node
+ * array). Rays that enter the redirected child then revisit nodes until
+ * their node budget or their stack runs out, which the traversal records;
+ * the next hdcx_render returns HDCX_ERROR_INTERNAL ("traversal fault") and
+ * the tracer stays usable. hdcx_set_scene rebuilds a valid BVH. Requires a
+ * BVH of at least 8 nodes (else HDCX_ERROR_INVALID_ARGUMENT). */
+HDCX_API hdcx_status hdcx_test_break_bvh(hdcx_tracer* tracer);
 
 #ifdef __cplusplus
 }

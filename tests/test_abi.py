@@ -117,3 +117,18 @@ def test_struct_fields_match_the_header(tmp_path):
     assert len(got) == len(expected)
     mismatched = [(c, f, e, g) for (c, f, e), g in zip(expected, got) if e != g]
     assert not mismatched, mismatched
+
+
+def test_device_memory_budget_entry_points(hdcx_lib):
+    """The budget is host bookkeeping: settable and readable without a GPU,
+    device ordinals outside 0..63 are rejected."""
+    from hdcodex_b200.tracer import device_memory_usage, set_device_memory_limit
+    set_device_memory_limit(5, 123456)
+    used, limit = device_memory_usage(5)
+    assert limit == 123456 and used == 0
+    set_device_memory_limit(5, 0)
+    assert device_memory_usage(5) == (0, 0)
+    with pytest.raises(RuntimeError):
+        set_device_memory_limit(64, 1)
+    with pytest.raises(RuntimeError):
+        set_device_memory_limit(-1, 1)
