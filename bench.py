@@ -17,11 +17,13 @@ Printed JSON line:
                 (32 B ray + 16 B hit + 80 B per wide node visited + 36 B per
                 triangle tested, visits counted by a counting pass) over its
                 CUDA-event time, against the measured HBM copy bandwidth;
-  cpu_baseline- the CPU oracle on the host cores on a centre crop.
+  cpu_baseline- the CPU oracle on the host cores over rows spread evenly
+                over the frame (cpu_sample_rows).
 `--impl reference` times the reference's own integrator on the host cores, on
 rank 0 only: its GLSL compiled as C++ (oracle/_ref, built from the reference's
 sources by oracle/ref_build.py) when that library is present, else the
-oracle's restatement; same workload and metric, a centre crop per step.
+oracle's restatement; same workload and metric, the same rows as
+cpu_baseline, a chunk of them per step.
 """
 from __future__ import annotations
 
@@ -106,10 +108,11 @@ def measured_peaks():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def traffic_from_profile():
+def traffic_from_profile(workload):
     """DRAM bytes per extension ray of the closest-hit kernel from the committed
-    ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "extend_kernel_traffic.json")
+    ncu summary of this workload (profiles/extend_kernel_traffic_<workload>.json),
+    or None where no capture of it was made."""
+    path = os.path.join(ROOT, "profiles", f"extend_kernel_traffic_{workload}.json")
     try:
         with open(path) as f:
             return json.load(f)
@@ -202,38 +205,56 @@ def max_over_ranks(value, world):
     return float(t.item())
 
 
+# The CPU sample: rows spread evenly over the frame, full width, at the
+# workload's spp, about 6M spectral paths in all. cpu_baseline and the
+# reference arm time the same rows, so the two CPU rates are comparable with
+# each other and, since the rows cross the whole frame, with a full-frame
+# GPU rate.
+CPU_SAMPLE_PATHS = 6_000_000
+
+
+def cpu_sample_rows(wl):
+    """Row indices of the CPU sample: R rows at y = floor((i + 1/2) H / R)."""
+    per_row = wl.width * wl.spp * 3
+    rows = int(min(wl.height, max(1, round(CPU_SAMPLE_PATHS / per_row))))
+    return [int((i + 0.5) * wl.height / rows) for i in range(rows)]
+
+
+def describe_rows(wl, rows):
+    shown = ", ".join(str(y) for y in rows[:6]) + (", ..." if len(rows) > 6 else "")
+    return (f"{len(rows)} rows spread evenly over the {wl.width}x{wl.height} frame (y = {shown}), full width, "
+            f"at {wl.spp} spp")
+
+
+def render_rows(t, wl, rows, sample_index, threads):
+    for y in rows:
+        t.render(wl.camera, wl.width, wl.height, sample_index, wl.max_bounces, wl.spp, crop=(0, y, wl.width, y + 1),
+                 threads=threads)
+
+
 def cpu_baseline(wl, target_seconds, rank0=True):
-    """The oracle on the host cores over a centre crop, sized to ~target_seconds."""
+    """The oracle on the host cores over the CPU sample (cpu_sample_rows),
+    repeated until about target_seconds have passed."""
     import oracle as O
     O.build()
     t = O.OracleTracer()
     t.set_scene(wl.scene)
     threads = os.cpu_count() or 1
-    cx, cy = wl.width // 2, wl.height // 2
-    side = 16
-    t0 = time.perf_counter()
-    t.render(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp,
-             crop=(cx - side // 2, cy - side // 2, cx + side // 2, cy + side // 2), threads=threads)
-    calib = max(time.perf_counter() - t0, 1e-3)
-    rate = side * side / calib
-    # The small calibration crop underestimates the rate (thread start-up):
-    # a sample that ends well short of the target is sized again from itself.
-    for _attempt in range(2):
-        side = int(max(16, min(wl.width, wl.height, (rate * target_seconds) ** 0.5)))
-        x0, y0 = cx - side // 2, cy - side // 2
+    rows = cpu_sample_rows(wl)
+    passes, secs, rays = 0, 0.0, 0
+    while passes == 0 or secs < target_seconds:
         t0 = time.perf_counter()
-        t.render(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp, crop=(x0, y0, x0 + side, y0 + side),
-                 threads=threads)
-        secs = time.perf_counter() - t0
-        rate = side * side / max(secs, 1e-3)
-        if secs >= 0.5 * target_seconds or side >= min(wl.width, wl.height):
-            break
-    paths = side * side * wl.spp * 3
-    ext, sh, ss = t.last_counters
+        for y in rows:
+            t.render(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp, crop=(0, y, wl.width, y + 1),
+                     threads=threads)
+            rays += sum(t.last_counters)
+        secs += time.perf_counter() - t0
+        passes += 1
+    paths = passes * len(rows) * wl.width * wl.spp * 3
     return {"value": paths / secs, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{side}x{side} centre crop of the {wl.width}x{wl.height} frame at {wl.spp} spp "
-                      f"({paths} spectral paths, {secs:.1f} s)",
-            "rays_per_s": (ext + sh + ss) / secs}
+            "sample": f"{describe_rows(wl, rows)}, {passes} pass(es): {paths} spectral paths in {secs:.1f} s; "
+                      f"the same rows as the reference arm",
+            "rays_per_s": rays / secs}
 
 
 def workload_config(wl, world):
@@ -261,22 +282,25 @@ def run_reference(args):
         t, kind = O.OracleTracer(), "port"
     t.set_scene(wl.scene)
     threads = os.cpu_count() or 1
-    side = 64
-    cx, cy = wl.width // 2, wl.height // 2
-    crop = (cx - side // 2, cy - side // 2, cx + side // 2, cy + side // 2)
+    # Each step renders one chunk of the CPU sample's rows, in turn: every
+    # few consecutive steps cover the sample cpu_baseline times.
+    rows = cpu_sample_rows(wl)
+    chunk = max(1, len(rows) // 4)
+    chunks = [rows[i:i + chunk] for i in range(0, len(rows), chunk)]
     for i in range(args.warmup):
-        t.render(wl.camera, wl.width, wl.height, i * wl.spp, wl.max_bounces, wl.spp, crop=crop, threads=threads)
-    times = []
+        render_rows(t, wl, chunks[i % len(chunks)], i * wl.spp, threads)
+    times, paths = [], 0
     for i in range(args.steps):
+        step_rows = chunks[(args.warmup + i) % len(chunks)]
         t0 = time.perf_counter()
-        t.render(wl.camera, wl.width, wl.height, (args.warmup + i) * wl.spp, wl.max_bounces, wl.spp, crop=crop,
-                 threads=threads)
+        render_rows(t, wl, step_rows, (args.warmup + i) * wl.spp, threads)
         times.append(time.perf_counter() - t0)
-    paths = side * side * wl.spp * 3 * args.steps
+        paths += len(step_rows) * wl.width * wl.spp * 3
     value = paths / sum(times)
-    sample = f"{side}x{side} centre crop of the {wl.width}x{wl.height} frame at {wl.spp} spp per step"
+    sample = (f"{describe_rows(wl, rows)}; each step renders {chunk} of these rows in turn "
+              f"(the rows cpu_baseline times)")
     if kind == "reference":
-        sample += " (the reference's GLSL integrator compiled as C++, ray queries on a CPU BVH)"
+        sample += "; the reference's GLSL integrator compiled as C++, ray queries on a CPU BVH"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / len(times),
@@ -630,12 +654,12 @@ def run_hdcx(args):
     bytes_per_ray = 32 + 16 + 80 * nodes_per_ray + 36 * tris_per_ray
     achieved_gbs = ext_rays * bytes_per_ray / (extend_ms / 1000.0) / 1e9 if extend_ms > 0 else None
     peak, peak_kind = measured_peaks()
-    traffic = traffic_from_profile()
+    traffic = traffic_from_profile(args.workload)
     roofline = {
         "kernel": "extendKernel (closest-hit traversal)",
         "bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
         "frac": (achieved_gbs / peak) if achieved_gbs else None, "peak_source": peak_kind,
-        # ncu DRAM bytes per extension ray (profiles/extend_kernel_traffic.json,
+        # ncu DRAM bytes per extension ray (profiles/extend_kernel_traffic_heavy.json,
         # captured on a smaller frame) times this run's rays per launch.
         "traffic": (traffic["dram_bytes_per_ray"] * ext_rays / extend_launches
                     if traffic and extend_launches else None),
