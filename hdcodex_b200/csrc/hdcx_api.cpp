@@ -201,6 +201,9 @@ ArenaLease checkoutArena(int device, bool wait)
     return ArenaLease{busy, std::unique_lock<std::mutex>(busy->busy)};
 }
 
+// Frames of hdcx_render_async in flight (defined with the render helpers).
+struct AsyncFrames;
+
 }  // namespace
 
 struct hdcx_nrc {
@@ -238,6 +241,14 @@ struct hdcx_tracer {
     // Path state of radiance-cache renders (other renders use the arenas).
     PathStore own;
     DeviceBuffer rgba, xyz, batch, batchXyz;
+    // Device AOVs (hdcx_set_aovs): primary hit and distance of the first
+    // sample of every render, per pixel of the render's size.
+    uint32_t aovFlags = 0;
+    DeviceBuffer aovIds, aovDepth;
+    uint32_t aovWidth = 0, aovHeight = 0;
+    DeviceBuffer preview;  // hdcx_render_preview's upscaled image
+    // Frames of hdcx_render_async in flight (created on first use).
+    AsyncFrames* async = nullptr;
     DeviceBuffer statsBuffer;  // this tracer's ray counters (8 x u64), whichever path buffers it renders with
     FrameBuffers fb;
     uint64_t xyzSamples = 0;
@@ -605,6 +616,10 @@ FrameConst makeFrame(const hdcx_tracer* t, const hdcx_camera& c, uint32_t w, uin
     return f;
 }
 
+// hdcx_render_async's frames (defined with the render helpers below).
+void drainAsync(hdcx_tracer* t);
+void destroyAsync(hdcx_tracer* t);
+
 }  // namespace
 
 extern "C" {
@@ -776,6 +791,7 @@ HDCX_API void hdcx_destroy(hdcx_tracer* t)
     if (!t) return;
     const int device = t->device;
     cudaSetDevice(device);
+    destroyAsync(t);
     delete t;
     // The device's last tracer takes the path arenas with it.
     ArenaPool& pool = arenaPool(device);
@@ -789,6 +805,7 @@ HDCX_API hdcx_status hdcx_set_scene(hdcx_tracer* t, const hdcx_scene_desc* desc)
 {
     if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
     return guarded(t, [&] {
+        drainAsync(t);
         if (!desc) {
             check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
             t->clearScene();
@@ -802,7 +819,10 @@ HDCX_API hdcx_status hdcx_set_scene(hdcx_tracer* t, const hdcx_scene_desc* desc)
 HDCX_API hdcx_status hdcx_set_scene_packed(hdcx_tracer* t, const hdcx_packed_scene* view)
 {
     if (!t || !view) return HDCX_ERROR_INVALID_ARGUMENT;
-    return guarded(t, [&] { uploadScene(t, copyPackedView(*view)); });
+    return guarded(t, [&] {
+        drainAsync(t);
+        uploadScene(t, copyPackedView(*view));
+    });
 }
 
 HDCX_API hdcx_status hdcx_pack_scene(const hdcx_scene_desc* desc, hdcx_packing** out)
@@ -862,6 +882,8 @@ HDCX_API hdcx_status hdcx_set_wave_size(hdcx_tracer* t, uint64_t paths)
 }  // extern "C"
 
 namespace {
+
+void enqueueAovs(hdcx_tracer* t, const FrameConst& frame);
 
 // One render in three phases. prepare: output and path buffers, the fallback
 // axis, counters cleared (may allocate and synchronise the tracer's stream).
@@ -931,6 +953,7 @@ void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut, bool timeEv
     if (timeEvents) check(cudaEventRecord(t->start, t->stream), "cudaEventRecord");
     renderFrame(t->scene, call.frame, call.paths, t->fb, t->stream, call.stageTiming ? &call.times : nullptr,
                 call.counting, &call.launches, t->radianceCache ? &t->cacheRun : nullptr);
+    enqueueAovs(t, call.frame);
     if (timeEvents) check(cudaEventRecord(t->stop, t->stream), "cudaEventRecord");
     if (pathsDone) check(cudaEventRecord(pathsDone, t->stream), "cudaEventRecord");
     if (rgbaOut) {
@@ -982,6 +1005,194 @@ void finishRender(hdcx_tracer* t, RenderCall& call, float graphMs = -1.0F)
     t->stats.shadow_triangle_tests = counters[6];
 }
 
+// Device AOVs of a render: the primary hit of the call's first sample (the
+// hdcx_trace_primary result for sample `sampleIndex`), when hdcx_set_aovs
+// enabled them.
+void enqueueAovs(hdcx_tracer* t, const FrameConst& frame)
+{
+    if (t->aovFlags == 0u) return;
+    const size_t pixels = size_t(frame.width) * frame.height;
+    if (t->aovWidth != frame.width || t->aovHeight != frame.height || !t->aovIds.ptr) {
+        check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+        t->aovIds.allocate(pixels * sizeof(uint32_t));
+        t->aovDepth.allocate(pixels * sizeof(float));
+        t->aovWidth = frame.width;
+        t->aovHeight = frame.height;
+    }
+    tracePrimary(t->scene, frame, frame.sampleIndex, t->aovIds.as<uint32_t>(), t->aovDepth.as<float>(), t->stream);
+}
+
+// ---------------------------------------------------------------------------
+// hdcx_render_async: two frames in flight per tracer. A frame renders on the
+// tracer's stream, copies its running mean and counters to device staging
+// there (so the next frame may overwrite the accumulation), and a second
+// stream copies the staging to pinned host memory while the next frame
+// renders. Frames complete in ticket order.
+// ---------------------------------------------------------------------------
+struct AsyncSlot {
+    uint64_t ticket = 0;
+    bool pending = false;  // enqueued, not yet completed
+    bool held = false;     // completed; its host image is valid
+    int32_t written = 0;
+    ArenaLease lease;
+    RenderCall call;
+    DeviceBuffer staging, stats;
+    float* host = nullptr;  // pinned
+    size_t hostBytes = 0;
+    unsigned long long* hostStats = nullptr;  // pinned, 8 counters
+    cudaEvent_t start = nullptr, stop = nullptr, staged = nullptr, copied = nullptr;
+};
+
+struct AsyncFrames {
+    cudaStream_t copyStream = nullptr;
+    AsyncSlot slot[2];
+    uint64_t next = 0;
+    ~AsyncFrames()
+    {
+        if (copyStream) cudaStreamSynchronize(copyStream);
+        for (AsyncSlot& s : slot) {
+            if (s.host) cudaFreeHost(s.host);
+            if (s.hostStats) cudaFreeHost(s.hostStats);
+            for (cudaEvent_t e : {s.start, s.stop, s.staged, s.copied})
+                if (e) cudaEventDestroy(e);
+        }
+        if (copyStream) cudaStreamDestroy(copyStream);
+    }
+};
+
+AsyncFrames& asyncFrames(hdcx_tracer* t)
+{
+    if (!t->async) {
+        auto a = std::make_unique<AsyncFrames>();
+        check(cudaStreamCreateWithFlags(&a->copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (AsyncSlot& s : a->slot) {
+            check(cudaEventCreate(&s.start), "cudaEventCreate");
+            check(cudaEventCreate(&s.stop), "cudaEventCreate");
+            check(cudaEventCreateWithFlags(&s.staged, cudaEventDisableTiming), "cudaEventCreate");
+            check(cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming), "cudaEventCreate");
+            check(cudaHostAlloc(reinterpret_cast<void**>(&s.hostStats), 8 * sizeof(unsigned long long),
+                                cudaHostAllocDefault),
+                  "cudaHostAlloc");
+        }
+        t->async = a.release();
+    }
+    return *t->async;
+}
+
+// Waits for a pending frame and takes its counters and device time into the
+// tracer's stats, as finishRender does for hdcx_render.
+void completeAsync(hdcx_tracer* t, AsyncSlot& s)
+{
+    if (!s.pending) return;
+    s.pending = false;
+    s.held = true;
+    if (!s.written) return;
+    const cudaError_t e = cudaEventSynchronize(s.copied);
+    s.lease = ArenaLease{};
+    check(e, "hdcx_render_async frame");
+    t->xyzSamples = (s.call.frame.sampleIndex == 0 ? 0 : t->xyzSamples) + s.call.frame.sampleCount;
+    float ms = 0.0F;
+    check(cudaEventElapsedTime(&ms, s.start, s.stop), "cudaEventElapsedTime");
+    const unsigned long long* c = s.hostStats;
+    t->stats = hdcx_render_stats{};
+    t->stats.spectral_paths = s.call.pathsNeeded;
+    t->stats.extension_rays = c[0];
+    t->stats.shadow_rays = c[1];
+    t->stats.subsurface_rays = c[2];
+    t->stats.render_ms = ms;
+    t->stats.kernel_launches = s.call.launches;
+    t->stats.extension_node_visits = c[3];
+    t->stats.extension_triangle_tests = c[4];
+    t->stats.shadow_node_visits = c[5];
+    t->stats.shadow_triangle_tests = c[6];
+    throwOnTraversalFault(c[7]);
+}
+
+// Completes every pending frame with a ticket up to `last`, oldest first.
+void completeAsyncUpTo(hdcx_tracer* t, uint64_t last)
+{
+    if (!t->async) return;
+    for (;;) {
+        AsyncSlot* oldest = nullptr;
+        for (AsyncSlot& s : t->async->slot)
+            if (s.pending && s.ticket <= last && (!oldest || s.ticket < oldest->ticket)) oldest = &s;
+        if (!oldest) return;
+        completeAsync(t, *oldest);
+    }
+}
+
+void drainAsync(hdcx_tracer* t) { completeAsyncUpTo(t, ~0ull); }
+
+void destroyAsync(hdcx_tracer* t)
+{
+    if (!t->async) return;
+    try {
+        drainAsync(t);
+    } catch (const std::exception&) {
+    }
+    delete t->async;
+    t->async = nullptr;
+}
+
+void enqueueAsync(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, uint32_t height, uint32_t sampleIndex,
+                  uint32_t maxBounces, uint32_t sampleCount, uint64_t* ticket)
+{
+    AsyncFrames& a = asyncFrames(t);
+    AsyncSlot& s = a.slot[a.next % 2u];
+    // The slot's previous frame (two tickets back) completes, and its host
+    // image is given up, before this frame takes the slot.
+    completeAsyncUpTo(t, s.ticket);
+    s.held = false;
+    s.written = 0;
+    s.ticket = a.next++;
+    s.call = RenderCall{};
+    if (t->geometryReady && width > 0 && height > 0) {
+        ArenaLease lease;
+        if (!t->radianceCache) lease = checkoutArena(t->device, true);
+        prepareRender(t, camera, width, height, sampleIndex, maxBounces, sampleCount, 0, false, s.call, lease.arena);
+        const size_t bytes = size_t(width) * height * sizeof(float4);
+        if (s.hostBytes < bytes) {
+            if (s.host) check(cudaFreeHost(s.host), "cudaFreeHost");
+            s.host = nullptr;
+            s.hostBytes = 0;
+            check(cudaHostAlloc(reinterpret_cast<void**>(&s.host), bytes, cudaHostAllocDefault), "cudaHostAlloc");
+            s.hostBytes = bytes;
+        }
+        if (s.staging.bytes < bytes) s.staging.allocate(bytes);
+        if (!s.stats.ptr) s.stats.allocate(8 * sizeof(unsigned long long));
+        check(cudaEventRecord(s.start, t->stream), "cudaEventRecord");
+        enqueueRender(t, s.call, nullptr, false);
+        check(cudaEventRecord(s.stop, t->stream), "cudaEventRecord");
+        check(cudaMemcpyAsync(s.staging.ptr, t->fb.rgba, bytes, cudaMemcpyDeviceToDevice, t->stream), "stage frame");
+        check(cudaMemcpyAsync(s.stats.ptr, s.call.paths.stats, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                              t->stream),
+              "stage counters");
+        check(cudaEventRecord(s.staged, t->stream), "cudaEventRecord");
+        check(cudaStreamWaitEvent(a.copyStream, s.staged, 0), "cudaStreamWaitEvent");
+        check(cudaMemcpyAsync(s.host, s.staging.ptr, bytes, cudaMemcpyDeviceToHost, a.copyStream), "read back frame");
+        check(cudaMemcpyAsync(s.hostStats, s.stats.ptr, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                              a.copyStream),
+              "read back counters");
+        check(cudaEventRecord(s.copied, a.copyStream), "cudaEventRecord");
+        s.lease = std::move(lease);
+        s.written = 1;
+    }
+    s.pending = true;
+    *ticket = s.ticket;
+}
+
+// Nearest-neighbour upscale of the interactive preview: the reference's
+// UpscaleNearest (render_pass.cpp:45-68) on the device.
+void upscalePreview(hdcx_tracer* t, uint32_t traceWidth, uint32_t traceHeight, uint32_t width, uint32_t height)
+{
+    const size_t bytes = size_t(width) * height * sizeof(float4);
+    if (t->preview.bytes < bytes) {
+        check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+        t->preview.allocate(bytes);
+    }
+    launchUpscaleNearest(t->fb.rgba, traceWidth, traceHeight, t->preview.as<float4>(), width, height, t->stream);
+}
+
 }  // namespace
 
 extern "C" {
@@ -995,6 +1206,7 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint
     if (!t->geometryReady || width == 0 || height == 0) return HDCX_OK;
     if (uint64_t(width) * height > (1ull << 28)) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels");
     return guarded(t, [&] {
+        drainAsync(t);
         // The arena stays checked out until the render's work has finished.
         ArenaLease lease;
         if (!t->radianceCache) lease = checkoutArena(t->device, true);
@@ -1003,6 +1215,95 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint
         enqueueRender(t, call, rgbaOut);
         finishRender(t, call);
         if (written) *written = 1;
+    });
+}
+
+HDCX_API hdcx_status hdcx_render_preview(hdcx_tracer* t, const hdcx_camera* camera, uint32_t width, uint32_t height,
+                                         float* rgbaOut, int32_t* written)
+{
+    if (!t || !camera) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (written) *written = 0;
+    if (!t->geometryReady || width == 0 || height == 0) return HDCX_OK;
+    if (uint64_t(width) * height > (1ull << 28)) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels");
+    // render_pass.cpp:191-208: half resolution (rounded up), sample 0, two
+    // bounces, one sample, upscaled by nearest neighbour.
+    constexpr uint32_t kScale = 2u, kBounces = 2u;
+    const uint32_t traceWidth = std::max(1u, (width + kScale - 1u) / kScale);
+    const uint32_t traceHeight = std::max(1u, (height + kScale - 1u) / kScale);
+    return guarded(t, [&] {
+        drainAsync(t);
+        ArenaLease lease;
+        if (!t->radianceCache) lease = checkoutArena(t->device, true);
+        RenderCall call;
+        prepareRender(t, *camera, traceWidth, traceHeight, 0u, kBounces, 1u, 0, true, call, lease.arena);
+        enqueueRender(t, call, nullptr);
+        upscalePreview(t, traceWidth, traceHeight, width, height);
+        if (rgbaOut) {
+            check(cudaMemcpyAsync(rgbaOut, t->preview.ptr, size_t(width) * height * sizeof(float4), cudaMemcpyDefault,
+                                  t->stream),
+                  "read back preview");
+        }
+        finishRender(t, call);
+        if (written) *written = 1;
+    });
+}
+
+HDCX_API hdcx_status hdcx_device_preview(hdcx_tracer* t, const float** device)
+{
+    if (!t || !device) return HDCX_ERROR_INVALID_ARGUMENT;
+    *device = t->preview.as<float>();
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_render_async(hdcx_tracer* t, const hdcx_camera* camera, uint32_t width, uint32_t height,
+                                       uint32_t sampleIndex, uint32_t maxBounces, uint32_t sampleCount, uint64_t* ticket)
+{
+    if (!t || !camera || !ticket) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (uint64_t(width) * height > (1ull << 28)) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels");
+    return guarded(t, [&] { enqueueAsync(t, *camera, width, height, sampleIndex, maxBounces, sampleCount, ticket); });
+}
+
+HDCX_API hdcx_status hdcx_wait_render(hdcx_tracer* t, uint64_t ticket, const float** hostRgba, int32_t* written)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (hostRgba) *hostRgba = nullptr;
+    if (written) *written = 0;
+    AsyncSlot* slot = nullptr;
+    if (t->async) {
+        for (AsyncSlot& s : t->async->slot)
+            if ((s.pending || s.held) && s.ticket == ticket) slot = &s;
+    }
+    if (!slot) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_wait_render: the ticket is not held (a frame's image is "
+                                                          "kept until the call two tickets later)");
+    return guarded(t, [&] {
+        completeAsyncUpTo(t, ticket);
+        if (hostRgba && slot->written) *hostRgba = slot->host;
+        if (written) *written = slot->written;
+    });
+}
+
+HDCX_API hdcx_status hdcx_set_aovs(hdcx_tracer* t, uint32_t flags)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if ((flags & ~(HDCX_AOV_PRIMITIVE_ID | HDCX_AOV_DEPTH)) != 0u)
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_set_aovs: unknown AOV flags");
+    t->aovFlags = flags;
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_read_aovs(hdcx_tracer* t, uint32_t* primitiveOut, float* depthOut, uint64_t pixelCount)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    return guarded(t, [&] {
+        drainAsync(t);
+        const uint64_t n = uint64_t(t->aovWidth) * t->aovHeight;
+        if (n == 0 || !t->aovIds.ptr) throw std::invalid_argument("hdcx_read_aovs: no render has written AOVs");
+        if (pixelCount < n) throw std::invalid_argument("hdcx_read_aovs: output smaller than width*height");
+        if (primitiveOut)
+            check(cudaMemcpyAsync(primitiveOut, t->aovIds.ptr, n * sizeof(uint32_t), cudaMemcpyDefault, t->stream), "read ids");
+        if (depthOut)
+            check(cudaMemcpyAsync(depthOut, t->aovDepth.ptr, n * sizeof(float), cudaMemcpyDefault, t->stream), "read depth");
+        check(cudaStreamSynchronize(t->stream), "read AOVs");
     });
 }
 
@@ -1258,6 +1559,13 @@ HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, 
             }
         }
     }
+    for (uint32_t j = 0; j < count; ++j) {
+        hdcx_tracer* t = jobs[j].tracer;
+        if (t->async) {
+            const hdcx_status drained = guarded(t, [&] { drainAsync(t); });
+            if (drained != HDCX_OK) return drained;
+        }
+    }
     std::vector<RenderCall> calls(count);
     auto record = [&](uint32_t j, hdcx_status status) {
         if (status != HDCX_OK) {
@@ -1328,6 +1636,10 @@ HDCX_API hdcx_status hdcx_render_static(hdcx_tracer* t, const hdcx_camera* camer
 {
     if (!t || !camera || !rgbaDevice) return HDCX_ERROR_INVALID_ARGUMENT;
     if (written) *written = 0;
+    if (t->async) {
+        const hdcx_status drained = guarded(t, [&] { drainAsync(t); });
+        if (drained != HDCX_OK) return drained;
+    }
     if (!t->geometryReady || width == 0 || height == 0) return HDCX_OK;
     if (uint64_t(width) * height > kStaticMaxPixels) {
         return fail(t, HDCX_ERROR_INVALID_ARGUMENT,

@@ -1566,6 +1566,28 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
     }
 }
 
+__global__ void upscaleNearestKernel(const float4* src, uint32_t srcWidth, uint32_t srcHeight, float4* dst,
+                                     uint32_t width, uint32_t height)
+{
+    const uint64_t pixel = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (pixel >= uint64_t(width) * height) return;
+    const uint32_t x = static_cast<uint32_t>(pixel % width), y = static_cast<uint32_t>(pixel / width);
+    // render_pass.cpp:55-60: source = min(size - 1, destination * size / destinationSize).
+    const uint32_t sy = static_cast<uint32_t>(min(uint64_t(srcHeight - 1u), uint64_t(y) * srcHeight / height));
+    const uint32_t sx = static_cast<uint32_t>(min(uint64_t(srcWidth - 1u), uint64_t(x) * srcWidth / width));
+    dst[pixel] = src[uint64_t(sy) * srcWidth + sx];
+}
+
+void launchUpscaleNearest(const float4* src, uint32_t srcWidth, uint32_t srcHeight, float4* dst, uint32_t width,
+                          uint32_t height, cudaStream_t stream)
+{
+    const uint64_t pixels = uint64_t(width) * height;
+    if (pixels == 0 || srcWidth == 0 || srcHeight == 0) return;
+    upscaleNearestKernel<<<static_cast<unsigned>((pixels + 255u) / 256u), 256, 0, stream>>>(src, srcWidth, srcHeight, dst,
+                                                                                          width, height);
+    CUDA_OK(cudaGetLastError());
+}
+
 void tracePrimary(const DeviceScene& scene, const FrameConst& frame, uint32_t sampleNumber, uint32_t* primitives,
                   float* distances, cudaStream_t stream)
 {

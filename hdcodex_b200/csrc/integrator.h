@@ -128,6 +128,11 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
                  cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches,
                  CacheRun* cacheRun = nullptr);
 
+// dst (width x height) = src (srcWidth x srcHeight) upscaled by nearest
+// neighbour: the reference's UpscaleNearest (render_pass.cpp:45-68).
+void launchUpscaleNearest(const float4* src, uint32_t srcWidth, uint32_t srcHeight, float4* dst, uint32_t width,
+                          uint32_t height, cudaStream_t stream);
+
 // Primary-hit ids and distances of sample `sampleNumber` (device outputs).
 void tracePrimary(const DeviceScene& scene, const FrameConst& frame, uint32_t sampleNumber, uint32_t* primitives,
                   float* distances, cudaStream_t stream);

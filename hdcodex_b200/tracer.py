@@ -88,6 +88,14 @@ SIGNATURES = {
     "hdcx_set_device_memory_limit": (C.c_int, [C.c_int32, C.c_uint64]),
     "hdcx_get_device_memory_usage": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hdcx_test_break_bvh": (C.c_int, [_P]),
+    "hdcx_render_preview": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_void_p,
+                                      C.POINTER(C.c_int32)]),
+    "hdcx_device_preview": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
+    "hdcx_render_async": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.c_uint32, C.POINTER(C.c_uint64)]),
+    "hdcx_wait_render": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_void_p), C.POINTER(C.c_int32)]),
+    "hdcx_set_aovs": (C.c_int, [_P, C.c_uint32]),
+    "hdcx_read_aovs": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_float), C.c_uint64]),
 }
 
 PROFILE_STAGE_TIMES = 1
@@ -217,6 +225,44 @@ class PathTracer:
         if written.value:
             self.width, self.height = width, height
         return bool(written.value)
+
+    def render_preview(self, camera, width, height):
+        """hdcx_render_preview: the half-resolution two-bounce preview,
+        upscaled to width x height on the device; returns the image."""
+        out = np.empty((height, width, 4), dtype=np.float32)
+        written = C.c_int32(0)
+        self._check(lib().hdcx_render_preview(self._h, C.byref(camera), width, height,
+                                              out.ctypes.data_as(C.c_void_p), C.byref(written)), "render_preview")
+        return out if written.value else None
+
+    def render_async(self, camera, width, height, sample_index, max_bounces=8, sample_count=1) -> int:
+        """hdcx_render_async: enqueues a render and its read-back; returns its ticket."""
+        ticket = C.c_uint64(0)
+        self._check(lib().hdcx_render_async(self._h, C.byref(camera), width, height, sample_index, max_bounces,
+                                            sample_count, C.byref(ticket)), "render_async")
+        return int(ticket.value)
+
+    def wait_render(self, ticket, width, height):
+        """hdcx_wait_render: a copy of the frame's image (None if it wrote nothing)."""
+        ptr = C.c_void_p()
+        written = C.c_int32(0)
+        self._check(lib().hdcx_wait_render(self._h, ticket, C.byref(ptr), C.byref(written)), "wait_render")
+        if not written.value:
+            return None
+        buf = (C.c_float * (width * height * 4)).from_address(ptr.value)
+        return np.frombuffer(buf, dtype=np.float32).reshape(height, width, 4).copy()
+
+    def set_aovs(self, flags=3):
+        """hdcx_set_aovs: 1 | 2 enables the primary-hit id and depth AOVs, 0 disables them."""
+        self._check(lib().hdcx_set_aovs(self._h, flags), "set_aovs")
+
+    def read_aovs(self, width, height):
+        """hdcx_read_aovs: (primitive ids uint32 [h, w], depth float32 [h, w])."""
+        ids = np.empty((height, width), dtype=np.uint32)
+        depth = np.empty((height, width), dtype=np.float32)
+        self._check(lib().hdcx_read_aovs(self._h, ids.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                         depth.ctypes.data_as(C.POINTER(C.c_float)), width * height), "read_aovs")
+        return ids, depth
 
     def read_xyz(self):
         """(xyz_sum (h, w, 3) float64, samples): FP64 CIE XYZ sums of the accumulation."""

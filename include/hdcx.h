@@ -442,6 +442,64 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* tracer, const hdcx_camera* camera,
                                  uint32_t sample_count, float* rgba_out,
                                  int32_t* written);
 
+/* The interactive preview of HdCodexRenderPass::_Execute (render_pass.cpp:
+ * 191-208) on the device: renders at half resolution (ceil(width/2) x
+ * ceil(height/2)) from sample 0 with two bounces and one sample per pixel,
+ * exactly as hdcx_render would (the running mean restarts at that size), then
+ * upscales the image to width x height by nearest neighbour on the GPU, with
+ * the reference's UpscaleNearest rule (render_pass.cpp:45-68: source pixel =
+ * min(size - 1, destination * size / destination size)), where the reference
+ * upscales on the CPU. When rgba_out is not NULL the upscaled RGBA32F image
+ * (width*height*4 floats; host or device memory) is copied into it; it also
+ * stays on the device (hdcx_device_preview). *written as hdcx_render. */
+HDCX_API hdcx_status hdcx_render_preview(hdcx_tracer* tracer, const hdcx_camera* camera,
+                                         uint32_t width, uint32_t height, float* rgba_out,
+                                         int32_t* written);
+/* Device pointer of the last upscaled preview (valid until the next preview
+ * of a larger size, or destroy). */
+HDCX_API hdcx_status hdcx_device_preview(hdcx_tracer* tracer, const float** device_rgba);
+
+/* hdcx_render without waiting: where the reference blocks on a fence and then
+ * copies the whole image (vulkan_path_tracer.cpp:3287-3305), this enqueues the
+ * render and the read-back of its running mean and returns a ticket at once.
+ * The render runs on the tracer's stream; the image is copied to device
+ * staging there, and from it to a pinned host buffer of the tracer on a
+ * second stream, so the copy of frame n overlaps the rendering of frame n+1.
+ * Two frames may be in flight: a call whose slot still holds the frame two
+ * tickets back completes that frame first (and gives up its image). Frames
+ * complete in ticket order. Same images, counters and running-mean rules as
+ * hdcx_render; hdcx_render, hdcx_render_preview, hdcx_render_static,
+ * hdcx_render_batch, hdcx_read_aovs and hdcx_set_scene complete pending frames
+ * first. A frame with no geometry or a zero size writes nothing. */
+HDCX_API hdcx_status hdcx_render_async(hdcx_tracer* tracer, const hdcx_camera* camera,
+                                       uint32_t width, uint32_t height,
+                                       uint32_t sample_index, uint32_t max_bounces,
+                                       uint32_t sample_count, uint64_t* ticket);
+/* Waits for the frame `ticket` (and every earlier pending frame) and gives
+ * its image: *host_rgba points at width*height*4 floats in pinned host memory
+ * owned by the tracer, valid until the hdcx_render_async call two tickets
+ * later (or destroy); *written = 0 and *host_rgba = NULL for a frame that
+ * wrote nothing. hdcx_get_stats then describes the frame. A ticket no longer
+ * held gives HDCX_ERROR_INVALID_ARGUMENT. */
+HDCX_API hdcx_status hdcx_wait_render(hdcx_tracer* tracer, uint64_t ticket, const float** host_rgba,
+                                      int32_t* written);
+
+/* Device AOVs written by every render (hdcx_render, _async, _batch,
+ * _preview's half-resolution render) once enabled: per pixel of the render,
+ * the flattened primitive index of the closest accepted primary hit
+ * (0xffffffff: miss) and its distance along the normalised camera ray (0 on a
+ * miss), for the render's first sample sample_index: the hdcx_trace_primary
+ * result for that sample, without a separate call. No counterpart in the
+ * reference, whose render buffer holds colour only (render_buffer.cpp:114-129).
+ * Either flag enables both; 0 disables them. */
+#define HDCX_AOV_PRIMITIVE_ID 1u
+#define HDCX_AOV_DEPTH 2u
+HDCX_API hdcx_status hdcx_set_aovs(hdcx_tracer* tracer, uint32_t flags);
+/* Copies the last render's AOVs (pixel_count >= width*height; host or device
+ * destinations; either may be NULL). */
+HDCX_API hdcx_status hdcx_read_aovs(hdcx_tracer* tracer, uint32_t* primitive_out, float* depth_out,
+                                    uint64_t pixel_count);
+
 /* hdcx_render for callers that cannot allocate device memory. No counterpart
  * in the reference: VulkanPathTracer has no entry point of this kind.
  *
