@@ -977,7 +977,7 @@ void throwOnTraversalFault(unsigned long long word)
     throw StatusError(HDCX_ERROR_INTERNAL, what);
 }
 
-// `graphMs` >= 0: the render ran inside a batch graph, whose device time it reports.
+// `graphMs` >= 0: the render ran inside a batch graph, which measured its device time.
 void finishRender(hdcx_tracer* t, RenderCall& call, float graphMs = -1.0F)
 {
     check(cudaStreamSynchronize(t->stream), "render");
@@ -1435,15 +1435,39 @@ struct BatchEvents {
     }
 };
 
+// The batch graph of a device, kept between calls: the executable graph of
+// the last batch (updated in place with cudaGraphExecUpdate when the next
+// batch has the same launch topology, instantiated anew otherwise), the
+// capture stream and the events the graph records. One batch at a time per
+// device uses it.
+struct BatchGraphCache {
+    std::mutex lock;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, start = nullptr, stop = nullptr;
+    std::vector<cudaEvent_t> jobStart, jobStop;  // timing events per job slot
+    uint64_t instantiations = 0, updates = 0;
+};
+
+BatchGraphCache& batchGraphCache(int device)
+{
+    static BatchGraphCache* caches = new BatchGraphCache[kArenaDevices];  // never destroyed, like the arenas
+    return caches[device];
+}
+
 // Captures the kernels of every active job (each on its own tracer's stream,
-// forked from and joined into one capture stream) into a single CUDA graph,
-// launches it once, then queues the read-backs. Returns the graph's device
-// time, or a negative value (nothing launched) when the batch cannot be
-// captured: jobs on several devices, a job in radiance-cache mode (it
-// synchronises with the host per wave) or a capture error. A launch,
+// forked from and joined into one capture stream) into a CUDA graph, brings
+// the device's cached executable graph up to date with it (or instantiates
+// one), launches it, then queues the read-backs. Returns the graph's device
+// time and, in jobMs, each job's device time from its first to its last
+// kernel (events recorded inside the graph; jobs overlap, so these do not add
+// up to the graph's time); a negative value (nothing launched) when the batch
+// cannot be captured: jobs on several devices, a job in radiance-cache mode
+// (it synchronises with the host per wave) or a capture error. A launch,
 // synchronisation or read-back error after instantiation sets the affected
 // jobs' status to HDCX_ERROR_CUDA and takes them out of the batch.
-float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<RenderCall>& calls, const BatchPlan& plan)
+float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<RenderCall>& calls, const BatchPlan& plan,
+                        std::vector<float>& jobMs)
 {
     int device = -1;
     for (uint32_t j = 0; j < count; ++j) {
@@ -1452,77 +1476,97 @@ float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<Render
         if (t->radianceCache || (device >= 0 && t->device != device)) return -1.0F;
         device = t->device;
     }
-    if (device < 0 || cudaSetDevice(device) != cudaSuccess) return -1.0F;
+    if (device < 0 || device >= kArenaDevices || cudaSetDevice(device) != cudaSuccess) return -1.0F;
     // The prepare phase queued clears on the tracers' streams; the graph runs
     // on its own stream, so they must have finished.
     for (uint32_t j = 0; j < count; ++j) {
         if (calls[j].active && cudaStreamSynchronize(jobs[j].tracer->stream) != cudaSuccess) return -1.0F;
     }
-    cudaStream_t batch = nullptr;
-    cudaEvent_t fork = nullptr, start = nullptr, stop = nullptr;
-    std::vector<cudaEvent_t> joins;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    float ms = -1.0F;
-    auto cleanup = [&] {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        for (cudaEvent_t e : joins) cudaEventDestroy(e);
-        if (fork) cudaEventDestroy(fork);
-        if (start) cudaEventDestroy(start);
-        if (stop) cudaEventDestroy(stop);
-        if (batch) cudaStreamDestroy(batch);
-    };
-    if (cudaStreamCreateWithFlags(&batch, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess || cudaEventCreate(&start) != cudaSuccess ||
-        cudaEventCreate(&stop) != cudaSuccess) {
-        cleanup();
-        return -1.0F;
+    BatchGraphCache& cache = batchGraphCache(device);
+    std::lock_guard<std::mutex> hold(cache.lock);
+    if (!cache.stream) {
+        if (cudaStreamCreateWithFlags(&cache.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&cache.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&cache.start) != cudaSuccess || cudaEventCreate(&cache.stop) != cudaSuccess) {
+            cudaGetLastError();
+            return -1.0F;
+        }
     }
-    bool captured = cudaStreamBeginCapture(batch, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+    while (cache.jobStart.size() < count) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+            if (a) cudaEventDestroy(a);
+            cudaGetLastError();
+            return -1.0F;
+        }
+        cache.jobStart.push_back(a);
+        cache.jobStop.push_back(b);
+    }
+    bool captured = cudaStreamBeginCapture(cache.stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
     try {
         if (captured) {
-            check(cudaEventRecord(fork, batch), "fork");
-            // A job starts after the fork, or after the previous job of its lane.
-            std::vector<cudaEvent_t> laneDone(plan.leases.size(), nullptr);
+            check(cudaEventRecord(cache.fork, cache.stream), "fork");
+            // A job starts after the fork, or after the previous job of its
+            // lane (its stop event, recorded after its last kernel).
+            std::vector<int> laneLast(plan.leases.size(), -1);
             for (uint32_t j : plan.order) {
                 if (!calls[j].active) continue;
                 hdcx_tracer* t = jobs[j].tracer;
                 const int lane = plan.lane[j];
-                check(cudaStreamWaitEvent(t->stream, lane >= 0 && laneDone[lane] ? laneDone[lane] : fork, 0),
+                const bool afterLane = lane >= 0 && laneLast[lane] >= 0;
+                check(cudaStreamWaitEvent(t->stream, afterLane ? cache.jobStop[laneLast[lane]] : cache.fork, 0),
                       "join the capture");
+                check(cudaEventRecord(cache.jobStart[j], t->stream), "job start");
                 enqueueRender(t, calls[j], nullptr, false);
-                cudaEvent_t join = nullptr;
-                check(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), "cudaEventCreate");
-                joins.push_back(join);
-                check(cudaEventRecord(join, t->stream), "join");
-                check(cudaStreamWaitEvent(batch, join, 0), "join");
-                if (lane >= 0) laneDone[lane] = join;
+                check(cudaEventRecord(cache.jobStop[j], t->stream), "job stop");
+                check(cudaStreamWaitEvent(cache.stream, cache.jobStop[j], 0), "join");
+                if (lane >= 0) laneLast[lane] = static_cast<int>(j);
             }
         }
     } catch (const std::exception&) {
         captured = false;
     }
-    cudaGraph_t capturedGraph = nullptr;
-    const cudaError_t end = cudaStreamEndCapture(batch, &capturedGraph);
-    graph = capturedGraph;
-    if (!captured || end != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+    cudaGraph_t graph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(cache.stream, &graph);
+    bool ready = captured && end == cudaSuccess && graph != nullptr;
+    if (ready && cache.exec) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(cache.exec, graph, &info) == cudaSuccess) {
+            cache.updates++;
+        } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(cache.exec);
+            cache.exec = nullptr;
+        }
+    }
+    if (ready && !cache.exec) {
+        if (cudaGraphInstantiate(&cache.exec, graph, 0) == cudaSuccess) {
+            cache.instantiations++;
+        } else {
+            cache.exec = nullptr;
+            ready = false;
+        }
+    }
+    if (graph) cudaGraphDestroy(graph);
+    if (!ready) {
         cudaGetLastError();
-        cleanup();
         return -1.0F;
     }
-    // Once the graph is instantiated the jobs' work is committed to it: a
-    // failure from here on fails every job of the graph (its images are not
-    // valid), and is not retried on the streams.
-    cudaError_t err = cudaEventRecord(start, batch);
-    if (err == cudaSuccess) err = cudaGraphLaunch(exec, batch);
-    if (err == cudaSuccess) err = cudaEventRecord(stop, batch);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(batch);
-    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, start, stop);
+    // Once the graph is launched the jobs' work is committed to it: a failure
+    // from here on fails every job of the graph (its images are not valid),
+    // and is not retried on the streams.
+    float ms = -1.0F;
+    cudaError_t err = cudaEventRecord(cache.start, cache.stream);
+    if (err == cudaSuccess) err = cudaGraphLaunch(cache.exec, cache.stream);
+    if (err == cudaSuccess) err = cudaEventRecord(cache.stop, cache.stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(cache.stream);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, cache.start, cache.stop);
+    jobMs.assign(count, 0.0F);
     for (uint32_t j = 0; j < count; ++j) {
         if (!calls[j].active) continue;
         hdcx_tracer* t = jobs[j].tracer;
         cudaError_t jobErr = err;
+        if (jobErr == cudaSuccess) jobErr = cudaEventElapsedTime(&jobMs[j], cache.jobStart[j], cache.jobStop[j]);
         if (jobErr == cudaSuccess && jobs[j].rgba_out) {
             jobErr = cudaMemcpyAsync(jobs[j].rgba_out, t->fb.rgba,
                                      size_t(calls[j].frame.width) * calls[j].frame.height * sizeof(float4),
@@ -1535,13 +1579,22 @@ float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<Render
         }
     }
     if (err != cudaSuccess) cudaGetLastError();
-    cleanup();
     return ms < 0.0F ? 0.0F : ms;
 }
 
 }  // namespace
 
 extern "C" {
+
+HDCX_API hdcx_status hdcx_get_batch_graph_stats(int32_t device, uint64_t* instantiations, uint64_t* updates)
+{
+    if (device < 0 || device >= kArenaDevices) return HDCX_ERROR_INVALID_ARGUMENT;
+    BatchGraphCache& cache = batchGraphCache(device);
+    std::lock_guard<std::mutex> hold(cache.lock);
+    if (instantiations) *instantiations = cache.instantiations;
+    if (updates) *updates = cache.updates;
+    return HDCX_OK;
+}
 
 HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, uint64_t pathBudget, uint32_t flags)
 {
@@ -1590,7 +1643,8 @@ HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, 
         }));
     }
     BatchEvents events(count);
-    const float graphMs = (flags & HDCX_BATCH_CUDA_GRAPH) ? enqueueBatchGraph(jobs, count, calls, plan) : -1.0F;
+    std::vector<float> jobMs;
+    const float graphMs = (flags & HDCX_BATCH_CUDA_GRAPH) ? enqueueBatchGraph(jobs, count, calls, plan, jobMs) : -1.0F;
     if (graphMs < 0.0F) {
         // Lane by lane: a job waits until the previous job of its lane no
         // longer uses the lane's path buffers.
@@ -1620,7 +1674,7 @@ HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, 
     for (uint32_t j = 0; j < count; ++j) {
         if (calls[j].active) {
             record(j, guarded(jobs[j].tracer, [&] {
-                finishRender(jobs[j].tracer, calls[j], graphMs);
+                finishRender(jobs[j].tracer, calls[j], graphMs < 0.0F ? -1.0F : jobMs[j]);
                 jobs[j].written = 1;
                 jobs[j].render_ms = jobs[j].tracer->stats.render_ms;
             }));

@@ -88,6 +88,7 @@ SIGNATURES = {
     "hdcx_set_device_memory_limit": (C.c_int, [C.c_int32, C.c_uint64]),
     "hdcx_get_device_memory_usage": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hdcx_test_break_bvh": (C.c_int, [_P]),
+    "hdcx_get_batch_graph_stats": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hdcx_render_preview": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_void_p,
                                       C.POINTER(C.c_int32)]),
     "hdcx_device_preview": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
@@ -135,6 +136,15 @@ def device_memory_usage(device: int):
     if status != 0:
         raise RuntimeError(f"hdcx_get_device_memory_usage failed: {STATUS.get(status, status)}")
     return int(used.value), int(limit.value)
+
+
+def batch_graph_stats(device: int = 0):
+    """(batch graphs instantiated, batch graphs updated in place) on `device`."""
+    inst, upd = C.c_uint64(0), C.c_uint64(0)
+    status = lib().hdcx_get_batch_graph_stats(device, C.byref(inst), C.byref(upd))
+    if status != 0:
+        raise RuntimeError(f"hdcx_get_batch_graph_stats failed: {STATUS.get(status, status)}")
+    return int(inst.value), int(upd.value)
 
 
 def probe_devices():

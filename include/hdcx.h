@@ -562,11 +562,18 @@ HDCX_API hdcx_status hdcx_render_batch(hdcx_batch_job* jobs, uint32_t count, uin
 
 /* hdcx_render_batch with options. HDCX_BATCH_CUDA_GRAPH: the kernels of all
  * jobs (each on its tracer's stream) are captured into one CUDA graph and
- * launched at once; every job's render_ms is then the whole graph's device
- * time. A batch that cannot be captured (jobs on several devices, a job in
- * radiance-cache mode) runs as hdcx_render_batch does. Same images either way. */
+ * launched at once. The device keeps the executable graph between calls: a
+ * batch with the same launch topology as the last one (same jobs, sizes and
+ * wave counts) updates it in place (cudaGraphExecUpdate) instead of
+ * instantiating a new one. Every job's render_ms is then its own device time
+ * from its first to its last kernel inside the graph (jobs overlap, so these
+ * do not add up to the batch's time). A batch that cannot be captured (jobs
+ * on several devices, a job in radiance-cache mode) runs as hdcx_render_batch
+ * does. Same images either way. */
 #define HDCX_BATCH_CUDA_GRAPH 1u
 HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, uint64_t path_budget, uint32_t flags);
+/* Batch graphs of `device` so far: instantiated anew, and updated in place. */
+HDCX_API hdcx_status hdcx_get_batch_graph_stats(int32_t device, uint64_t* instantiations, uint64_t* updates);
 
 /* Copies the current device RGBA32F accumulation (width*height*4 floats). */
 HDCX_API hdcx_status hdcx_read_rgba(hdcx_tracer* tracer, float* rgba_out, uint64_t float_count);

@@ -131,3 +131,38 @@ def test_jobs_sharing_lane_buffers_equal_sequential(graph):
     finally:
         for t in tracers:
             t.close()
+
+
+def test_batch_graph_is_updated_in_place_and_times_jobs():
+    """A second batch with the same launch topology updates the device's cached
+    executable graph (cudaGraphExecUpdate) instead of instantiating a new one;
+    the images still equal one hdcx_render per job, and each job reports its
+    own device time inside the graph (at most the whole batch's time)."""
+    from hdcodex_b200.tracer import batch_graph_stats
+    spec = [(workloads.closed_box(width=w, height=h, spp=spp), w, h, spp)
+            for w, h, spp in [(64, 48, 2), (96, 64, 3), (32, 32, 4)]]
+    tracers = [PathTracer(0) for _ in spec]
+    try:
+        for t, (wl, *_rest) in zip(tracers, spec):
+            t.set_scene(wl.scene)
+        images = [np.zeros((h, w, 4), np.float32) for _, w, h, _ in spec]
+        for call, sample_index in enumerate((0, 7)):
+            before = batch_graph_stats(0)
+            jobs = [(t, wl.camera, w, h, sample_index, 8, spp, img)
+                    for t, (wl, w, h, spp), img in zip(tracers, spec, images)]
+            results = render_batch(jobs, 0, graph=True)
+            after = batch_graph_stats(0)
+            assert all(r["status"] == 0 and r["written"] == 1 for r in results)
+            if call == 1:
+                assert after[1] == before[1] + 1 and after[0] == before[0], (before, after)
+            ms = [r["render_ms"] for r in results]
+            assert all(m > 0 for m in ms)
+        for k, (wl, w, h, spp) in enumerate(spec):
+            with PathTracer(0) as ref:
+                ref.set_scene(wl.scene)
+                ref.render(wl.camera, w, h, 0, 8, spp)
+                expected = ref.render(wl.camera, w, h, 7, 8, spp)
+            assert np.array_equal(images[k], expected), k
+    finally:
+        for t in tracers:
+            t.close()
