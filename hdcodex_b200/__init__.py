@@ -7,12 +7,13 @@ tests and the benchmark: ``PathTracer`` mirrors the reference's
 VulkanPathTracer and ``scene`` mirrors its SceneSnapshot types.
 """
 from . import scene
-from .scene import (AUTOMATIC, CYLINDER, DISK, DISTANT, DOME, LATLONG, RECT, SPHERE, Light, Material, Mesh,
-                    Scene, Texture, camera)
+from .scene import (AUTOMATIC, CYLINDER, DISK, DISTANT, DOME, LATLONG, RECT, SPHERE, Instancer, Light, Material,
+                    Mesh, Scene, Texture, camera)
 from .tracer import FUSED, MODULAR, RASTER_PREVIEW, PathTracer, lib, pack_scene, probe_devices, render_batch, RadianceCache
 
 __all__ = [
-    "scene", "Scene", "Mesh", "Material", "Texture", "Light", "camera", "PathTracer", "pack_scene", "render_batch", "RadianceCache",
+    "scene", "Scene", "Mesh", "Material", "Texture", "Light", "Instancer", "camera", "PathTracer", "pack_scene",
+    "render_batch", "RadianceCache",
     "probe_devices", "lib", "FUSED", "MODULAR", "RASTER_PREVIEW", "DOME", "RECT", "DISK", "SPHERE",
     "CYLINDER", "DISTANT", "AUTOMATIC", "LATLONG",
 ]

@@ -272,9 +272,29 @@ class Tuning(C.Structure):
     ]
 
 
+class InstancerDesc(C.Structure):
+    _fields_ = [
+        ("mesh_index", C.c_uint64),
+        ("transforms", C.POINTER(C.c_double)),
+        ("instance_count", C.c_uint64),
+    ]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [
+        ("triangles", C.c_uint64),
+        ("instances", C.c_uint64),
+        ("bottom_levels", C.c_uint64),
+        ("bvh_bytes", C.c_uint64),
+        ("scene_bytes", C.c_uint64),
+        ("build_ms", C.c_double),
+        ("bvh_build_ms", C.c_double),
+    ]
+
+
 STRUCTS_IN_ABI_ORDER = [
     Camera, MeshDesc, MaterialDesc, TextureDesc, LightDesc, SceneDesc, PackedTexture, PackedScene,
-    RenderStats, BatchJob, NrcConfig, Tuning,
+    RenderStats, BatchJob, NrcConfig, Tuning, InstancerDesc, SceneInfo,
 ]
 
 GPU_MATERIAL_BYTES = 368

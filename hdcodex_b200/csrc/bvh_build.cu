@@ -218,6 +218,39 @@ __device__ __forceinline__ int ceilLog2Double(double x)
     return m == 0.5 ? e - 1 : e;
 }
 
+// Quantisation frame of a wide node whose children span [lo, hi]: per axis a
+// power-of-two step (at least the box extent / 252 and the floor
+// max(|coordinate|, sceneScale) / 65536) and an origin one step below lo,
+// rounded down. Shared by the build and the refit, so both quantise alike.
+__device__ void nodeFrame(float4 lo, float4 hi, float sceneScale, float origin[3], double step[3], uint8_t biased[3])
+{
+    const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z};
+    for (int k = 0; k < 3; ++k) {
+        const double extent = static_cast<double>(h3[k]) - static_cast<double>(l3[k]);
+        const double floorStep = fmax(fmax(fabs(static_cast<double>(l3[k])), fabs(static_cast<double>(h3[k]))),
+                                      static_cast<double>(sceneScale)) * (1.0 / 65536.0);
+        double q = fmax(fmax(extent / 252.0, floorStep), 1e-30);
+        int e = ceilLog2Double(q);
+        e = max(-126, min(127, e));
+        step[k] = ldexp(1.0, e);
+        biased[k] = static_cast<uint8_t>(e + 127);
+        origin[k] = __double2float_rd(static_cast<double>(l3[k]) - step[k]);
+    }
+}
+
+// A child box [cl, ch] on the node's grid, padded by one step on every side.
+__device__ void quantizeChild(float4 cl, float4 ch, const float origin[3], const double step[3], uint8_t ql[3],
+                              uint8_t qh[3])
+{
+    const float cl3[3] = {cl.x, cl.y, cl.z}, ch3[3] = {ch.x, ch.y, ch.z};
+    for (int k = 0; k < 3; ++k) {
+        const double lo_q = floor((static_cast<double>(cl3[k]) - origin[k]) / step[k]) - 1.0;
+        const double hi_q = ceil((static_cast<double>(ch3[k]) - origin[k]) / step[k]) + 1.0;
+        ql[k] = static_cast<uint8_t>(fmin(fmax(lo_q, 0.0), 255.0));
+        qh[k] = static_cast<uint8_t>(fmin(fmax(hi_q, 0.0), 255.0));
+    }
+}
+
 struct CollapseArgs {
     int n;
     const int* left;
@@ -225,6 +258,7 @@ struct CollapseArgs {
     const float4* nodeLo;
     const float4* nodeHi;
     const uint32_t* sortedIds;
+    const uint32_t* primIds;  // null: a triangle's id is its position in the input list
     const float4* vertices;
     const uint32_t* indices;
     float sceneScale;  // max |coordinate| and scene extent, for the padding floor
@@ -321,21 +355,10 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
     }
 
     // Quantisation grid per axis.
-    const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z};
     float origin[3];
     double step[3];
     uint8_t biased[3];
-    for (int k = 0; k < 3; ++k) {
-        const double extent = static_cast<double>(h3[k]) - static_cast<double>(l3[k]);
-        const double floorStep = fmax(fmax(fabs(static_cast<double>(l3[k])), fabs(static_cast<double>(h3[k]))),
-                                      static_cast<double>(a.sceneScale)) * (1.0 / 65536.0);
-        double q = fmax(fmax(extent / 252.0, floorStep), 1e-30);
-        int e = ceilLog2Double(q);
-        e = max(-126, min(127, e));
-        step[k] = ldexp(1.0, e);
-        biased[k] = static_cast<uint8_t>(e + 127);
-        origin[k] = __double2float_rd(static_cast<double>(l3[k]) - step[k]);
-    }
+    nodeFrame(lo, hi, a.sceneScale, origin, step, biased);
 
     // Allocate internal children and leaf triangles.
     int internalCount = 0, triangleCount = 0;
@@ -368,15 +391,8 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
         node.qhix[s] = node.qhiy[s] = node.qhiz[s] = 0;
         if (i < 0) continue;
         const int b = entries[i];
-        const float4 cl = a.nodeLo[b], ch = a.nodeHi[b];
-        const float cl3[3] = {cl.x, cl.y, cl.z}, ch3[3] = {ch.x, ch.y, ch.z};
         uint8_t ql[3], qh[3];
-        for (int k = 0; k < 3; ++k) {
-            const double lo_q = floor((static_cast<double>(cl3[k]) - origin[k]) / step[k]) - 1.0;
-            const double hi_q = ceil((static_cast<double>(ch3[k]) - origin[k]) / step[k]) + 1.0;
-            ql[k] = static_cast<uint8_t>(fmin(fmax(lo_q, 0.0), 255.0));
-            qh[k] = static_cast<uint8_t>(fmin(fmax(hi_q, 0.0), 255.0));
-        }
+        quantizeChild(a.nodeLo[b], a.nodeHi[b], origin, step, ql, qh);
         node.qlox[s] = ql[0]; node.qloy[s] = ql[1]; node.qloz[s] = ql[2];
         node.qhix[s] = qh[0]; node.qhiy[s] = qh[1]; node.qhiz[s] = qh[2];
         if (!isLeaf(b) && count(b) > kMaxLeafTriangles) {
@@ -399,7 +415,8 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
                     const float4 v0 = a.vertices[a.indices[3 * prim + 0]];
                     const float4 v1 = a.vertices[a.indices[3 * prim + 1]];
                     const float4 v2 = a.vertices[a.indices[3 * prim + 2]];
-                    a.triVerts[3 * dst + 0] = make_float4(v0.x, v0.y, v0.z, __uint_as_float(prim));
+                    const uint32_t id = a.primIds ? a.primIds[prim] : prim;
+                    a.triVerts[3 * dst + 0] = make_float4(v0.x, v0.y, v0.z, __uint_as_float(id));
                     a.triVerts[3 * dst + 1] = make_float4(v1.x, v1.y, v1.z, 0.0f);
                     a.triVerts[3 * dst + 2] = make_float4(v2.x, v2.y, v2.z, 0.0f);
                     written++;
@@ -424,8 +441,105 @@ T* deviceAlloc(size_t count)
 
 }  // namespace
 
+namespace {
+
+// Leaf triangle copies from the current vertices (a refit keeps the leaf
+// order; the id in .w is the triangle's position in the input list).
+__global__ void refitTrianglesKernel(const float4* vertices, const uint32_t* indices, float4* triVerts, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float w = triVerts[3 * i].w;
+    const uint32_t id = __float_as_uint(w);
+    for (int k = 0; k < 3; ++k) {
+        const float4 v = vertices[indices[3 * id + k]];
+        triVerts[3 * i + k] = make_float4(v.x, v.y, v.z, k == 0 ? w : 0.0f);
+    }
+}
+
+// One level of a refit: each node's children get their boxes from the level
+// below (internal children) or from their triangles (leaf children), and the
+// node is quantised again exactly as the build quantises it.
+__global__ void refitLevelKernel(WideNode* nodes, const float4* triVerts, float4* boxes, uint32_t begin, uint32_t end,
+                                 float sceneScale)
+{
+    const uint32_t n = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= end) return;
+    WideNode node = nodes[n];
+    float4 cl[8], ch[8];
+    uint32_t present = 0u;
+    float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.0f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+    for (int s = 0; s < 8; ++s) {
+        const uint32_t meta = node.meta[s];
+        if ((node.imask >> s) & 1u) {
+            const uint32_t child = node.childBase + __popc(node.imask & ((1u << s) - 1u));
+            cl[s] = boxes[2 * child];
+            ch[s] = boxes[2 * child + 1];
+        } else if (meta != 0u) {
+            const uint32_t first = node.triBase + (meta & 31u), count = __popc(meta >> 5);
+            cl[s] = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
+            ch[s] = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+            for (uint32_t t = first; t < first + count; ++t) {
+                for (int k = 0; k < 3; ++k) {
+                    const float4 v = triVerts[3 * t + k];
+                    cl[s] = make_float4(fminf(cl[s].x, v.x), fminf(cl[s].y, v.y), fminf(cl[s].z, v.z), 0.0f);
+                    ch[s] = make_float4(fmaxf(ch[s].x, v.x), fmaxf(ch[s].y, v.y), fmaxf(ch[s].z, v.z), 0.0f);
+                }
+            }
+        } else {
+            continue;
+        }
+        present |= 1u << s;
+        lo = make_float4(fminf(lo.x, cl[s].x), fminf(lo.y, cl[s].y), fminf(lo.z, cl[s].z), 0.0f);
+        hi = make_float4(fmaxf(hi.x, ch[s].x), fmaxf(hi.y, ch[s].y), fmaxf(hi.z, ch[s].z), 0.0f);
+    }
+    float origin[3];
+    double step[3];
+    uint8_t biased[3];
+    nodeFrame(lo, hi, sceneScale, origin, step, biased);
+    node.px = origin[0];
+    node.py = origin[1];
+    node.pz = origin[2];
+    node.ex = biased[0];
+    node.ey = biased[1];
+    node.ez = biased[2];
+    for (int s = 0; s < 8; ++s) {
+        uint8_t ql[3] = {0, 0, 0}, qh[3] = {0, 0, 0};
+        if ((present >> s) & 1u) quantizeChild(cl[s], ch[s], origin, step, ql, qh);
+        node.qlox[s] = ql[0];
+        node.qloy[s] = ql[1];
+        node.qloz[s] = ql[2];
+        node.qhix[s] = qh[0];
+        node.qhiy[s] = qh[1];
+        node.qhiz[s] = qh[2];
+    }
+    nodes[n] = node;
+    boxes[2 * n] = lo;
+    boxes[2 * n + 1] = hi;
+}
+
+}  // namespace
+
+void refitWideBvh(WideBvh& bvh, const float4* vertices, const uint32_t* indices, float sceneScale, cudaStream_t stream)
+{
+    if (bvh.nodeCount == 0 || bvh.levelStart.size() < 2) return;
+    if (!bvh.nodeBoxes) bvh.nodeBoxes = deviceAlloc<float4>(2 * size_t(bvh.nodeCount));
+    refitTrianglesKernel<<<(bvh.triangleCount + kBlock - 1) / kBlock, kBlock, 0, stream>>>(vertices, indices, bvh.triVerts,
+                                                                                          bvh.triangleCount);
+    CUDA_OK(cudaGetLastError());
+    for (size_t d = bvh.levelStart.size() - 1; d-- > 0;) {
+        const uint32_t begin = bvh.levelStart[d], end = bvh.levelStart[d + 1];
+        if (end <= begin) continue;
+        refitLevelKernel<<<(end - begin + kBlock - 1) / kBlock, kBlock, 0, stream>>>(bvh.nodes, bvh.triVerts,
+                                                                                    bvh.nodeBoxes, begin, end, sceneScale);
+        CUDA_OK(cudaGetLastError());
+    }
+    bvh.sceneScale = sceneScale;
+    CUDA_OK(cudaStreamSynchronize(stream));
+}
+
 WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t triangleCount, float sceneScale,
-                     cudaStream_t stream)
+                     cudaStream_t stream, const uint32_t* primIds)
 {
     WideBvh out;
     if (triangleCount == 0) return out;
@@ -496,19 +610,25 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
         CollapseItem* itemsB = static_cast<CollapseItem*>(tmp(sizeof(CollapseItem) * n));
         const CollapseItem root{rootNode, 0u, 0u, 0u};
         CUDA_OK(cudaMemcpyAsync(itemsA, &root, sizeof root, cudaMemcpyHostToDevice, stream));
-        CollapseArgs args{n, left, right, nodeLo, nodeHi, idsSorted, vertices, indices, sceneScale,
+        CollapseArgs args{n, left, right, nodeLo, nodeHi, idsSorted, primIds, vertices, indices, sceneScale,
                           out.nodes, out.triVerts, counters + 0, counters + 1, counters + 2};
         uint32_t itemCount = 1;
         uint32_t depth = 0;
+        // Nodes are allocated level by level: level d is [levelStart[d], levelStart[d+1]).
+        out.levelStart = {0u, 1u};
         while (itemCount > 0) {
             CUDA_OK(cudaMemsetAsync(counters + 3, 0, sizeof(uint32_t), stream));
             collapseKernel<<<(itemCount + kBlock - 1) / kBlock, kBlock, 0, stream>>>(args, itemsA, itemCount, itemsB, counters + 3);
             CUDA_OK(cudaGetLastError());
-            CUDA_OK(cudaMemcpyAsync(&itemCount, counters + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            uint32_t progress[4];
+            CUDA_OK(cudaMemcpyAsync(progress, counters, sizeof progress, cudaMemcpyDeviceToHost, stream));
             CUDA_OK(cudaStreamSynchronize(stream));
+            itemCount = progress[3];
+            if (itemCount > 0) out.levelStart.push_back(progress[0]);
             std::swap(itemsA, itemsB);
             ++depth;
         }
+        out.sceneScale = sceneScale;
         uint32_t finalCounters[4];
         CUDA_OK(cudaMemcpyAsync(finalCounters, counters, sizeof finalCounters, cudaMemcpyDeviceToHost, stream));
         CUDA_OK(cudaStreamSynchronize(stream));
@@ -531,6 +651,7 @@ void freeWideBvh(WideBvh& bvh)
 {
     deviceFree(bvh.nodes);
     deviceFree(bvh.triVerts);
+    deviceFree(bvh.nodeBoxes);
     bvh = WideBvh{};
 }
 

@@ -112,6 +112,29 @@ struct __align__(16) WideNode {
 };
 static_assert(sizeof(WideNode) == 80, "wide node is 80 bytes");
 
+// Two-level scenes (instancers): a bottom-level BVH per instanced mesh, in
+// object space, plus one over the scene's other triangles in world space; the
+// top-level BVH's leaves are instances.
+struct BlasDesc {
+    const WideNode* nodes;
+    const float4* triVerts;  // leaf triangle copies; .w of the first: flattened id (world BLAS) or local index
+    uint32_t nodeCount;
+    uint32_t pad;
+};
+
+struct InstanceDesc {
+    // World to object: object[j] = sum_i (world[i] - inv_i.w) * inv_i[j] for the
+    // rows inv0..inv2 of the inverse of the instance's 3x3 (row vectors, the
+    // translation in .w).
+    float4 inv0, inv1, inv2;
+    uint32_t blas;       // index into DeviceScene::blases
+    uint32_t triBase;    // flattened id of the instance's first triangle
+    uint32_t identity;   // 1: a world-space BLAS (ray and triangle ids used as they are)
+    float margin;        // object-space widening of the boxes for the transformed ray's rounding
+    float invNorm;       // max over j of sum_i |inverse[i][j]|: how much world lengths grow in object space
+    float pad0, pad1, pad2;
+};
+
 // DeviceScene::status bits.
 constexpr unsigned int kTraversalOverflow = 1u;  // a pending node group found the stack full and was dropped
 constexpr unsigned int kTraversalBudget = 2u;    // a traversal visited more nodes than the BVH holds
@@ -137,6 +160,11 @@ struct DeviceScene {
     uint32_t nodeCount;
     uint32_t fullShading;    // 0: no material uses textures or layered lobes (see shadeKernel)
     uint32_t hasSubsurface;  // some material can take the subsurface random walk
+    // Two-level scenes: instances, their BLASes; nodes/triVerts/nodeCount
+    // are then the top-level BVH (its leaf "triangles" carry instance indices).
+    const InstanceDesc* instances;  // null: single-level scene
+    const BlasDesc* blases;
+    uint32_t instanceCount;
     // Traversal faults of the current render (kTraversalOverflow,
     // kTraversalBudget; null: not recorded). Set per render to a word the
     // host reads back with the render's counters.

@@ -198,6 +198,71 @@ HDCX_D void beginTraversal(Traversal& st, const DeviceScene& s, float3 o, float3
     st.rayRng = rayRng;
 }
 
+// Tests the eight children of node `nodeIndex` against a ray (origin o,
+// inverse direction id, octant mask octInv) up to bestT: hit internal
+// children become nodeGroup (hit bits in 24..31 by visiting order | imask),
+// hit leaf triangles triGroup (first slot, bits).
+template <bool kMargin>
+HDCX_D void testNode(const WideNode* nodes, uint32_t nodeIndex, float3 o, float idx, float idy, float idz,
+                     uint32_t octInv, float bestT, float mx, float my, float mz, uint2& nodeGroup, uint2& triGroup)
+{
+    const uint4* np = reinterpret_cast<const uint4*>(nodes + nodeIndex);
+    const uint4 n0 = __ldg(np + 0), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+    const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+    const uint32_t e = n0.w;
+    const float scx = __uint_as_float((e & 0xffu) << 23);
+    const float scy = __uint_as_float(((e >> 8) & 0xffu) << 23);
+    const float scz = __uint_as_float(((e >> 16) & 0xffu) << 23);
+    const uint32_t imask = e >> 24;
+    // t = q * (scale * invd) + (p - o) * invd per plane.
+    const float ax = scx * idx, ay = scy * idy, az = scz * idz;
+    const float bx = (px - o.x) * idx, by = (py - o.y) * idy, bz = (pz - o.z) * idz;
+    const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
+    // With kMargin every box is widened by (mx, my, mz) in t per axis: the
+    // near plane's distance drops by the margin, the far plane's grows.
+    const float2 bxn = kMargin ? make_float2(bx - mx, bx - mx) : make_float2(bx, bx);
+    const float2 byn = kMargin ? make_float2(by - my, by - my) : make_float2(by, by);
+    const float2 bzn = kMargin ? make_float2(bz - mz, bz - mz) : make_float2(bz, bz);
+    const float2 bxf = kMargin ? make_float2(bx + mx, bx + mx) : make_float2(bx, bx);
+    const float2 byf = kMargin ? make_float2(by + my, by + my) : make_float2(by, by);
+    const float2 bzf = kMargin ? make_float2(bz + mz, bz + mz) : make_float2(bz, bz);
+    // Near/far planes by direction sign: words of qlo (n2.x..n3.y) and qhi (n3.z..n4.w).
+    const uint32_t loX0 = n2.x, loX1 = n2.y, loY0 = n2.z, loY1 = n2.w, loZ0 = n3.x, loZ1 = n3.y;
+    const uint32_t hiX0 = n3.z, hiX1 = n3.w, hiY0 = n4.x, hiY1 = n4.y, hiZ0 = n4.z, hiZ1 = n4.w;
+    const bool sx = idx >= 0.0f, sy = idy >= 0.0f, sz = idz >= 0.0f;
+    const uint32_t nearX0 = sx ? loX0 : hiX0, nearX1 = sx ? loX1 : hiX1, farX0 = sx ? hiX0 : loX0, farX1 = sx ? hiX1 : loX1;
+    const uint32_t nearY0 = sy ? loY0 : hiY0, nearY1 = sy ? loY1 : hiY1, farY0 = sy ? hiY0 : loY0, farY1 = sy ? hiY1 : loY1;
+    const uint32_t nearZ0 = sz ? loZ0 : hiZ0, nearZ1 = sz ? loZ1 : hiZ1, farZ0 = sz ? hiZ0 : loZ0, farZ1 = sz ? hiZ1 : loZ1;
+    const uint32_t meta0 = n1.z, meta1 = n1.w;
+    uint32_t nodeHits = 0u, triHits = 0u;
+    // Children 2j and 2j+1 share a word per plane (bytes k and k+1). An
+    // empty slot has meta 0 and is not internal, so it adds no bits.
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int k = (2 * j) & 3;
+        const bool low = j < 2;
+        const float2 tnx = planePair(low ? nearX0 : nearX1, k, ax2, bxn);
+        const float2 tny = planePair(low ? nearY0 : nearY1, k, ay2, byn);
+        const float2 tnz = planePair(low ? nearZ0 : nearZ1, k, az2, bzn);
+        const float2 tfx = planePair(low ? farX0 : farX1, k, ax2, bxf);
+        const float2 tfy = planePair(low ? farY0 : farY1, k, ay2, byf);
+        const float2 tfz = planePair(low ? farZ0 : farZ1, k, az2, bzf);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = 2 * j + h;
+            const uint32_t meta = ((low ? meta0 : meta1) >> (8 * (k + h))) & 0xffu;
+            const float tNear = fmaxf(fmaxf(h ? tnx.y : tnx.x, h ? tny.y : tny.x), fmaxf(h ? tnz.y : tnz.x, 0.0f));
+            const float tFar = fminf(fminf(h ? tfx.y : tfx.x, h ? tfy.y : tfy.x), fminf(h ? tfz.y : tfz.x, bestT));
+            if (tNear <= tFar) {
+                if ((imask >> i) & 1u) nodeHits |= 1u << (static_cast<uint32_t>(i) ^ octInv);
+                else triHits |= (meta >> 5) << (meta & 31u);
+            }
+        }
+    }
+    nodeGroup = make_uint2(n1.x, (nodeHits << 24) | imask);
+    triGroup = make_uint2(n1.y, triHits);
+}
+
 // One traversal step: the triangles of the current triangle group, then one
 // node (its eight children are tested; hit internal children become the new
 // node group, hit leaf triangles the new triangle group). Returns
@@ -272,69 +337,204 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
     }
 
     if (kCount) work->x++;
-    const uint4* np = reinterpret_cast<const uint4*>(s.nodes + nodeIndex);
-    const uint4 n0 = __ldg(np + 0), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
-    const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
-    const uint32_t e = n0.w;
-    const float scx = __uint_as_float((e & 0xffu) << 23);
-    const float scy = __uint_as_float(((e >> 8) & 0xffu) << 23);
-    const float scz = __uint_as_float(((e >> 16) & 0xffu) << 23);
-    const uint32_t imask = e >> 24;
-    const float3 o = st.pre.o;
-    const float idx = st.idx, idy = st.idy, idz = st.idz;
-    // t = q * (scale * invd) + (p - o) * invd per plane.
-    const float ax = scx * idx, ay = scy * idy, az = scz * idz;
-    const float bx = (px - o.x) * idx, by = (py - o.y) * idy, bz = (pz - o.z) * idz;
-    const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
-    const float2 bx2 = make_float2(bx, bx), by2 = make_float2(by, by), bz2 = make_float2(bz, bz);
-    // Near/far planes by direction sign: words of qlo (n2.x..n3.y) and qhi (n3.z..n4.w).
-    const uint32_t loX0 = n2.x, loX1 = n2.y, loY0 = n2.z, loY1 = n2.w, loZ0 = n3.x, loZ1 = n3.y;
-    const uint32_t hiX0 = n3.z, hiX1 = n3.w, hiY0 = n4.x, hiY1 = n4.y, hiZ0 = n4.z, hiZ1 = n4.w;
-    const bool sx = idx >= 0.0f, sy = idy >= 0.0f, sz = idz >= 0.0f;
-    const uint32_t nearX0 = sx ? loX0 : hiX0, nearX1 = sx ? loX1 : hiX1, farX0 = sx ? hiX0 : loX0, farX1 = sx ? hiX1 : loX1;
-    const uint32_t nearY0 = sy ? loY0 : hiY0, nearY1 = sy ? loY1 : hiY1, farY0 = sy ? hiY0 : loY0, farY1 = sy ? hiY1 : loY1;
-    const uint32_t nearZ0 = sz ? loZ0 : hiZ0, nearZ1 = sz ? loZ1 : hiZ1, farZ0 = sz ? hiZ0 : loZ0, farZ1 = sz ? hiZ1 : loZ1;
-    const uint32_t meta0 = n1.z, meta1 = n1.w;
-    const uint32_t octInv = st.octInv;
-    const float bestT = st.bestT;
-    uint32_t nodeHits = 0u, triHits = 0u;
-    // Children 2j and 2j+1 share a word per plane (bytes k and k+1). An
-    // empty slot has meta 0 and is not internal, so it adds no bits.
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int k = (2 * j) & 3;
-        const bool low = j < 2;
-        const float2 tnx = planePair(low ? nearX0 : nearX1, k, ax2, bx2);
-        const float2 tny = planePair(low ? nearY0 : nearY1, k, ay2, by2);
-        const float2 tnz = planePair(low ? nearZ0 : nearZ1, k, az2, bz2);
-        const float2 tfx = planePair(low ? farX0 : farX1, k, ax2, bx2);
-        const float2 tfy = planePair(low ? farY0 : farY1, k, ay2, by2);
-        const float2 tfz = planePair(low ? farZ0 : farZ1, k, az2, bz2);
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int i = 2 * j + h;
-            const uint32_t meta = ((low ? meta0 : meta1) >> (8 * (k + h))) & 0xffu;
-            const float tNear = fmaxf(fmaxf(h ? tnx.y : tnx.x, h ? tny.y : tny.x), fmaxf(h ? tnz.y : tnz.x, 0.0f));
-            const float tFar = fminf(fminf(h ? tfx.y : tfx.x, h ? tfy.y : tfy.x), fminf(h ? tfz.y : tfz.x, bestT));
-            if (tNear <= tFar) {
-                if ((imask >> i) & 1u) nodeHits |= 1u << (static_cast<uint32_t>(i) ^ octInv);
-                else triHits |= (meta >> 5) << (meta & 31u);
-            }
-        }
-    }
-    st.nodeGroup = make_uint2(n1.x, (nodeHits << 24) | imask);
-    st.triGroup = make_uint2(n1.y, triHits);
+    testNode<false>(s.nodes, nodeIndex, st.pre.o, st.idx, st.idy, st.idz, st.octInv, st.bestT, 0.0f, 0.0f, 0.0f,
+                    st.nodeGroup, st.triGroup);
     return kStepContinue;
 }
 
-// Traverses the wide BVH. kAny: stop at the first confirmed candidate.
+// ---------------------------------------------------------------------------
+// Two-level scenes. The top-level BVH's leaves are instances; for each hit
+// instance its BLAS is traversed with the ray in object space (the BLAS of
+// the scene's non-instanced triangles is in world space), sharing the
+// closest hit. Node tests of an instanced BLAS use the object-space ray with
+// boxes widened by a margin that covers the rounding of the transformed ray
+// and of the world vertices; triangle tests always use the world ray and the
+// world-space (flattened) vertices, so hits, distances, barycentrics and the
+// tie rule are those of the flattened scene bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kTopStack = 32;
+
+struct ClosestHit {
+    float t;
+    uint32_t prim;
+    float b1, b2;
+};
+
+// Same acceptance as the single-level traversal (closest, ties to the
+// smaller id; any-hit opacity rules).
+template <Accept kMode, bool kAny>
+HDCX_D bool confirmCandidate(const DeviceScene& s, uint32_t rayRng, uint32_t prim, float t, float b1, float b2,
+                             const ClosestHit& best)
+{
+    if (!kAny) {
+        if (t > best.t) return false;
+        if (t == best.t && prim > best.prim) return false;
+    }
+    if (kMode == Accept::Stochastic) {
+        const float opacity = surfaceOpacity(s, prim, b1, b2);
+        if (opacity < 1.0f && !(anyHitThreshold(rayRng, prim) <= opacity)) return false;
+    } else if (kMode == Accept::Threshold) {
+        if (!(surfaceOpacity(s, prim, b1, b2) >= 0.5f)) return false;
+    }
+    return true;
+}
+
+HDCX_D float3 inverseDirection(float3 d)
+{
+    const float tiny = 8.271806e-25f;  // 2^-80, as beginTraversal
+    return make_float3(1.0f / (fabsf(d.x) > tiny ? d.x : copysignf(tiny, d.x)),
+                       1.0f / (fabsf(d.y) > tiny ? d.y : copysignf(tiny, d.y)),
+                       1.0f / (fabsf(d.z) > tiny ? d.z : copysignf(tiny, d.z)));
+}
+
+HDCX_D uint32_t octantMask(float3 d)
+{
+    return ((d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u)) ^ 7u;
+}
+
+HDCX_D float maxAbs3(float3 v) { return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fabsf(v.z)); }
+
+// Pops the next child node of `group` (nearest octant first), pushing the
+// rest of the group. Returns false when the group and the stack are empty.
+HDCX_D bool nextNode(uint2& group, uint2* stack, int& sp, int capacity, uint32_t octInv, uint32_t& nodeIndex,
+                     const DeviceScene& s)
+{
+    if ((group.y & 0xff000000u) == 0u) {
+        if (sp == 0) return false;
+        group = stack[--sp];
+    }
+    const uint32_t hitBits = group.y >> 24;
+    const uint32_t pos = 31u - __clz(hitBits);
+    group.y &= ~(1u << (24u + pos));
+    const uint32_t childSlot = pos ^ octInv;
+    nodeIndex = group.x + __popc((group.y & 0xffu) & ((1u << childSlot) - 1u));
+    if ((group.y & 0xff000000u) != 0u) {
+        if (sp < capacity) stack[sp++] = group;
+        else traversalFault(s, kTraversalOverflow);
+    }
+    return true;
+}
+
+// The BLAS of instance `inst`; returns true for kAny at the first confirmed
+// candidate, else updates `best`.
+template <Accept kMode, bool kAny, bool kCount>
+HDCX_D bool traceInstance(const DeviceScene& s, const RayPre& pre, float3 o, float3 d, float tmin, uint32_t rayRng,
+                          uint32_t inst, ClosestHit& best, uint2* stack, uint2* work)
+{
+    const InstanceDesc I = s.instances[inst];
+    const BlasDesc B = s.blases[I.blas];
+    float3 ro = o, rd = d;
+    float margin = 0.0f;
+    if (!I.identity) {
+        const float ox = o.x - I.inv0.w, oy = o.y - I.inv1.w, oz = o.z - I.inv2.w;
+        ro = make_float3((ox * I.inv0.x + oy * I.inv1.x) + oz * I.inv2.x, (ox * I.inv0.y + oy * I.inv1.y) + oz * I.inv2.y,
+                         (ox * I.inv0.z + oy * I.inv1.z) + oz * I.inv2.z);
+        rd = make_float3((d.x * I.inv0.x + d.y * I.inv1.x) + d.z * I.inv2.x, (d.x * I.inv0.y + d.y * I.inv1.y) + d.z * I.inv2.y,
+                         (d.x * I.inv0.z + d.y * I.inv1.z) + d.z * I.inv2.z);
+        // Rounding of the transformed ray: a few ulps of the magnitudes that
+        // enter it, along the whole segment up to the current closest hit.
+        margin = I.margin + 9.5367432e-7f * (maxAbs3(ro) + I.invNorm * maxAbs3(o) + fminf(best.t, 3.0e38f) * maxAbs3(rd));
+    }
+    const float3 id = inverseDirection(rd);
+    const uint32_t octInv = octantMask(rd);
+    const float mx = margin * fabsf(id.x), my = margin * fabsf(id.y), mz = margin * fabsf(id.z);
+    uint2 group = B.nodeCount == 0u ? make_uint2(0u, 0u) : make_uint2(0u, (1u << (24u + octInv)) | 1u);
+    uint2 tris = make_uint2(0u, 0u);
+    int sp = 0;
+    uint32_t budget = B.nodeCount + 1u;
+    for (;;) {
+        while (tris.y != 0u) {
+            const int bit = __ffs(tris.y) - 1;
+            tris.y &= tris.y - 1u;
+            const uint32_t slot = tris.x + static_cast<uint32_t>(bit);
+            const float4 w0 = __ldg(B.triVerts + slot * 3u + 0u);
+            float3 v0, v1, v2;
+            uint32_t prim;
+            if (I.identity) {
+                prim = __float_as_uint(w0.w);
+                v0 = xyz(w0);
+                v1 = xyz(__ldg(B.triVerts + slot * 3u + 1u));
+                v2 = xyz(__ldg(B.triVerts + slot * 3u + 2u));
+            } else {
+                // The instance's flattened triangle: world-space vertices.
+                prim = I.triBase + __float_as_uint(w0.w);
+                v0 = xyz(__ldg(s.vertices + __ldg(s.indices + prim * 3u + 0u)));
+                v1 = xyz(__ldg(s.vertices + __ldg(s.indices + prim * 3u + 1u)));
+                v2 = xyz(__ldg(s.vertices + __ldg(s.indices + prim * 3u + 2u)));
+            }
+            if (kCount) work->y++;
+            float t, b1, b2;
+            if (!intersectTriangle(pre, v0, v1, v2, tmin, best.t, t, b1, b2)) continue;
+            if (!confirmCandidate<kMode, kAny>(s, rayRng, prim, t, b1, b2, best)) continue;
+            if (kAny) return true;
+            best = ClosestHit{t, prim, b1, b2};
+        }
+        uint32_t nodeIndex;
+        if (!nextNode(group, stack, sp, kTraversalStack, octInv, nodeIndex, s)) return false;
+        if (budget-- == 0u) {
+            traversalFault(s, kTraversalBudget);
+            return false;
+        }
+        if (kCount) work->x++;
+        if (I.identity) {
+            testNode<false>(B.nodes, nodeIndex, ro, id.x, id.y, id.z, octInv, best.t, 0.0f, 0.0f, 0.0f, group, tris);
+        } else {
+            testNode<true>(B.nodes, nodeIndex, ro, id.x, id.y, id.z, octInv, best.t, mx, my, mz, group, tris);
+        }
+    }
+}
+
+template <Accept kMode, bool kAny, bool kCount>
+HDCX_D bool traceInstanced(const DeviceScene& s, float3 o, float3 d, float tmin, float tmax, uint32_t rayRng,
+                           HitRecord& hit, uint2* work)
+{
+    const RayPre pre = precomputeRay(o, d);
+    const float3 id = inverseDirection(d);
+    const uint32_t octInv = octantMask(d);
+    ClosestHit best{tmax, kInvalidPrimitive, 0.0f, 0.0f};
+    uint2 topStack[kTopStack];
+    uint2 stack[kTraversalStack];
+    uint2 group = make_uint2(0u, (1u << (24u + octInv)) | 1u);
+    uint2 leaves = make_uint2(0u, 0u);
+    int sp = 0;
+    uint32_t budget = s.nodeCount + 1u;
+    for (;;) {
+        while (leaves.y != 0u) {
+            const int bit = __ffs(leaves.y) - 1;
+            leaves.y &= leaves.y - 1u;
+            const uint32_t slot = leaves.x + static_cast<uint32_t>(bit);
+            const uint32_t inst = __float_as_uint(__ldg(&s.triVerts[slot * 3u].w));
+            if (traceInstance<kMode, kAny, kCount>(s, pre, o, d, tmin, rayRng, inst, best, stack, work)) return true;
+        }
+        uint32_t nodeIndex;
+        if (!nextNode(group, topStack, sp, kTopStack, octInv, nodeIndex, s)) break;
+        if (budget-- == 0u) {
+            traversalFault(s, kTraversalBudget);
+            break;
+        }
+        if (kCount) work->x++;
+        testNode<false>(s.nodes, nodeIndex, o, id.x, id.y, id.z, octInv, best.t, 0.0f, 0.0f, 0.0f, group, leaves);
+    }
+    if (kAny || best.prim == kInvalidPrimitive) return false;
+    hit.t = best.t;
+    hit.primitive = best.prim;
+    hit.b1 = best.b1;
+    hit.b2 = best.b2;
+    return true;
+}
+
+// Traverses the scene. kAny: stop at the first confirmed candidate.
 // Returns true on a (confirmed) hit; for closest queries fills `hit`.
 // kCount adds the wide nodes loaded to work.x and the triangle tests to work.y.
-template <Accept kMode, bool kAny, bool kCount = false>
+// kInst: 0 single-level scenes only, 1 two-level scenes only, -1 either
+// (decided per call by DeviceScene::instances).
+template <Accept kMode, bool kAny, bool kCount = false, int kInst = -1>
 HDCX_D bool traceRay(const DeviceScene& s, float3 o, float3 d, float tmin, float tmax, uint32_t rayRng, HitRecord& hit,
                      uint2* work = nullptr)
 {
     if (s.nodeCount == 0u) return false;
+    if (kInst == 1 || (kInst == -1 && s.instances != nullptr))
+        return traceInstanced<kMode, kAny, kCount>(s, o, d, tmin, tmax, rayRng, hit, work);
     Traversal st;
     beginTraversal(st, s, o, d, tmin, tmax, rayRng);
     uint2 stack[kTraversalStack];

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstddef>
 #include <memory>
 #include <mutex>
@@ -204,6 +205,45 @@ ArenaLease checkoutArena(int device, bool wait)
 // Frames of hdcx_render_async in flight (defined with the render helpers).
 struct AsyncFrames;
 
+// A scene with instancers: the bottom-level BVHs (index 0: the scene's
+// non-instanced triangles in world space, when it has any; then one per
+// instancer, in object space), the top-level BVH over the instances, the
+// device tables behind DeviceScene::instances / blases, and the packed scene
+// kept on the host for hdcx_update_instancer_points.
+struct TwoLevel {
+    std::vector<WideBvh> blases;
+    std::vector<int> blasOfInstancer;  // per instancer: its index in blases
+    WideBvh top;
+    std::vector<DeviceBuffer*> buffers;
+    std::vector<float4*> objectPoints;      // per instancer, device
+    std::vector<uint32_t*> objectIndices;   // per instancer, device
+    std::vector<float> objectScale;         // per instancer: the BLAS's quantisation floor
+    std::vector<InstanceDesc> instances;
+    std::vector<BlasDesc> blasTable;
+    InstanceDesc* instancesDevice = nullptr;
+    BlasDesc* blasDevice = nullptr;
+    uint32_t plainInstance = 0;             // 1 when instance 0 is the world-space BLAS
+    PackedSceneData host;
+    TwoLevel() = default;
+    TwoLevel(const TwoLevel&) = delete;
+    TwoLevel& operator=(const TwoLevel&) = delete;
+    ~TwoLevel()
+    {
+        for (WideBvh& b : blases) freeWideBvh(b);
+        freeWideBvh(top);
+        for (DeviceBuffer* b : buffers) delete b;
+    }
+    template <typename T>
+    T* upload(const std::vector<T>& data, cudaStream_t stream)
+    {
+        auto* b = new DeviceBuffer();
+        buffers.push_back(b);
+        b->allocate(std::max<size_t>(1, data.size()) * sizeof(T));
+        if (!data.empty()) check(cudaMemcpyAsync(b->ptr, data.data(), data.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
+        return b->as<T>();
+    }
+};
+
 }  // namespace
 
 struct hdcx_nrc {
@@ -249,6 +289,10 @@ struct hdcx_tracer {
     DeviceBuffer preview;  // hdcx_render_preview's upscaled image
     // Frames of hdcx_render_async in flight (created on first use).
     AsyncFrames* async = nullptr;
+    // Two-level scenes (hdcx_set_scene_instanced); null for single-level ones.
+    std::unique_ptr<TwoLevel> twoLevel;
+    double sceneBuildMs = 0.0;  // host wall time of the last set_scene
+    double bvhBuildMs = 0.0;    // of which building the BVHs
     DeviceBuffer statsBuffer;  // this tracer's ray counters (8 x u64), whichever path buffers it renders with
     FrameBuffers fb;
     uint64_t xyzSamples = 0;
@@ -280,6 +324,7 @@ struct hdcx_tracer {
         sceneBuffers.clear();
         texDescs.reset();
         freeWideBvh(bvh);
+        twoLevel.reset();
         scene = DeviceScene{};
         geometryReady = false;
     }
@@ -415,6 +460,170 @@ bool buildCdfArrays(const PackedTexture& pt, std::vector<float>& block)
     return true;
 }
 
+// Object-space scale of a point set (max |coordinate|, max extent): the
+// quantisation floor of its BVH.
+float pointScale(const float* xyzw, size_t count)
+{
+    float scale = 0.0F;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = 0; i < count; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            const float v = xyzw[4 * i + k];
+            if (!std::isfinite(v)) continue;
+            lo[k] = std::min(lo[k], v);
+            hi[k] = std::max(hi[k], v);
+            scale = std::max(scale, std::fabs(v));
+        }
+    }
+    for (int k = 0; k < 3; ++k)
+        if (hi[k] >= lo[k]) scale = std::max(scale, hi[k] - lo[k]);
+    return std::max(scale, 1e-20F);
+}
+
+// World boxes of the instances (over their flattened vertices) as the
+// degenerate triangles (lo, hi, lo) the top-level build takes, and the
+// instances' margins; then the top-level BVH.
+void buildTopLevel(hdcx_tracer* t, TwoLevel& tl, const PackedSceneData& d, const std::vector<uint32_t>& plainVertices)
+{
+    std::vector<float> boxes;
+    std::vector<uint32_t> boxIndices;
+    auto addBox = [&](const float* xyzw, const uint32_t* which, size_t count) {
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        float mag = 0.0F;
+        for (size_t i = 0; i < count; ++i) {
+            const float* v = xyzw + 4 * size_t(which ? which[i] : i);
+            for (int k = 0; k < 3; ++k) {
+                if (!std::isfinite(v[k])) continue;
+                lo[k] = std::min(lo[k], v[k]);
+                hi[k] = std::max(hi[k], v[k]);
+                mag = std::max(mag, std::fabs(v[k]));
+            }
+        }
+        const uint32_t b = static_cast<uint32_t>(boxes.size() / 4);
+        boxes.insert(boxes.end(), {lo[0], lo[1], lo[2], 1.0F, hi[0], hi[1], hi[2], 1.0F});
+        boxIndices.insert(boxIndices.end(), {b, b + 1u, b});
+        return mag;
+    };
+    size_t inst = 0;
+    if (tl.plainInstance) {
+        addBox(d.vertices.data(), plainVertices.data(), plainVertices.size());
+        inst = 1;
+    }
+    for (size_t k = 0; k < d.instancers.size(); ++k) {
+        const PackedInstancer& pi = d.instancers[k];
+        float objectMag = 0.0F;
+        for (size_t i = 0; i < pi.points.size(); i += 4)
+            for (int c = 0; c < 3; ++c)
+                if (std::isfinite(pi.points[i + c])) objectMag = std::max(objectMag, std::fabs(pi.points[i + c]));
+        for (uint32_t j = 0; j < pi.instanceCount; ++j, ++inst) {
+            const float worldMag = addBox(d.vertices.data() + 4 * (size_t(pi.firstVertex) + size_t(j) * pi.pointCount()), nullptr,
+                                          pi.pointCount());
+            InstanceDesc& I = tl.instances[inst];
+            const float translation = std::max({std::fabs(I.inv0.w), std::fabs(I.inv1.w), std::fabs(I.inv2.w)});
+            // 2^-20 of every magnitude that enters the transformed ray and the
+            // world vertices, taken to object space.
+            I.margin = 9.5367432e-7F * (objectMag + (worldMag + translation) * I.invNorm);
+        }
+    }
+    float* boxDev = tl.upload(boxes, t->stream);
+    uint32_t* boxIdxDev = tl.upload(boxIndices, t->stream);
+    freeWideBvh(tl.top);
+    tl.top = buildWideBvh(reinterpret_cast<const float4*>(boxDev), boxIdxDev, static_cast<uint32_t>(boxIndices.size() / 3),
+                          pointScale(boxes.data(), boxes.size() / 4), t->stream);
+    check(cudaMemcpyAsync(tl.instancesDevice, tl.instances.data(), tl.instances.size() * sizeof(InstanceDesc),
+                          cudaMemcpyHostToDevice, t->stream),
+          "upload instances");
+}
+
+// The two-level form of a scene with instancers (see TwoLevel).
+void buildTwoLevel(hdcx_tracer* t, const PackedSceneData& d, DeviceScene& s, float worldScale)
+{
+    auto tl = std::make_unique<TwoLevel>();
+    tl->host = d;
+    const size_t n = d.triangleCount();
+    std::vector<uint8_t> instanced(n, 0u);
+    for (const PackedInstancer& pi : d.instancers) {
+        const size_t end = size_t(pi.firstTriangle) + size_t(pi.instanceCount) * pi.triangles();
+        for (size_t p = pi.firstTriangle; p < end; ++p) instanced[p] = 1u;
+    }
+    std::vector<uint32_t> plainIds, plainIndices, plainVertices;
+    for (size_t p = 0; p < n; ++p) {
+        if (instanced[p]) continue;
+        plainIds.push_back(static_cast<uint32_t>(p));
+        for (int c = 0; c < 3; ++c) {
+            plainIndices.push_back(d.indices[3 * p + c]);
+            plainVertices.push_back(d.indices[3 * p + c]);
+        }
+    }
+    if (!plainIds.empty()) {
+        uint32_t* idsDev = tl->upload(plainIds, t->stream);
+        uint32_t* idxDev = tl->upload(plainIndices, t->stream);
+        tl->blases.push_back(buildWideBvh(s.vertices, idxDev, static_cast<uint32_t>(plainIds.size()), worldScale, t->stream,
+                                          idsDev));
+        tl->plainInstance = 1;
+        InstanceDesc I{};
+        I.inv0 = make_float4(1.0F, 0.0F, 0.0F, 0.0F);
+        I.inv1 = make_float4(0.0F, 1.0F, 0.0F, 0.0F);
+        I.inv2 = make_float4(0.0F, 0.0F, 1.0F, 0.0F);
+        I.blas = 0;
+        I.identity = 1;
+        I.invNorm = 1.0F;
+        tl->instances.push_back(I);
+    }
+    for (const PackedInstancer& pi : d.instancers) {
+        const uint32_t blas = static_cast<uint32_t>(tl->blases.size());
+        tl->blasOfInstancer.push_back(static_cast<int>(blas));
+        float4* pts = reinterpret_cast<float4*>(tl->upload(pi.points, t->stream));
+        uint32_t* idx = tl->upload(pi.indices, t->stream);
+        tl->objectPoints.push_back(pts);
+        tl->objectIndices.push_back(idx);
+        tl->objectScale.push_back(pointScale(pi.points.data(), pi.pointCount()));
+        tl->blases.push_back(buildWideBvh(pts, idx, pi.triangles(), tl->objectScale.back(), t->stream));
+        for (uint32_t j = 0; j < pi.instanceCount; ++j) {
+            const double* T = pi.transforms.data() + 16u * j;
+            // inverse(A) by cofactors, as the flattening computes it.
+            const double a00 = T[0], a01 = T[1], a02 = T[2], a10 = T[4], a11 = T[5], a12 = T[6], a20 = T[8], a21 = T[9],
+                         a22 = T[10];
+            const double c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
+            const double det = (a00 * c00 + a01 * c01) + a02 * c02;
+            const double inv[9] = {c00 / det,
+                                   (a02 * a21 - a01 * a22) / det,
+                                   (a01 * a12 - a02 * a11) / det,
+                                   c01 / det,
+                                   (a00 * a22 - a02 * a20) / det,
+                                   (a02 * a10 - a00 * a12) / det,
+                                   c02 / det,
+                                   (a01 * a20 - a00 * a21) / det,
+                                   (a00 * a11 - a01 * a10) / det};
+            InstanceDesc I{};
+            I.inv0 = make_float4(float(inv[0]), float(inv[1]), float(inv[2]), float(T[12]));
+            I.inv1 = make_float4(float(inv[3]), float(inv[4]), float(inv[5]), float(T[13]));
+            I.inv2 = make_float4(float(inv[6]), float(inv[7]), float(inv[8]), float(T[14]));
+            I.blas = blas;
+            I.triBase = pi.firstTriangle + j * pi.triangles();
+            I.identity = 0;
+            float norm = 0.0F;
+            for (int c = 0; c < 3; ++c)
+                norm = std::max(norm, float(std::fabs(inv[c]) + std::fabs(inv[3 + c]) + std::fabs(inv[6 + c])));
+            if (!std::isfinite(norm) || !std::isfinite(det) || det == 0.0)
+                throw std::invalid_argument("instancer: a transform is singular or not finite");
+            I.invNorm = norm;
+            tl->instances.push_back(I);
+        }
+    }
+    for (const WideBvh& b : tl->blases) tl->blasTable.push_back(BlasDesc{b.nodes, b.triVerts, b.nodeCount, 0u});
+    tl->blasDevice = tl->upload(tl->blasTable, t->stream);
+    tl->instancesDevice = tl->upload(tl->instances, t->stream);
+    buildTopLevel(t, *tl, d, plainVertices);
+    s.nodes = tl->top.nodes;
+    s.triVerts = tl->top.triVerts;
+    s.nodeCount = tl->top.nodeCount;
+    s.instances = tl->instancesDevice;
+    s.blases = tl->blasDevice;
+    s.instanceCount = static_cast<uint32_t>(tl->instances.size());
+    t->twoLevel = std::move(tl);
+}
+
 void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
 {
     check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
@@ -501,11 +710,17 @@ void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
     for (int k = 0; k < 3; ++k) {
         if (hi[k] >= lo[k]) scale = std::max(scale, hi[k] - lo[k]);
     }
-    t->bvh = buildWideBvh(s.vertices, s.indices, s.primitiveCount, std::max(scale, 1e-20F), t->stream);
-    s.nodes = t->bvh.nodes;
-    s.triVerts = t->bvh.triVerts;
-    s.nodeCount = t->bvh.nodeCount;
+    const auto bvhStart = std::chrono::steady_clock::now();
+    if (d.instancers.empty()) {
+        t->bvh = buildWideBvh(s.vertices, s.indices, s.primitiveCount, std::max(scale, 1e-20F), t->stream);
+        s.nodes = t->bvh.nodes;
+        s.triVerts = t->bvh.triVerts;
+        s.nodeCount = t->bvh.nodeCount;
+    } else {
+        buildTwoLevel(t, d, s, std::max(scale, 1e-20F));
+    }
     check(cudaStreamSynchronize(t->stream), "scene upload");
+    t->bvhBuildMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - bvhStart).count();
     t->scene = s;
     t->geometryReady = true;
 }
@@ -631,7 +846,8 @@ HDCX_API uint32_t hdcx_abi_struct_sizes(uint64_t* sizes, uint32_t capacity)
     const uint64_t all[] = {sizeof(hdcx_camera),         sizeof(hdcx_mesh_desc),  sizeof(hdcx_material_desc),
                             sizeof(hdcx_texture_desc),   sizeof(hdcx_light_desc), sizeof(hdcx_scene_desc),
                             sizeof(hdcx_packed_texture), sizeof(hdcx_packed_scene), sizeof(hdcx_render_stats),
-                            sizeof(hdcx_batch_job), sizeof(hdcx_nrc_config), sizeof(hdcx_tuning)};
+                            sizeof(hdcx_batch_job), sizeof(hdcx_nrc_config), sizeof(hdcx_tuning),
+                            sizeof(hdcx_instancer_desc), sizeof(hdcx_scene_info)};
     const uint32_t n = static_cast<uint32_t>(sizeof(all) / sizeof(all[0]));
     for (uint32_t i = 0; i < std::min(n, capacity); ++i) sizes[i] = all[i];
     return n;
@@ -803,6 +1019,12 @@ HDCX_API const char* hdcx_last_error(const hdcx_tracer* t) { return t ? t->lastE
 
 HDCX_API hdcx_status hdcx_set_scene(hdcx_tracer* t, const hdcx_scene_desc* desc)
 {
+    return hdcx_set_scene_instanced(t, desc, nullptr, 0);
+}
+
+HDCX_API hdcx_status hdcx_set_scene_instanced(hdcx_tracer* t, const hdcx_scene_desc* desc,
+                                              const hdcx_instancer_desc* instancers, uint64_t instancerCount)
+{
     if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
     return guarded(t, [&] {
         drainAsync(t);
@@ -811,9 +1033,95 @@ HDCX_API hdcx_status hdcx_set_scene(hdcx_tracer* t, const hdcx_scene_desc* desc)
             t->clearScene();
             return;
         }
-        const PackedSceneData d = packScene(*desc);
+        const auto start = std::chrono::steady_clock::now();
+        const PackedSceneData d = packScene(*desc, instancers, instancerCount);
         uploadScene(t, d);
+        t->sceneBuildMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - start).count();
     });
+}
+
+HDCX_API hdcx_status hdcx_update_instancer_points(hdcx_tracer* t, uint64_t instancer, const float* positions,
+                                                  uint64_t positionCount)
+{
+    if (!t || !positions) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (!t->twoLevel || instancer >= t->twoLevel->host.instancers.size())
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_update_instancer_points: no such instancer in the scene");
+    TwoLevel& tl = *t->twoLevel;
+    PackedInstancer& pi = tl.host.instancers[instancer];
+    if (positionCount != 3u * uint64_t(pi.pointCount()))
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT,
+                    "hdcx_update_instancer_points: position_count must be 3 x the mesh's point count (" +
+                        std::to_string(3u * uint64_t(pi.pointCount())) + ")");
+    return guarded(t, [&] {
+        drainAsync(t);
+        check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+        for (uint32_t p = 0; p < pi.pointCount(); ++p)
+            for (int c = 0; c < 3; ++c) pi.points[4 * p + c] = positions[3 * p + c];
+        // The flattened world vertices of every instance and the emissive CDF.
+        const std::vector<float> world = instancerWorldPoints(pi);
+        std::copy(world.begin(), world.end(), tl.host.vertices.begin() + 4 * size_t(pi.firstVertex));
+        recomputeEmissive(tl.host);
+        auto* vertices = const_cast<float4*>(t->scene.vertices);
+        check(cudaMemcpyAsync(vertices + pi.firstVertex, world.data(), world.size() * sizeof(float), cudaMemcpyHostToDevice,
+                              t->stream),
+              "update vertices");
+        check(cudaMemcpyAsync(const_cast<float4*>(t->scene.emissive), tl.host.emissive.data(),
+                              tl.host.emissive.size() * sizeof(float), cudaMemcpyHostToDevice, t->stream),
+              "update emissive");
+        // Refit of the instancer's bottom level in object space, then a new
+        // top level over the moved instances.
+        check(cudaMemcpyAsync(tl.objectPoints[instancer], pi.points.data(), pi.points.size() * sizeof(float),
+                              cudaMemcpyHostToDevice, t->stream),
+              "update object points");
+        tl.objectScale[instancer] = pointScale(pi.points.data(), pi.pointCount());
+        WideBvh& blas = tl.blases[tl.blasOfInstancer[instancer]];
+        refitWideBvh(blas, tl.objectPoints[instancer], tl.objectIndices[instancer], tl.objectScale[instancer], t->stream);
+        std::vector<uint32_t> plainVertices;
+        if (tl.plainInstance) {
+            std::vector<uint8_t> instanced(tl.host.triangleCount(), 0u);
+            for (const PackedInstancer& q : tl.host.instancers) {
+                const size_t end = size_t(q.firstTriangle) + size_t(q.instanceCount) * q.triangles();
+                for (size_t p = q.firstTriangle; p < end; ++p) instanced[p] = 1u;
+            }
+            for (size_t p = 0; p < instanced.size(); ++p)
+                if (!instanced[p])
+                    for (int c = 0; c < 3; ++c) plainVertices.push_back(tl.host.indices[3 * p + c]);
+        }
+        buildTopLevel(t, tl, tl.host, plainVertices);
+        check(cudaStreamSynchronize(t->stream), "update instancer");
+        t->scene.nodes = tl.top.nodes;
+        t->scene.triVerts = tl.top.triVerts;
+        t->scene.nodeCount = tl.top.nodeCount;
+        const size_t nt = tl.host.triangleCount();
+        t->scene.hasMeshLights = (nt > 0 && tl.host.emissive[(nt - 1) * 4u] > 0.0F) ? 1u : 0u;
+    });
+}
+
+HDCX_API hdcx_status hdcx_get_scene_info(const hdcx_tracer* t, hdcx_scene_info* info)
+{
+    if (!t || !info) return HDCX_ERROR_INVALID_ARGUMENT;
+    *info = hdcx_scene_info{};
+    if (!t->geometryReady) return HDCX_OK;
+    auto bvhBytes = [](const WideBvh& b) {
+        return uint64_t(b.nodeCount) * sizeof(WideNode) + uint64_t(b.triangleCount) * 3u * sizeof(float4);
+    };
+    info->triangles = t->scene.primitiveCount;
+    uint64_t sceneBytes = 0;
+    for (const DeviceBuffer* b : t->sceneBuffers) sceneBytes += b->bytes;
+    if (t->twoLevel) {
+        const TwoLevel& tl = *t->twoLevel;
+        info->instances = tl.instances.size();
+        info->bottom_levels = tl.blases.size();
+        info->bvh_bytes = bvhBytes(tl.top);
+        for (const WideBvh& b : tl.blases) info->bvh_bytes += bvhBytes(b);
+        for (const DeviceBuffer* b : tl.buffers) sceneBytes += b->bytes;
+    } else {
+        info->bvh_bytes = bvhBytes(t->bvh);
+    }
+    info->scene_bytes = sceneBytes + info->bvh_bytes;
+    info->build_ms = t->sceneBuildMs;
+    info->bvh_build_ms = t->bvhBuildMs;
+    return HDCX_OK;
 }
 
 HDCX_API hdcx_status hdcx_set_scene_packed(hdcx_tracer* t, const hdcx_packed_scene* view)
@@ -827,13 +1135,19 @@ HDCX_API hdcx_status hdcx_set_scene_packed(hdcx_tracer* t, const hdcx_packed_sce
 
 HDCX_API hdcx_status hdcx_pack_scene(const hdcx_scene_desc* desc, hdcx_packing** out)
 {
+    return hdcx_pack_scene_instanced(desc, nullptr, 0, out);
+}
+
+HDCX_API hdcx_status hdcx_pack_scene_instanced(const hdcx_scene_desc* desc, const hdcx_instancer_desc* instancers,
+                                               uint64_t instancerCount, hdcx_packing** out)
+{
     if (!desc || !out) return HDCX_ERROR_INVALID_ARGUMENT;
     *out = nullptr;
     try {
-        auto* p = new hdcx_packing();
-        p->data = packScene(*desc);
+        auto p = std::make_unique<hdcx_packing>();
+        p->data = packScene(*desc, instancers, instancerCount);
         makePackedView(p->data, p->textureViews, &p->view);
-        *out = p;
+        *out = p.release();
         return HDCX_OK;
     } catch (const std::bad_alloc&) {
         return HDCX_ERROR_OUT_OF_MEMORY;
@@ -1445,7 +1759,8 @@ struct BatchGraphCache {
     cudaGraphExec_t exec = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t fork = nullptr, start = nullptr, stop = nullptr;
-    std::vector<cudaEvent_t> jobStart, jobStop;  // timing events per job slot
+    std::vector<cudaEvent_t> jobStart, jobStop;  // timing events per job slot (event-record nodes of the graph)
+    std::vector<cudaEvent_t> jobDone;            // per job slot: ordering only (lane order, the join)
     uint64_t instantiations = 0, updates = 0;
 };
 
@@ -1493,14 +1808,17 @@ float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<Render
         }
     }
     while (cache.jobStart.size() < count) {
-        cudaEvent_t a = nullptr, b = nullptr;
-        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+        cudaEvent_t a = nullptr, b = nullptr, c = nullptr;
+        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c, cudaEventDisableTiming) != cudaSuccess) {
             if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
             cudaGetLastError();
             return -1.0F;
         }
         cache.jobStart.push_back(a);
         cache.jobStop.push_back(b);
+        cache.jobDone.push_back(c);
     }
     bool captured = cudaStreamBeginCapture(cache.stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
     try {
@@ -1514,12 +1832,15 @@ float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<Render
                 hdcx_tracer* t = jobs[j].tracer;
                 const int lane = plan.lane[j];
                 const bool afterLane = lane >= 0 && laneLast[lane] >= 0;
-                check(cudaStreamWaitEvent(t->stream, afterLane ? cache.jobStop[laneLast[lane]] : cache.fork, 0),
+                check(cudaStreamWaitEvent(t->stream, afterLane ? cache.jobDone[laneLast[lane]] : cache.fork, 0),
                       "join the capture");
-                check(cudaEventRecord(cache.jobStart[j], t->stream), "job start");
+                // Timing events become event-record nodes of the graph (a
+                // plain record inside a capture only orders the streams).
+                check(cudaEventRecordWithFlags(cache.jobStart[j], t->stream, cudaEventRecordExternal), "job start");
                 enqueueRender(t, calls[j], nullptr, false);
-                check(cudaEventRecord(cache.jobStop[j], t->stream), "job stop");
-                check(cudaStreamWaitEvent(cache.stream, cache.jobStop[j], 0), "join");
+                check(cudaEventRecordWithFlags(cache.jobStop[j], t->stream, cudaEventRecordExternal), "job stop");
+                check(cudaEventRecord(cache.jobDone[j], t->stream), "job done");
+                check(cudaStreamWaitEvent(cache.stream, cache.jobDone[j], 0), "join");
                 if (lane >= 0) laneLast[lane] = static_cast<int>(j);
             }
         }
@@ -1576,6 +1897,7 @@ float enqueueBatchGraph(hdcx_batch_job* jobs, uint32_t count, std::vector<Render
             jobs[j].status = fail(t, HDCX_ERROR_CUDA, std::string("hdcx_render_batch (CUDA graph): ") +
                                                            cudaGetErrorString(jobErr));
             calls[j].active = false;
+            cudaGetLastError();
         }
     }
     if (err != cudaSuccess) cudaGetLastError();

@@ -143,7 +143,8 @@ __global__ void generateKernel(FrameConst f, WaveDesc w, PathBuffers p)
 #define HDCX_TRACE_MIN_BLOCKS 8
 #endif
 
-template <Accept kMode, bool kCount>
+// kInst (traversal kernels): 0 single-level scenes, 1 scenes with instancers.
+template <Accept kMode, bool kCount, int kInst>
 __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) extendKernel(DeviceScene s, PathBuffers p, const uint32_t* queue,
                                                     const uint32_t* count)
 {
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) extendKernel(Devic
         const float4 o = p.rayOrigin[slot];
         const float4 d = p.rayDirection[slot];
         HitRecord h;
-        const bool found = traceRay<kMode, false, kCount>(s, xyz(o), xyz(d), 0.001f, 10000.0f, p.rng[slot], h, &work);
+        const bool found = traceRay<kMode, false, kCount, kInst>(s, xyz(o), xyz(d), 0.001f, 10000.0f, p.rng[slot], h, &work);
         p.hit[slot] = found ? make_float4(h.t, __uint_as_float(h.primitive), h.b1, h.b2)
                             : make_float4(0.0f, __uint_as_float(kInvalidPrimitive), 0.0f, 0.0f);
         // Hits and misses go to separate queues, so that shading warps hold
@@ -245,13 +246,14 @@ __device__ void traceSurfaceLightSample(PathBuffers& p, const DeviceScene& s, co
     }
 }
 
+template <int kInst = -1>
 __device__ bool traceOpaqueBoundary(const DeviceScene& s, PathBuffers& p, float3 origin, float3 direction,
                                     float3& boundary, float3& boundaryNormal, float& boundaryDistance)
 {
     // :1130-1151
     atomicAdd(p.stats + 2, 1ull);
     HitRecord h;
-    if (!traceRay<Accept::Opaque, false>(s, origin, direction, 0.001f, 10000.0f, 0u, h)) return false;
+    if (!traceRay<Accept::Opaque, false, false, kInst>(s, origin, direction, 0.001f, 10000.0f, 0u, h)) return false;
     const uint32_t primitive = h.primitive;
     const float3 p0 = xyz(__ldg(s.vertices + __ldg(s.indices + primitive * 3u + 0u)));
     const float3 p1 = xyz(__ldg(s.vertices + __ldg(s.indices + primitive * 3u + 1u)));
@@ -263,6 +265,7 @@ __device__ bool traceOpaqueBoundary(const DeviceScene& s, PathBuffers& p, float3
     return true;
 }
 
+template <int kInst = -1>
 __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float3 entry, float3 outwardNormal,
                                      float meanFreePath, float albedo, float anisotropy, uint32_t& state,
                                      float3& exitOrigin, float3& exitDirection, float& attenuation)
@@ -277,7 +280,7 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
     for (int step = 0; step < 8; ++step) {
         float3 boundary, boundaryNormal;
         float boundaryDistance;
-        if (!traceOpaqueBoundary(s, p, origin, direction, boundary, boundaryNormal, boundaryDistance)) return false;
+        if (!traceOpaqueBoundary<kInst>(s, p, origin, direction, boundary, boundaryNormal, boundaryDistance)) return false;
         const float scatterDistance = -glog(gmax(1.0f - randomFloat(state), 1e-6f)) / sigmaS;
         const bool forceExit = step == 7;
         const float travel = forceExit ? boundaryDistance : gmin(scatterDistance, boundaryDistance);
@@ -944,6 +947,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
 // a walk whose boundary ray escapes stores its RNG state and queues the path
 // for shadeKernel<..., kWalkReplay>, which finishes the bounce the inline way.
 // ---------------------------------------------------------------------------
+template <int kInst>
 __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS)
     walkKernel(DeviceScene s, PathBuffers p, const uint32_t* walks, uint32_t* nextQueue, uint32_t* nextCount,
                uint32_t* replayQueue)
@@ -957,7 +961,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS)
         uint32_t rng = __float_as_uint(state.y);
         float3 exitOrigin, exitDirection;
         float attenuation;
-        if (randomWalkSubsurface(s, p, xyz(entry), xyz(outward), entry.w, outward.w, state.x, rng, exitOrigin,
+        if (randomWalkSubsurface<kInst>(s, p, xyz(entry), xyz(outward), entry.w, outward.w, state.x, rng, exitOrigin,
                                  exitDirection, attenuation)) {
             p.rng[slot] = rng;
             p.throughput[slot] = state.z * attenuation;
@@ -1006,7 +1010,7 @@ __global__ void __launch_bounds__(128) missKernel(DeviceScene s, FrameConst f, P
 // ---------------------------------------------------------------------------
 // shadow: visibility of light samples (vulkan_path_tracer.cpp:855-912)
 // ---------------------------------------------------------------------------
-template <bool kOpaque, bool kCount>
+template <bool kOpaque, bool kCount, int kInst>
 __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(DeviceScene s, PathBuffers p)
 {
     const uint32_t n = p.counters[2];
@@ -1025,7 +1029,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(Devic
         const float tmax = o.w;
         HitRecord h;
         if (kind == kShadowMesh) {
-            const bool occluded = traceRay<kMode, true, kCount>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+            const bool occluded = traceRay<kMode, true, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
             if (occluded) p.contributionValid[k * p.capacity + slot] = 0;
             else p.contribution[k * p.capacity + slot] = d.w * fct.x;
             continue;
@@ -1036,10 +1040,10 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(Devic
         bool hitSomething;
         float hitDistance = 0.0f;
         if (falloff) {
-            hitSomething = traceRay<kMode, false, kCount>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+            hitSomething = traceRay<kMode, false, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
             hitDistance = h.t;
         } else {
-            hitSomething = traceRay<kMode, true, kCount>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+            hitSomething = traceRay<kMode, true, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
         }
         if (hitSomething) {
             float strength = 1.0f;
@@ -1388,6 +1392,31 @@ __global__ void __launch_bounds__(256) sortRaysKernel(PathBuffers p, uint32_t* q
     }
 }
 
+template <int kInst>
+void launchExtend(const DeviceScene& scene, PathBuffers& paths, const uint32_t* inQueue, const uint32_t* inCount,
+                  bool count, int grid, cudaStream_t stream)
+{
+    if (count) {
+        if (scene.opaque) extendKernel<Accept::Opaque, true, kInst><<<grid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
+        else extendKernel<Accept::Stochastic, true, kInst><<<grid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
+    } else {
+        if (scene.opaque) extendKernel<Accept::Opaque, false, kInst><<<grid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
+        else extendKernel<Accept::Stochastic, false, kInst><<<grid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
+    }
+}
+
+template <int kInst>
+void launchShadow(const DeviceScene& scene, PathBuffers& paths, bool count, int grid, cudaStream_t stream)
+{
+    if (count) {
+        if (scene.opaque) shadowKernel<true, true, kInst><<<grid, 128, 0, stream>>>(scene, paths);
+        else shadowKernel<false, true, kInst><<<grid, 128, 0, stream>>>(scene, paths);
+    } else {
+        if (scene.opaque) shadowKernel<true, false, kInst><<<grid, 128, 0, stream>>>(scene, paths);
+        else shadowKernel<false, false, kInst><<<grid, 128, 0, stream>>>(scene, paths);
+    }
+}
+
 // Whether the full shade kernel defers subsurface walks to walkKernel: the
 // plain (non-cache) mode with walk buffers.
 bool deferWalks(const PathBuffers& paths, bool cacheMode)
@@ -1467,13 +1496,8 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
                 launched += 1;
             }
             timed(0, [&] {
-                if (countTraversal) {
-                    if (scene.opaque) extendKernel<Accept::Opaque, true><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
-                    else extendKernel<Accept::Stochastic, true><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
-                } else {
-                    if (scene.opaque) extendKernel<Accept::Opaque, false><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
-                    else extendKernel<Accept::Stochastic, false><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, inCount);
-                }
+                if (scene.instances) launchExtend<1>(scene, paths, inQueue, inCount, countTraversal, traceGrid, stream);
+                else launchExtend<0>(scene, paths, inQueue, inCount, countTraversal, traceGrid, stream);
             });
             CUDA_OK(cudaGetLastError());
             CUDA_OK(cudaMemsetAsync(outCount, 0, sizeof(uint32_t), stream));
@@ -1494,7 +1518,8 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
                     // The deferred walks (in this bounce's traced extension
                     // queue), then the failed ones re-shaded (queued in the
                     // miss queue, which missKernel has consumed).
-                    walkKernel<<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, outQueue, outCount, paths.missQueue);
+                    if (scene.instances) walkKernel<1><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, outQueue, outCount, paths.missQueue);
+                    else walkKernel<0><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, outQueue, outCount, paths.missQueue);
                     const bool lit = scene.lightCount > 0u && !scene.hasMeshLights;
                     if (lit) {
                         shadeKernel<true, true, false, kWalkReplay><<<missGrid, 128, 0, stream>>>(
@@ -1507,13 +1532,8 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
             });
             CUDA_OK(cudaGetLastError());
             timed(2, [&] {
-                if (countTraversal) {
-                    if (scene.opaque) shadowKernel<true, true><<<traceGrid, 128, 0, stream>>>(scene, paths);
-                    else shadowKernel<false, true><<<traceGrid, 128, 0, stream>>>(scene, paths);
-                } else {
-                    if (scene.opaque) shadowKernel<true, false><<<traceGrid, 128, 0, stream>>>(scene, paths);
-                    else shadowKernel<false, false><<<traceGrid, 128, 0, stream>>>(scene, paths);
-                }
+                if (scene.instances) launchShadow<1>(scene, paths, countTraversal, traceGrid, stream);
+                else launchShadow<0>(scene, paths, countTraversal, traceGrid, stream);
             });
             CUDA_OK(cudaGetLastError());
             launched += (sortHits ? 7 : 4) + (walks ? 2 : 0);

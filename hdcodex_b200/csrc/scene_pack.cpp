@@ -169,7 +169,160 @@ void writeDefaultMaterial(std::vector<uint8_t>& out, const std::array<float, 3>&
     for (int i = 0; i < 6; ++i) w.u(kMissing, kMissing, kMissing, kMissing);
 }
 
+// A flattened instanced mesh: owned arrays behind an hdcx_mesh_desc.
+struct FlatMesh {
+    std::vector<float> positions, texcoords, normals;
+    std::vector<uint32_t> indices;
+    std::vector<const char*> triangleMaterialIds;
+    hdcx_mesh_desc desc{};
+};
+
+// Row-vector affine transform of a point in binary64 (mesh.cpp:964-969).
+void transformPoint(const double* m, double x, double y, double z, double out[3])
+{
+    for (int j = 0; j < 3; ++j) out[j] = ((x * m[j] + y * m[4 + j]) + z * m[8 + j]) + m[12 + j];
+}
+
+// inverse(A) of the upper 3x3 (rows A[i] = m[4i..4i+2]) by cofactors.
+void inverse3(const double* m, double inv[9])
+{
+    const double a00 = m[0], a01 = m[1], a02 = m[2];
+    const double a10 = m[4], a11 = m[5], a12 = m[6];
+    const double a20 = m[8], a21 = m[9], a22 = m[10];
+    const double c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
+    const double det = (a00 * c00 + a01 * c01) + a02 * c02;
+    inv[0] = c00 / det;
+    inv[1] = (a02 * a21 - a01 * a22) / det;
+    inv[2] = (a01 * a12 - a02 * a11) / det;
+    inv[3] = c01 / det;
+    inv[4] = (a00 * a22 - a02 * a20) / det;
+    inv[5] = (a02 * a10 - a00 * a12) / det;
+    inv[6] = c02 / det;
+    inv[7] = (a01 * a20 - a00 * a21) / det;
+    inv[8] = (a00 * a11 - a01 * a10) / det;
+}
+
+void checkAffine(const double* m)
+{
+    if (m[3] != 0.0 || m[7] != 0.0 || m[11] != 0.0 || m[15] != 1.0)
+        throw std::invalid_argument("instancer: transforms must be affine (column 3 = 0, 0, 0, 1)");
+}
+
+// mesh.cpp:955-1004 for one instanced mesh.
+void flattenInstancer(const hdcx_mesh_desc& m, const double* transforms, uint64_t count, FlatMesh& f)
+{
+    const uint64_t points = m.position_count / 3u;
+    const uint64_t triangles = m.index_count / 3u;
+    const uint64_t cornerNormals = m.normals ? m.normal_count / 3u : 0u;
+    for (uint64_t inst = 0; inst < count; ++inst) {
+        const double* T = transforms + 16u * inst;
+        checkAffine(T);
+        double inv[9];
+        inverse3(T, inv);
+        const uint32_t vertexBase = static_cast<uint32_t>(f.positions.size() / 3u);
+        for (uint64_t p = 0; p < points; ++p) {
+            double w[3];
+            transformPoint(T, m.positions[3 * p], m.positions[3 * p + 1], m.positions[3 * p + 2], w);
+            for (double c : w) f.positions.push_back(static_cast<float>(c));
+        }
+        for (uint64_t t = 0; t < triangles; ++t) {
+            bool valid = true;
+            for (int c = 0; c < 3; ++c) valid = valid && m.indices[3 * t + c] < points;
+            if (!valid) continue;
+            f.triangleMaterialIds.push_back(m.triangle_material_ids && t < m.triangle_material_id_count
+                                                ? m.triangle_material_ids[t]
+                                                : m.material_id);
+            for (int c = 0; c < 3; ++c) {
+                f.indices.push_back(vertexBase + m.indices[3 * t + c]);
+                const uint64_t corner = 3 * t + c, uv = corner * 2u;
+                const bool hasUv = m.texcoords && uv + 1u < m.texcoord_count;
+                f.texcoords.push_back(hasUv ? m.texcoords[uv] : 0.0F);
+                f.texcoords.push_back(hasUv ? m.texcoords[uv + 1] : 0.0F);
+                double n[3] = {0.0, 0.0, 0.0};
+                if (corner < cornerNormals) {
+                    const double nx = m.normals[3 * corner], ny = m.normals[3 * corner + 1], nz = m.normals[3 * corner + 2];
+                    for (int j = 0; j < 3; ++j) n[j] = (nx * inv[3 * j] + ny * inv[3 * j + 1]) + nz * inv[3 * j + 2];
+                    const double length = std::sqrt((n[0] * n[0] + n[1] * n[1]) + n[2] * n[2]);
+                    const double d = length > 1e-10 ? length : 1e-10;
+                    for (double& x : n) x = length <= 1e-12 ? 0.0 : x / d;
+                }
+                for (double x : n) f.normals.push_back(static_cast<float>(x));
+            }
+        }
+    }
+    f.desc = m;
+    f.desc.positions = f.positions.data();
+    f.desc.position_count = f.positions.size();
+    f.desc.indices = f.indices.data();
+    f.desc.index_count = f.indices.size();
+    f.desc.texcoords = f.texcoords.data();
+    f.desc.texcoord_count = f.texcoords.size();
+    f.desc.normals = f.normals.data();
+    f.desc.normal_count = f.normals.size();
+    f.desc.triangle_material_ids = f.triangleMaterialIds.data();
+    f.desc.triangle_material_id_count = f.triangleMaterialIds.size();
+}
+
+// The emissive-triangle CDF (vulkan_path_tracer.cpp:2944-2993): binary64
+// areas and weights, entry (cdf, probability / area, area, 0) per triangle.
+void computeEmissive(PackedSceneData& out)
+{
+    const size_t n = out.triangleMaterials.size();
+    out.emissive.assign(n * 4u, 0.0F);
+    std::vector<double> weight(n, 0.0);
+    std::vector<float> area(n, 0.0F);
+    double total = 0.0;
+    for (size_t p = 0; p < n; ++p) {
+        const float* a = &out.vertices[size_t(out.indices[3 * p]) * 4u];
+        const float* b = &out.vertices[size_t(out.indices[3 * p + 1]) * 4u];
+        const float* c = &out.vertices[size_t(out.indices[3 * p + 2]) * 4u];
+        const double e1x = static_cast<double>(b[0]) - a[0], e1y = static_cast<double>(b[1]) - a[1],
+                     e1z = static_cast<double>(b[2]) - a[2];
+        const double e2x = static_cast<double>(c[0]) - a[0], e2y = static_cast<double>(c[1]) - a[1],
+                     e2z = static_cast<double>(c[2]) - a[2];
+        const double cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+        const float ar = static_cast<float>(0.5 * std::sqrt(cx * cx + cy * cy + cz * cz));
+        area[p] = std::isfinite(ar) ? ar : 0.0F;
+        const uint32_t mat = out.triangleMaterials[p];
+        const float power = mat < out.materialEmission.size() ? out.materialEmission[mat] : 0.0F;
+        const double w = static_cast<double>(area[p]) * static_cast<double>(power);
+        if (w > 0.0 && std::isfinite(w)) {
+            weight[p] = w;
+            total += w;
+        }
+    }
+    if (total > 0.0 && std::isfinite(total)) {
+        double cdf = 0.0;
+        for (size_t p = 0; p < n; ++p) {
+            const double probability = weight[p] / total;
+            cdf += probability;
+            float* e = &out.emissive[p * 4u];
+            e[0] = static_cast<float>(p + 1u == n ? 1.0 : cdf);
+            e[1] = area[p] > 0.0F ? static_cast<float>(probability) / area[p] : 0.0F;
+            e[2] = area[p];
+            e[3] = 0.0F;
+        }
+    }
+}
+
 }  // namespace
+
+std::vector<float> instancerWorldPoints(const PackedInstancer& ins)
+{
+    std::vector<float> out;
+    out.reserve(size_t(ins.instanceCount) * ins.pointCount() * 4u);
+    for (uint32_t inst = 0; inst < ins.instanceCount; ++inst) {
+        const double* T = ins.transforms.data() + 16u * inst;
+        for (uint32_t p = 0; p < ins.pointCount(); ++p) {
+            double w[3];
+            transformPoint(T, ins.points[4 * p], ins.points[4 * p + 1], ins.points[4 * p + 2], w);
+            out.insert(out.end(), {static_cast<float>(w[0]), static_cast<float>(w[1]), static_cast<float>(w[2]), 1.0F});
+        }
+    }
+    return out;
+}
+
+void recomputeEmissive(PackedSceneData& data) { computeEmissive(data); }
 
 void srgbTable(float table[256])
 {
@@ -179,9 +332,30 @@ void srgbTable(float table[256])
     }
 }
 
-PackedSceneData packScene(const hdcx_scene_desc& snap)
+PackedSceneData packScene(const hdcx_scene_desc& scene, const hdcx_instancer_desc* instancers, uint64_t instancerCount)
 {
     PackedSceneData out;
+    // Instanced meshes are flattened first; the rest of the packing sees the
+    // flattened snapshot.
+    hdcx_scene_desc snap = scene;
+    std::vector<hdcx_mesh_desc> meshes;
+    std::vector<FlatMesh> flat(instancerCount);
+    std::vector<int> instancerOfMesh(scene.mesh_count, -1);
+    if (instancerCount > 0) {
+        if (!instancers) throw std::invalid_argument("instancer array is null");
+        meshes.assign(scene.meshes, scene.meshes + scene.mesh_count);
+        for (uint64_t k = 0; k < instancerCount; ++k) {
+            const hdcx_instancer_desc& ins = instancers[k];
+            if (ins.mesh_index >= scene.mesh_count) throw std::invalid_argument("instancer: mesh_index out of range");
+            if (instancerOfMesh[ins.mesh_index] >= 0)
+                throw std::invalid_argument("instancer: a mesh is instanced by more than one instancer");
+            if (ins.instance_count > 0 && !ins.transforms) throw std::invalid_argument("instancer: transforms are null");
+            instancerOfMesh[ins.mesh_index] = static_cast<int>(k);
+            flattenInstancer(scene.meshes[ins.mesh_index], ins.transforms, ins.instance_count, flat[k]);
+            meshes[ins.mesh_index] = flat[k].desc;
+        }
+        snap.meshes = meshes.data();
+    }
     out.opaque = true;
     for (uint64_t i = 0; i < snap.material_count; ++i) {
         const hdcx_material_desc& m = snap.materials[i];
@@ -353,6 +527,24 @@ PackedSceneData packScene(const hdcx_scene_desc& snap)
     for (uint64_t mi = 0; mi < snap.mesh_count; ++mi) {
         const hdcx_mesh_desc& mesh = snap.meshes[mi];
         const uint32_t base = out.vertexCount();
+        if (instancerCount > 0 && instancerOfMesh[mi] >= 0) {
+            const hdcx_instancer_desc& ins = instancers[instancerOfMesh[mi]];
+            const hdcx_mesh_desc& proto = scene.meshes[mi];
+            PackedInstancer pi;
+            pi.mesh = static_cast<uint32_t>(mi);
+            const uint64_t points = proto.position_count / 3u;
+            for (uint64_t p = 0; p < points; ++p)
+                pi.points.insert(pi.points.end(), {proto.positions[3 * p], proto.positions[3 * p + 1], proto.positions[3 * p + 2], 1.0F});
+            for (uint64_t t = 0; t + 2 < proto.index_count; t += 3) {
+                if (proto.indices[t] < points && proto.indices[t + 1] < points && proto.indices[t + 2] < points)
+                    pi.indices.insert(pi.indices.end(), {proto.indices[t], proto.indices[t + 1], proto.indices[t + 2]});
+            }
+            pi.transforms.assign(ins.transforms, ins.transforms + 16u * ins.instance_count);
+            pi.instanceCount = static_cast<uint32_t>(ins.instance_count);
+            pi.firstTriangle = out.triangleCount();
+            pi.firstVertex = base;
+            if (pi.instanceCount > 0 && !pi.indices.empty()) out.instancers.push_back(std::move(pi));
+        }
         for (uint64_t i = 0; i + 2 < mesh.position_count; i += 3) {
             out.vertices.insert(out.vertices.end(), {mesh.positions[i], mesh.positions[i + 1], mesh.positions[i + 2], 1.0F});
         }
@@ -406,42 +598,8 @@ PackedSceneData packScene(const hdcx_scene_desc& snap)
         out.geometryReady = false;
         return out;
     }
-    const size_t n = out.triangleMaterials.size();
-    out.emissive.assign(n * 4u, 0.0F);
-    std::vector<double> weight(n, 0.0);
-    std::vector<float> area(n, 0.0F);
-    double total = 0.0;
-    for (size_t p = 0; p < n; ++p) {
-        const float* a = &out.vertices[size_t(out.indices[3 * p]) * 4u];
-        const float* b = &out.vertices[size_t(out.indices[3 * p + 1]) * 4u];
-        const float* c = &out.vertices[size_t(out.indices[3 * p + 2]) * 4u];
-        const double e1x = static_cast<double>(b[0]) - a[0], e1y = static_cast<double>(b[1]) - a[1],
-                     e1z = static_cast<double>(b[2]) - a[2];
-        const double e2x = static_cast<double>(c[0]) - a[0], e2y = static_cast<double>(c[1]) - a[1],
-                     e2z = static_cast<double>(c[2]) - a[2];
-        const double cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
-        const float ar = static_cast<float>(0.5 * std::sqrt(cx * cx + cy * cy + cz * cz));
-        area[p] = std::isfinite(ar) ? ar : 0.0F;
-        const uint32_t mat = out.triangleMaterials[p];
-        const float power = mat < emissionPower.size() ? emissionPower[mat] : 0.0F;
-        const double w = static_cast<double>(area[p]) * static_cast<double>(power);
-        if (w > 0.0 && std::isfinite(w)) {
-            weight[p] = w;
-            total += w;
-        }
-    }
-    if (total > 0.0 && std::isfinite(total)) {
-        double cdf = 0.0;
-        for (size_t p = 0; p < n; ++p) {
-            const double probability = weight[p] / total;
-            cdf += probability;
-            float* e = &out.emissive[p * 4u];
-            e[0] = static_cast<float>(p + 1u == n ? 1.0 : cdf);
-            e[1] = area[p] > 0.0F ? static_cast<float>(probability) / area[p] : 0.0F;
-            e[2] = area[p];
-            e[3] = 0.0F;
-        }
-    }
+    out.materialEmission = emissionPower;
+    computeEmissive(out);
     out.geometryReady = true;
     return out;
 }

@@ -88,6 +88,11 @@ SIGNATURES = {
     "hdcx_set_device_memory_limit": (C.c_int, [C.c_int32, C.c_uint64]),
     "hdcx_get_device_memory_usage": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hdcx_test_break_bvh": (C.c_int, [_P]),
+    "hdcx_pack_scene_instanced": (C.c_int, [C.c_void_p, C.POINTER(_abi.InstancerDesc), C.c_uint64,
+                                            C.POINTER(C.c_void_p)]),
+    "hdcx_set_scene_instanced": (C.c_int, [_P, C.c_void_p, C.POINTER(_abi.InstancerDesc), C.c_uint64]),
+    "hdcx_update_instancer_points": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_float), C.c_uint64]),
+    "hdcx_get_scene_info": (C.c_int, [_P, C.POINTER(_abi.SceneInfo)]),
     "hdcx_get_batch_graph_stats": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hdcx_render_preview": (C.c_int, [_P, C.POINTER(_abi.Camera), C.c_uint32, C.c_uint32, C.c_void_p,
                                       C.POINTER(C.c_int32)]),
@@ -195,7 +200,23 @@ class PathTracer:
             self._check(lib().hdcx_set_scene(self._h, None), "set_scene")
             return
         holder = scene.to_desc()
-        self._check(lib().hdcx_set_scene(self._h, C.cast(holder.pointer(), C.c_void_p)), "set_scene")
+        if holder.instancer_count:
+            self._check(lib().hdcx_set_scene_instanced(self._h, C.cast(holder.pointer(), C.c_void_p), holder.instancers,
+                                                       holder.instancer_count), "set_scene")
+        else:
+            self._check(lib().hdcx_set_scene(self._h, C.cast(holder.pointer(), C.c_void_p)), "set_scene")
+
+    def update_instancer_points(self, instancer: int, positions):
+        """hdcx_update_instancer_points: new object-space points (3 floats each)."""
+        p = np.ascontiguousarray(np.asarray(positions, dtype=np.float32).reshape(-1))
+        self._check(lib().hdcx_update_instancer_points(self._h, instancer, p.ctypes.data_as(C.POINTER(C.c_float)),
+                                                       p.size), "update_instancer_points")
+
+    def scene_info(self) -> dict:
+        """hdcx_get_scene_info: triangles, instances, bottom levels, BVH and scene bytes, build times."""
+        info = _abi.SceneInfo()
+        self._check(lib().hdcx_get_scene_info(self._h, C.byref(info)), "get_scene_info")
+        return {name: getattr(info, name) for name, _ in _abi.SceneInfo._fields_}
 
     def set_shading_mode(self, mode: int):
         if mode == RASTER_PREVIEW:
@@ -457,7 +478,8 @@ def pack_scene(scene: Scene) -> dict:
     """Host packing of a snapshot (no device needed), as numpy arrays."""
     holder = scene.to_desc()
     handle = C.c_void_p()
-    status = lib().hdcx_pack_scene(C.cast(holder.pointer(), C.c_void_p), C.byref(handle))
+    status = lib().hdcx_pack_scene_instanced(C.cast(holder.pointer(), C.c_void_p), holder.instancers,
+                                             holder.instancer_count, C.byref(handle))
     if status != 0:
         raise RuntimeError(f"hdcx_pack_scene failed: {STATUS.get(status, status)}")
     try:

@@ -183,7 +183,15 @@ def _dome_texture(width, height, seed, hotspots=3, sigma=2.0) -> np.ndarray:
 
 
 def heavy_geometry(width=1920, height=1080, spp=64, max_bounces=8, seed=0, sphere_level=3,
-                   grid_vertices=581, dome_size=(2048, 1024)) -> Workload:
+                   grid_vertices=581, dome_size=(2048, 1024), instanced=False) -> Workload:
+    """The 1.0M-triangle scene: a noise-displaced heightfield and 256 displaced
+    icospheres, lit by a lat-long HDR dome. With instanced=True the spheres are
+    instances (hdcx_instancer_desc) of four displaced icosphere prototypes,
+    each with its own uniform scale, rotation about y and position: the same
+    triangle count and layout, given as instancers instead of flattened
+    copies."""
+    if instanced:
+        return _heavy_instanced(width, height, spp, max_bounces, seed, sphere_level, grid_vertices, dome_size)
     rng = np.random.default_rng(seed)
     s = Scene(revision=1)
     # Material palette: Lambert, GGX dielectric (reflective over diffuse), GGX conductor.
@@ -249,6 +257,36 @@ def heavy_geometry(width=1920, height=1080, spp=64, max_bounces=8, seed=0, spher
     s.lights.append(Light(id="/dome", type=DOME, intensity=1.0, texture="dome#hdr", texture_format=LATLONG))
     cam = look_at_camera((0.0, 7.5, 17.0), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), 45.0, width / height)
     return Workload("heavy-geometry-1.0M-tri-dome", s, cam, width, height, spp, max_bounces)
+
+
+def _heavy_instanced(width, height, spp, max_bounces, seed, sphere_level, grid_vertices, dome_size) -> Workload:
+    from .scene import Instancer
+    flat = heavy_geometry(width, height, spp, max_bounces, seed, sphere_level, grid_vertices, dome_size)
+    s = flat.scene
+    s.meshes = [m for m in s.meshes if m.id != "/spheres"]
+    rng = np.random.default_rng(seed + 101)
+    ids = [m.id for m in s.materials]
+    base_v, base_f = _icosphere(sphere_level)
+    protos = 4
+    for k in range(protos):
+        disp = 1.0 + 0.18 * _noise3(base_v * 2.0, rng, 3)
+        v = (base_v * disp[:, None]).astype(np.float32)
+        tri_ids = [ids[int(i)] for i in rng.integers(0, len(ids), size=len(base_f))]
+        s.meshes.append(Mesh(id=f"/sphere{k}", positions=v.ravel(), indices=base_f.astype(np.uint32).ravel(),
+                             material_id="/lambert0", triangle_material_ids=tri_ids))
+    transforms = [[] for _ in range(protos)]
+    for k in range(256):
+        gx, gz = k % 16, k // 16
+        cx = -10.5 + gx * 1.4 + rng.uniform(-0.3, 0.3)
+        cz = -10.5 + gz * 1.4 + rng.uniform(-0.3, 0.3)
+        r = rng.uniform(0.25, 0.55)
+        th = rng.uniform(0.0, 2.0 * np.pi)
+        c, sn = np.cos(th), np.sin(th)
+        M = np.array([[r * c, 0.0, -r * sn, 0.0], [0.0, r, 0.0, 0.0], [r * sn, 0.0, r * c, 0.0],
+                      [cx, 1.2 + r, cz, 1.0]], dtype=np.float64)
+        transforms[k % protos].append(M)
+    s.instancers = [Instancer(f"/sphere{k}", np.array(transforms[k])) for k in range(protos)]
+    return Workload("heavy-geometry-1.0M-tri-instanced", s, flat.camera, width, height, spp, max_bounces)
 
 
 def _torus(major: float, minor: float, segments: int, rings: int):

@@ -246,6 +246,28 @@ typedef struct hdcx_scene_desc {
     uint64_t light_count;
 } hdcx_scene_desc;
 
+/* An instancer: mesh `mesh_index` of the scene, given in object space, drawn
+ * once per transform. No counterpart in the reference's scene ABI: its Hydra
+ * mesh adapter flattens an instanced mesh into world-space copies before the
+ * tracer sees it (mesh.cpp:955-1004). hdcx_set_scene_instanced renders the
+ * scene exactly as hdcx_set_scene renders that flattened scene (same
+ * triangles, ids, images), with one bottom-level BVH per instanced mesh under
+ * a top-level BVH of instances instead of one BVH over every copy.
+ * Transforms are affine 4x4 matrices, 16 doubles each, row-major in the
+ * row-vector convention of the reference's Gf matrices (world = [p 1] M; the
+ * translation in elements 12..14; column 3 must be (0, 0, 0, 1)). The
+ * flattening, per instance in order and then per valid triangle: positions
+ * ((x*m00 + y*m10) + z*m20) + m30 (likewise y, z) in binary64 rounded to
+ * float; corner normals n' = n inverse(A) (A the upper 3x3, inverse by
+ * cofactors / determinant) normalised in binary64 (divided by max(length,
+ * 1e-10), zero when length <= 1e-12) and rounded; texcoords and per-triangle
+ * materials copied. */
+typedef struct hdcx_instancer_desc {
+    uint64_t mesh_index;
+    const double* transforms;
+    uint64_t instance_count;
+} hdcx_instancer_desc;
+
 /* Device records, byte-identical to the reference's GpuMaterial (23 x 16 B,
  * vulkan_path_tracer.cpp:1907-1933) and GpuLight (14 x 16 B, :1935-1952). */
 #define HDCX_GPU_MATERIAL_BYTES 368u
@@ -401,9 +423,45 @@ HDCX_API hdcx_status hdcx_set_scene(hdcx_tracer* tracer, const hdcx_scene_desc* 
 /* Uploads an already packed scene (a caller that packs on its own side). */
 HDCX_API hdcx_status hdcx_set_scene_packed(hdcx_tracer* tracer, const hdcx_packed_scene* scene);
 
+/* hdcx_set_scene with instancers (hdcx_instancer_desc): the meshes they name
+ * are given in object space and drawn once per transform. Same triangles,
+ * flattened ids and images as hdcx_set_scene of the flattened scene; the
+ * acceleration structure is two-level: one 8-wide BVH per instanced mesh
+ * (object space) and one over the other triangles (world space), under a
+ * top-level BVH of instances. Invalid or singular transforms give
+ * HDCX_ERROR_INVALID_ARGUMENT. */
+HDCX_API hdcx_status hdcx_set_scene_instanced(hdcx_tracer* tracer, const hdcx_scene_desc* scene,
+                                              const hdcx_instancer_desc* instancers, uint64_t instancer_count);
+
+/* Moves the object-space points of instancer `instancer` (its index in the
+ * last hdcx_set_scene_instanced call; position_count = 3 x its point count)
+ * for a deforming mesh: the flattened world vertices of all its instances and
+ * the emissive-triangle CDF are recomputed, its bottom-level BVH is refitted
+ * (same topology, boxes and quantisation recomputed level by level from the
+ * leaves up) and the top-level BVH is rebuilt. Corner normals, texcoords and
+ * materials are kept. Renders afterwards equal those of the flattened scene
+ * with the moved points. */
+HDCX_API hdcx_status hdcx_update_instancer_points(hdcx_tracer* tracer, uint64_t instancer, const float* positions,
+                                                  uint64_t position_count);
+
+/* Size and build cost of the current scene. */
+typedef struct hdcx_scene_info {
+    uint64_t triangles;      /* flattened triangles */
+    uint64_t instances;      /* top-level leaves (0: a single-level scene) */
+    uint64_t bottom_levels;  /* bottom-level BVHs */
+    uint64_t bvh_bytes;      /* nodes and leaf triangle copies of every BVH */
+    uint64_t scene_bytes;    /* every device buffer of the scene, BVHs included */
+    double build_ms;         /* host wall time of the last set_scene: packing, upload, BVH builds */
+    double bvh_build_ms;     /* of which the BVH builds */
+} hdcx_scene_info;
+HDCX_API hdcx_status hdcx_get_scene_info(const hdcx_tracer* tracer, hdcx_scene_info* info);
+
 /* Packs a snapshot on the host without a device; the view stays valid until
  * hdcx_packing_destroy. Used to check the packing against the reference rules. */
 HDCX_API hdcx_status hdcx_pack_scene(const hdcx_scene_desc* scene, hdcx_packing** packing);
+/* hdcx_pack_scene with instancers: the packing of the flattened scene. */
+HDCX_API hdcx_status hdcx_pack_scene_instanced(const hdcx_scene_desc* scene, const hdcx_instancer_desc* instancers,
+                                               uint64_t instancer_count, hdcx_packing** packing);
 HDCX_API const hdcx_packed_scene* hdcx_packing_view(const hdcx_packing* packing);
 HDCX_API void hdcx_packing_destroy(hdcx_packing* packing);
 

@@ -75,6 +75,8 @@ class OracleTracer:
         if scene is None:
             lib().oracle_set_scene(self._h, None)
             return
+        if scene.instancers:  # the oracle renders the flattened scene (hdcx_instancer_desc)
+            scene = scene.flattened()
         holder = scene.to_desc()
         lib().oracle_set_scene(self._h, C.cast(holder.pointer(), C.c_void_p))
 

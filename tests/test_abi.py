@@ -90,7 +90,7 @@ def test_raster_preview_is_rejected_without_a_device(hdcx_lib):
 
 C_STRUCT_NAMES = ["hdcx_camera", "hdcx_mesh_desc", "hdcx_material_desc", "hdcx_texture_desc", "hdcx_light_desc",
                   "hdcx_scene_desc", "hdcx_packed_texture", "hdcx_packed_scene", "hdcx_render_stats",
-                  "hdcx_batch_job", "hdcx_nrc_config", "hdcx_tuning"]
+                  "hdcx_batch_job", "hdcx_nrc_config", "hdcx_tuning", "hdcx_instancer_desc", "hdcx_scene_info"]
 
 
 def test_struct_fields_match_the_header(tmp_path):
