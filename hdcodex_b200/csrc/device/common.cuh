@@ -135,7 +135,8 @@ struct InstanceDesc {
     float pad0, pad1, pad2;
 };
 
-// DeviceScene::status bits.
+// Traversal fault bits (a traversal's `fault` out-parameter; the kernels OR
+// them into the render's counters[7], which the host reads back).
 constexpr unsigned int kTraversalOverflow = 1u;  // a pending node group found the stack full and was dropped
 constexpr unsigned int kTraversalBudget = 2u;    // a traversal visited more nodes than the BVH holds
 
@@ -165,10 +166,6 @@ struct DeviceScene {
     const InstanceDesc* instances;  // null: single-level scene
     const BlasDesc* blases;
     uint32_t instanceCount;
-    // Traversal faults of the current render (kTraversalOverflow,
-    // kTraversalBudget; null: not recorded). Set per render to a word the
-    // host reads back with the render's counters.
-    unsigned int* status;
 };
 
 // Per-render constants: the reference's CameraBlock (vulkan_path_tracer.cpp:91-98)

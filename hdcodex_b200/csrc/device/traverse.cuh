@@ -29,8 +29,9 @@
 //   not depend on the order of the tests.
 // * Faults: a node group that finds the stack full, or a traversal that
 //   visits more nodes than the BVH holds (a malformed node array), sets a
-//   bit in DeviceScene::status, which the host reports as an error of the
-//   render.
+//   bit in the traversal's fault word; the kernels OR it into the render's
+//   counters once per thread, outside their loops, and the host reports it
+//   as an error of the render.
 #pragma once
 
 #include "common.cuh"
@@ -49,10 +50,6 @@ constexpr uint32_t kPostponeLanes = HDCX_POSTPONE_LANES;
 // need at most one entry per BVH level, which the build caps at 64).
 constexpr int kPostponeDepth = 32;
 
-HDCX_D void traversalFault(const DeviceScene& s, unsigned int code)
-{
-    if (s.status != nullptr) atomicOr(s.status, code);
-}
 
 enum class Accept : int {
     Opaque = 0,      // every candidate is confirmed
@@ -172,6 +169,7 @@ struct Traversal {
     int sp;
     uint32_t budget;  // every node is entered at most once; guards against a malformed node array
     uint32_t rayRng;
+    uint32_t fault;   // kTraversalOverflow | kTraversalBudget
 };
 
 enum : int { kStepContinue = 0, kStepDone = 1, kStepAnyHit = 2 };
@@ -196,6 +194,7 @@ HDCX_D void beginTraversal(Traversal& st, const DeviceScene& s, float3 o, float3
     st.sp = 0;
     st.budget = s.nodeCount + 1u;
     st.rayRng = rayRng;
+    st.fault = 0u;
 }
 
 // Tests the eight children of node `nodeIndex` against a ray (origin o,
@@ -321,7 +320,7 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
         st.nodeGroup = entry;
     }
     if (st.budget-- == 0u) {
-        traversalFault(s, kTraversalBudget);
+        st.fault |= kTraversalBudget;
         return kStepDone;
     }
     // Next child of the current group, nearest octant first.
@@ -333,7 +332,7 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
     const uint32_t nodeIndex = st.nodeGroup.x + __popc(parentMask & ((1u << childSlot) - 1u));
     if ((st.nodeGroup.y & 0xff000000u) != 0u) {
         if (st.sp < kTraversalStack) stack[st.sp++] = st.nodeGroup;
-        else traversalFault(s, kTraversalOverflow);
+        else st.fault |= kTraversalOverflow;
     }
 
     if (kCount) work->x++;
@@ -397,7 +396,7 @@ HDCX_D float maxAbs3(float3 v) { return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fab
 // Pops the next child node of `group` (nearest octant first), pushing the
 // rest of the group. Returns false when the group and the stack are empty.
 HDCX_D bool nextNode(uint2& group, uint2* stack, int& sp, int capacity, uint32_t octInv, uint32_t& nodeIndex,
-                     const DeviceScene& s)
+                     uint32_t& fault)
 {
     if ((group.y & 0xff000000u) == 0u) {
         if (sp == 0) return false;
@@ -410,7 +409,7 @@ HDCX_D bool nextNode(uint2& group, uint2* stack, int& sp, int capacity, uint32_t
     nodeIndex = group.x + __popc((group.y & 0xffu) & ((1u << childSlot) - 1u));
     if ((group.y & 0xff000000u) != 0u) {
         if (sp < capacity) stack[sp++] = group;
-        else traversalFault(s, kTraversalOverflow);
+        else fault |= kTraversalOverflow;
     }
     return true;
 }
@@ -419,7 +418,7 @@ HDCX_D bool nextNode(uint2& group, uint2* stack, int& sp, int capacity, uint32_t
 // candidate, else updates `best`.
 template <Accept kMode, bool kAny, bool kCount>
 HDCX_D bool traceInstance(const DeviceScene& s, const RayPre& pre, float3 o, float3 d, float tmin, uint32_t rayRng,
-                          uint32_t inst, ClosestHit& best, uint2* stack, uint2* work)
+                          uint32_t inst, ClosestHit& best, uint2* stack, uint2* work, uint32_t& fault)
 {
     const InstanceDesc I = s.instances[inst];
     const BlasDesc B = s.blases[I.blas];
@@ -470,9 +469,9 @@ HDCX_D bool traceInstance(const DeviceScene& s, const RayPre& pre, float3 o, flo
             best = ClosestHit{t, prim, b1, b2};
         }
         uint32_t nodeIndex;
-        if (!nextNode(group, stack, sp, kTraversalStack, octInv, nodeIndex, s)) return false;
+        if (!nextNode(group, stack, sp, kTraversalStack, octInv, nodeIndex, fault)) return false;
         if (budget-- == 0u) {
-            traversalFault(s, kTraversalBudget);
+            fault |= kTraversalBudget;
             return false;
         }
         if (kCount) work->x++;
@@ -486,7 +485,7 @@ HDCX_D bool traceInstance(const DeviceScene& s, const RayPre& pre, float3 o, flo
 
 template <Accept kMode, bool kAny, bool kCount>
 HDCX_D bool traceInstanced(const DeviceScene& s, float3 o, float3 d, float tmin, float tmax, uint32_t rayRng,
-                           HitRecord& hit, uint2* work)
+                           HitRecord& hit, uint2* work, uint32_t& fault)
 {
     const RayPre pre = precomputeRay(o, d);
     const float3 id = inverseDirection(d);
@@ -504,12 +503,12 @@ HDCX_D bool traceInstanced(const DeviceScene& s, float3 o, float3 d, float tmin,
             leaves.y &= leaves.y - 1u;
             const uint32_t slot = leaves.x + static_cast<uint32_t>(bit);
             const uint32_t inst = __float_as_uint(__ldg(&s.triVerts[slot * 3u].w));
-            if (traceInstance<kMode, kAny, kCount>(s, pre, o, d, tmin, rayRng, inst, best, stack, work)) return true;
+            if (traceInstance<kMode, kAny, kCount>(s, pre, o, d, tmin, rayRng, inst, best, stack, work, fault)) return true;
         }
         uint32_t nodeIndex;
-        if (!nextNode(group, topStack, sp, kTopStack, octInv, nodeIndex, s)) break;
+        if (!nextNode(group, topStack, sp, kTopStack, octInv, nodeIndex, fault)) break;
         if (budget-- == 0u) {
-            traversalFault(s, kTraversalBudget);
+            fault |= kTraversalBudget;
             break;
         }
         if (kCount) work->x++;
@@ -527,20 +526,22 @@ HDCX_D bool traceInstanced(const DeviceScene& s, float3 o, float3 d, float tmin,
 // Returns true on a (confirmed) hit; for closest queries fills `hit`.
 // kCount adds the wide nodes loaded to work.x and the triangle tests to work.y.
 // kInst: 0 single-level scenes only, 1 two-level scenes only, -1 either
-// (decided per call by DeviceScene::instances).
+// (decided per call by DeviceScene::instances). Traversal faults are ORed
+// into *fault.
 template <Accept kMode, bool kAny, bool kCount = false, int kInst = -1>
 HDCX_D bool traceRay(const DeviceScene& s, float3 o, float3 d, float tmin, float tmax, uint32_t rayRng, HitRecord& hit,
-                     uint2* work = nullptr)
+                     uint32_t& fault, uint2* work = nullptr)
 {
     if (s.nodeCount == 0u) return false;
     if (kInst == 1 || (kInst == -1 && s.instances != nullptr))
-        return traceInstanced<kMode, kAny, kCount>(s, o, d, tmin, tmax, rayRng, hit, work);
+        return traceInstanced<kMode, kAny, kCount>(s, o, d, tmin, tmax, rayRng, hit, work, fault);
     Traversal st;
     beginTraversal(st, s, o, d, tmin, tmax, rayRng);
     uint2 stack[kTraversalStack];
     int r;
     while ((r = traversalStep<kMode, kAny, kCount>(st, stack, s, work)) == kStepContinue) {
     }
+    fault |= st.fault;
     if (kAny) return r == kStepAnyHit;
     if (st.bestPrim == kInvalidPrimitive) return false;
     hit.t = st.bestT;

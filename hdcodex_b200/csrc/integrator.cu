@@ -151,12 +151,13 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) extendKernel(Devic
     const uint32_t n = *count;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(p.stats + 0, static_cast<unsigned long long>(n));
     uint2 work = make_uint2(0u, 0u);
+    uint32_t fault = 0u;  // traversal faults of this thread's rays
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t slot = queue[i];
         const float4 o = p.rayOrigin[slot];
         const float4 d = p.rayDirection[slot];
         HitRecord h;
-        const bool found = traceRay<kMode, false, kCount, kInst>(s, xyz(o), xyz(d), 0.001f, 10000.0f, p.rng[slot], h, &work);
+        const bool found = traceRay<kMode, false, kCount, kInst>(s, xyz(o), xyz(d), 0.001f, 10000.0f, p.rng[slot], h, fault, &work);
         p.hit[slot] = found ? make_float4(h.t, __uint_as_float(h.primitive), h.b1, h.b2)
                             : make_float4(0.0f, __uint_as_float(kInvalidPrimitive), 0.0f, 0.0f);
         // Hits and misses go to separate queues, so that shading warps hold
@@ -164,6 +165,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) extendKernel(Devic
         if (found) p.hitQueue[appendIndex(p.counters + 4)] = slot;
         else p.missQueue[appendIndex(p.counters + 5)] = slot;
     }
+    if (fault != 0u) atomicOr(reinterpret_cast<unsigned int*>(p.stats + 7), fault);
     if (kCount) {
         atomicAdd(p.stats + 3, static_cast<unsigned long long>(work.x));
         atomicAdd(p.stats + 4, static_cast<unsigned long long>(work.y));
@@ -253,7 +255,10 @@ __device__ bool traceOpaqueBoundary(const DeviceScene& s, PathBuffers& p, float3
     // :1130-1151
     atomicAdd(p.stats + 2, 1ull);
     HitRecord h;
-    if (!traceRay<Accept::Opaque, false, false, kInst>(s, origin, direction, 0.001f, 10000.0f, 0u, h)) return false;
+    uint32_t fault = 0u;
+    const bool found = traceRay<Accept::Opaque, false, false, kInst>(s, origin, direction, 0.001f, 10000.0f, 0u, h, fault);
+    if (fault != 0u) atomicOr(reinterpret_cast<unsigned int*>(p.stats + 7), fault);
+    if (!found) return false;
     const uint32_t primitive = h.primitive;
     const float3 p0 = xyz(__ldg(s.vertices + __ldg(s.indices + primitive * 3u + 0u)));
     const float3 p1 = xyz(__ldg(s.vertices + __ldg(s.indices + primitive * 3u + 1u)));
@@ -1017,6 +1022,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(Devic
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(p.stats + 1, static_cast<unsigned long long>(n));
     constexpr Accept kMode = kOpaque ? Accept::Opaque : Accept::Threshold;
     uint2 work = make_uint2(0u, 0u);
+    uint32_t fault = 0u;  // traversal faults of this thread's rays
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const float4 o = p.shadowOrigin[j];
         const float4 d = p.shadowDirection[j];
@@ -1029,7 +1035,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(Devic
         const float tmax = o.w;
         HitRecord h;
         if (kind == kShadowMesh) {
-            const bool occluded = traceRay<kMode, true, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+            const bool occluded = traceRay<kMode, true, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, fault, &work);
             if (occluded) p.contributionValid[k * p.capacity + slot] = 0;
             else p.contribution[k * p.capacity + slot] = d.w * fct.x;
             continue;
@@ -1040,10 +1046,10 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(Devic
         bool hitSomething;
         float hitDistance = 0.0f;
         if (falloff) {
-            hitSomething = traceRay<kMode, false, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+            hitSomething = traceRay<kMode, false, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, fault, &work);
             hitDistance = h.t;
         } else {
-            hitSomething = traceRay<kMode, true, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, &work);
+            hitSomething = traceRay<kMode, true, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, fault, &work);
         }
         if (hitSomething) {
             float strength = 1.0f;
@@ -1058,6 +1064,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(Devic
         const float sv = reflectanceSpectrum(visibility, spec);
         p.contribution[k * p.capacity + slot] = combineShadow(kind, d.w, sv, fct.x, fct.y, fct.z);
     }
+    if (fault != 0u) atomicOr(reinterpret_cast<unsigned int*>(p.stats + 7), fault);
     if (kCount) {
         atomicAdd(p.stats + 5, static_cast<unsigned long long>(work.x));
         atomicAdd(p.stats + 6, static_cast<unsigned long long>(work.y));
@@ -1133,8 +1140,9 @@ __global__ void primaryKernel(DeviceScene s, FrameConst f, uint32_t sampleNumber
     const float v = (u2f(py) + jy) / u2f(f.height);
     const float3 direction = normalize(f.lowerLeft + u * f.horizontal + v * f.vertical - f.origin);
     HitRecord h;
-    const bool found = s.opaque ? traceRay<Accept::Opaque, false>(s, f.origin, direction, 0.001f, 10000.0f, rng, h)
-                                : traceRay<Accept::Stochastic, false>(s, f.origin, direction, 0.001f, 10000.0f, rng, h);
+    uint32_t fault = 0u;  // primary hits of hdcx_trace_primary and the AOVs: a fault leaves the pixel a miss
+    const bool found = s.opaque ? traceRay<Accept::Opaque, false>(s, f.origin, direction, 0.001f, 10000.0f, rng, h, fault)
+                                : traceRay<Accept::Stochastic, false>(s, f.origin, direction, 0.001f, 10000.0f, rng, h, fault);
     primitives[pixel] = found ? h.primitive : kInvalidPrimitive;
     distances[pixel] = found ? h.t : 0.0f;
 }
@@ -1447,9 +1455,7 @@ void launchShade(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
 void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffers& paths, FrameBuffers& fb,
                  cudaStream_t stream, StageTimes* timing, bool countTraversal, uint64_t* launches, CacheRun* cacheRun)
 {
-    // Traversal faults go to the last word of the render's counters.
-    DeviceScene scene = sceneIn;
-    scene.status = reinterpret_cast<unsigned int*>(paths.stats + 7);
+    const DeviceScene& scene = sceneIn;
     const bool cacheMode = cacheRun != nullptr && cacheRun->cache != nullptr && paths.cache.enabled != 0u;
     if (!cacheMode) paths.cache.enabled = 0u;
     uint64_t launched = 0;
