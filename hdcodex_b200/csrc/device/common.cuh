@@ -93,6 +93,12 @@ struct TexDesc {
     //   conditional[h * w] (texel (col, row).x), conditionalSkip[h * ceil(w/32)],
     // where skip[k] = values[min(32k + 31, n - 1)].
     const float* cdf;
+    // Texture LOD (hdcx_set_texture_lod): levels 1..levels-1 of the mip
+    // pyramid as linear RGBA32F, level k (max(1, width >> k) x max(1, height >>
+    // k) texels) after level k-1; null and levels 1 without a pyramid.
+    const float4* mips;
+    uint32_t levels;
+    uint32_t pad;
 };
 
 // 8-wide BVH node with quantised child boxes (80 bytes). The layout is the
@@ -181,6 +187,9 @@ struct FrameConst {
     uint32_t sampleCount;
     uint32_t maxBounces;
     uint32_t zUp;
+    // Texture LOD: 0 off (every lookup at level 0, as the reference samples);
+    // else the spread angle of a camera ray per unit distance (ray cones).
+    float pixelSpread;
 };
 
 // ---------------------------------------------------------------------------

@@ -148,7 +148,52 @@ HDCX_D float4 textureSample(const DeviceScene& s, uint32_t index, float2 uv)
     return sampleBilinear(t, uv);
 }
 
-HDCX_D float4 sampleMaterialTexture(const DeviceScene& s, uint32_t textureIndex, float2 uv, float4 fallbackValue)
+// Texture LOD (not in the reference, whose sampler has one mip level): the
+// bilinear filter on mip level `level` >= 1 of the pyramid (REPEAT).
+HDCX_D float4 sampleMipBilinear(const TexDesc& t, uint32_t level, float2 uv)
+{
+    const float4* m = t.mips;
+    uint32_t w = t.width, h = t.height;
+    for (uint32_t k = 1; k <= level; ++k) {
+        const uint32_t nw = max(1u, w >> 1), nh = max(1u, h >> 1);
+        if (k < level) m += size_t(nw) * nh;
+        w = nw;
+        h = nh;
+    }
+    const float x = texelCoordinate(uv.x, w), y = texelCoordinate(uv.y, h);
+    const float fx = floorf(x), fy = floorf(y);
+    const float a = x - fx, b = y - fy;
+    const int i0 = wrapIndex(static_cast<int>(fx), static_cast<int>(w)), j0 = wrapIndex(static_cast<int>(fy), static_cast<int>(h));
+    const int i1 = wrapIndex(i0 + 1, static_cast<int>(w)), j1 = wrapIndex(j0 + 1, static_cast<int>(h));
+    const float4 t00 = __ldg(m + size_t(j0) * w + i0), t10 = __ldg(m + size_t(j0) * w + i1);
+    const float4 t01 = __ldg(m + size_t(j1) * w + i0), t11 = __ldg(m + size_t(j1) * w + i1);
+    const float w00 = (1.0f - a) * (1.0f - b), w10 = a * (1.0f - b), w01 = (1.0f - a) * b, w11 = a * b;
+    return make_float4(w00 * t00.x + w10 * t10.x + w01 * t01.x + w11 * t11.x,
+                       w00 * t00.y + w10 * t10.y + w01 * t01.y + w11 * t11.y,
+                       w00 * t00.z + w10 * t10.z + w01 * t01.z + w11 * t11.z,
+                       w00 * t00.w + w10 * t10.w + w01 * t01.w + w11 * t11.w);
+}
+
+// A lookup at level of detail lodBase + log2(sqrt(width * height)) (ray
+// cones: lodBase holds the hit's texture-independent terms), trilinear
+// between the two nearest levels; lodBase = -inf samples level 0 exactly as
+// textureSample does.
+HDCX_D float4 textureSampleLod(const DeviceScene& s, uint32_t index, float2 uv, float lodBase)
+{
+    if (index >= s.textureCount) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const TexDesc t = s.textures[index];
+    if (!(lodBase > -1e30f) || t.levels <= 1u || t.mips == nullptr) return sampleBilinear(t, uv);
+    const float lod = fminf(fmaxf(lodBase + 0.5f * log2f(u2f(t.width) * u2f(t.height)), 0.0f), u2f(t.levels - 1u));
+    const uint32_t l0 = static_cast<uint32_t>(lod);
+    const float f = lod - u2f(l0);
+    const float4 a = l0 == 0u ? sampleBilinear(t, uv) : sampleMipBilinear(t, l0, uv);
+    if (f <= 0.0f || l0 + 1u >= t.levels) return a;
+    const float4 b = sampleMipBilinear(t, l0 + 1u, uv);
+    return make_float4(a.x + (b.x - a.x) * f, a.y + (b.y - a.y) * f, a.z + (b.z - a.z) * f, a.w + (b.w - a.w) * f);
+}
+
+HDCX_D float4 sampleMaterialTexture(const DeviceScene& s, uint32_t textureIndex, float2 uv, float4 fallbackValue,
+                                    float lodBase = -INFINITY)
 {
     // :760-775
     if (textureIndex == kMissingTexture) return fallbackValue;
@@ -162,10 +207,10 @@ HDCX_D float4 sampleMaterialTexture(const DeviceScene& s, uint32_t textureIndex,
         if ((presentTiles & tileBit) == 0u) return fallbackValue;
         const uint32_t descriptorIndex = (textureIndex & 0xffu) + static_cast<uint32_t>(__popc(presentTiles & (tileBit - 1u)));
         if (descriptorIndex >= s.textureCount) return fallbackValue;
-        return textureSample(s, descriptorIndex, make_float2(fract(uv.x), fract(uv.y)));
+        return textureSampleLod(s, descriptorIndex, make_float2(fract(uv.x), fract(uv.y)), lodBase);
     }
     if (textureIndex >= s.textureCount) return fallbackValue;
-    return textureSample(s, textureIndex, uv);
+    return textureSampleLod(s, textureIndex, uv, lodBase);
 }
 
 HDCX_D float4 f4(float v) { return make_float4(v, v, v, v); }

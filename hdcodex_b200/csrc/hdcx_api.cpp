@@ -132,6 +132,7 @@ struct PathStore {
         p.walkEntry = alloc<float4>(n);
         p.walkNormal = alloc<float4>(n);
         p.walkState = alloc<float4>(n);
+        p.cone = alloc<float2>(n);
     }
 };
 
@@ -292,6 +293,8 @@ struct hdcx_tracer {
     // Two-level scenes (hdcx_set_scene_instanced); null for single-level ones.
     std::unique_ptr<TwoLevel> twoLevel;
     double sceneBuildMs = 0.0;  // host wall time of the last set_scene
+    uint32_t textureLod = 0;    // hdcx_set_texture_lod
+    std::vector<TexDesc> texDescHost;  // the device table's host copy (mip pyramids added on demand)
     double bvhBuildMs = 0.0;    // of which building the BVHs
     DeviceBuffer statsBuffer;  // this tracer's ray counters (8 x u64), whichever path buffers it renders with
     FrameBuffers fb;
@@ -458,6 +461,22 @@ bool buildCdfArrays(const PackedTexture& pt, std::vector<float>& block)
     if (!monotone(marginal, h)) return false;
     for (size_t k = 0; k < hs; ++k) marginalSkip[k] = marginal[std::min(32 * k + 31, h - 1)];
     return true;
+}
+
+// The mip pyramids of every texture without one (texture LOD), built on the
+// GPU into scene buffers; updates the host copy of the descriptor table.
+void buildTextureMips(hdcx_tracer* t)
+{
+    for (TexDesc& td : t->texDescHost) {
+        if (td.mips != nullptr || td.width == 0u || td.height == 0u) continue;
+        uint32_t levels = 1;
+        const uint64_t n = mipTexels(td.width, td.height, levels);
+        if (n == 0) continue;
+        auto* b = new DeviceBuffer();
+        t->sceneBuffers.push_back(b);
+        b->allocate(n * sizeof(float4));
+        buildMips(td, b->as<float4>(), t->stream);
+    }
 }
 
 // Object-space scale of a point set (max |coordinate|, max extent): the
@@ -660,6 +679,10 @@ void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
             descs[index].cdf = t->upload(block);
         }
     }
+    for (TexDesc& td : descs) td.levels = 1u;
+    t->texDescHost = descs;
+    if (t->textureLod) buildTextureMips(t);
+    descs = t->texDescHost;
     t->texDescs.allocate(std::max<size_t>(1, descs.size()) * sizeof(TexDesc));
     if (!descs.empty()) {
         check(cudaMemcpyAsync(t->texDescs.ptr, descs.data(), descs.size() * sizeof(TexDesc), cudaMemcpyHostToDevice, t->stream),
@@ -750,7 +773,7 @@ void ensureOutput(hdcx_tracer* t, uint32_t w, uint32_t h)
 constexpr uint64_t kAutomaticWavePaths = 12ull << 20;  // ~12.6M paths per wave
 // Device bytes of path state per path (PathBuffers with three shadow slots
 // and the deferred subsurface-walk records).
-constexpr uint64_t kPathStateBytes = 143 + 48 + 3 * 56;
+constexpr uint64_t kPathStateBytes = 143 + 48 + 8 + 3 * 56;
 
 // Smallest wave an automatic wave is shrunk to when device memory is short.
 constexpr uint64_t kMinimumAutomaticWave = 1ull << 16;
@@ -828,6 +851,17 @@ FrameConst makeFrame(const hdcx_tracer* t, const hdcx_camera& c, uint32_t w, uin
     f.sampleCount = std::max(sampleCount, 1u);
     f.maxBounces = std::clamp(maxBounces, 1u, HDCX_MAX_PATH_BOUNCES);
     f.zUp = t->fallbackZUp ? 1u : 0u;
+    if (t->textureLod) {
+        // Spread angle of a camera ray per pixel: the image's vertical extent
+        // over its height in pixels, at the distance of the image plane.
+        const double cx = double(f.lowerLeft.x) + 0.5 * f.horizontal.x + 0.5 * f.vertical.x - f.origin.x;
+        const double cy = double(f.lowerLeft.y) + 0.5 * f.horizontal.y + 0.5 * f.vertical.y - f.origin.y;
+        const double cz = double(f.lowerLeft.z) + 0.5 * f.horizontal.z + 0.5 * f.vertical.z - f.origin.z;
+        const double distance = std::sqrt(cx * cx + cy * cy + cz * cz);
+        const double extent = std::sqrt(double(f.vertical.x) * f.vertical.x + double(f.vertical.y) * f.vertical.y +
+                                        double(f.vertical.z) * f.vertical.z);
+        if (distance > 0.0 && h > 0u) f.pixelSpread = static_cast<float>(extent / (double(h) * distance));
+    }
     return f;
 }
 
@@ -1094,6 +1128,53 @@ HDCX_API hdcx_status hdcx_update_instancer_points(hdcx_tracer* t, uint64_t insta
         t->scene.nodeCount = tl.top.nodeCount;
         const size_t nt = tl.host.triangleCount();
         t->scene.hasMeshLights = (nt > 0 && tl.host.emissive[(nt - 1) * 4u] > 0.0F) ? 1u : 0u;
+    });
+}
+
+HDCX_API hdcx_status hdcx_set_texture_lod(hdcx_tracer* t, uint32_t mode)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (mode > 1u) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_set_texture_lod: mode must be 0 or 1");
+    return guarded(t, [&] {
+        drainAsync(t);
+        t->textureLod = mode;
+        if (mode && t->geometryReady && !t->texDescHost.empty()) {
+            check(cudaStreamSynchronize(t->stream), "cudaStreamSynchronize");
+            buildTextureMips(t);
+            check(cudaMemcpyAsync(t->texDescs.ptr, t->texDescHost.data(), t->texDescHost.size() * sizeof(TexDesc),
+                                  cudaMemcpyHostToDevice, t->stream),
+                  "upload textures");
+            check(cudaStreamSynchronize(t->stream), "texture LOD");
+        }
+    });
+}
+
+HDCX_API hdcx_status hdcx_read_texture_level(hdcx_tracer* t, uint32_t texture, uint32_t level, float* rgba,
+                                             uint64_t floatCount, uint32_t* width, uint32_t* height)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (texture >= t->texDescHost.size())
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_read_texture_level: no such texture");
+    const TexDesc& td = t->texDescHost[texture];
+    if (level == 0u || level >= td.levels || td.mips == nullptr)
+        return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_read_texture_level: no such mip level (levels " +
+                                                        std::to_string(td.levels) + "; level 0 is the texture itself)");
+    uint32_t w = td.width, h = td.height;
+    uint64_t offset = 0;
+    for (uint32_t k = 1; k <= level; ++k) {
+        const uint32_t nw = std::max(1u, w >> 1), nh = std::max(1u, h >> 1);
+        if (k < level) offset += uint64_t(nw) * nh;
+        w = nw;
+        h = nh;
+    }
+    if (width) *width = w;
+    if (height) *height = h;
+    if (!rgba) return HDCX_OK;
+    if (floatCount < uint64_t(w) * h * 4u) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "hdcx_read_texture_level: output too small");
+    return guarded(t, [&] {
+        check(cudaMemcpyAsync(rgba, td.mips + offset, uint64_t(w) * h * sizeof(float4), cudaMemcpyDefault, t->stream),
+              "read mip level");
+        check(cudaStreamSynchronize(t->stream), "read mip level");
     });
 }
 

@@ -126,6 +126,7 @@ __global__ void generateKernel(FrameConst f, WaveDesc w, PathBuffers p)
         }
     }
     p.flags[slot] = flags;
+    if (p.cone != nullptr) p.cone[slot] = make_float2(0.0f, f.pixelSpread);
     p.previousPdf[slot] = make_float2(0.0f, 0.0f);
     p.medium[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     p.contributionValid[slot] = 0;
@@ -184,10 +185,10 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) extendKernel(Devic
 // carries far less code and state.
 // ---------------------------------------------------------------------------
 template <bool kFull>
-HDCX_D float4 materialTexture(const DeviceScene& s, uint32_t index, float2 uv, float4 fallback)
+HDCX_D float4 materialTexture(float lodBase, const DeviceScene& s, uint32_t index, float2 uv, float4 fallback)
 {
     if (!kFull) return fallback;
-    return sampleMaterialTexture(s, index, uv, fallback);
+    return sampleMaterialTexture(s, index, uv, fallback, lodBase);
 }
 struct ShadeCtx {
     const DeviceScene& s;
@@ -369,6 +370,11 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
         const uint32_t primitive = __float_as_uint(hitRec.y);
         bool alive = true;
         bool deferred = false;  // kWalkDefer: walkKernel finishes this bounce
+        // Ray cone (width, spread) of texture LOD; spread <= 0: level 0.
+        const bool lodOn = kFull && f.pixelSpread > 0.0f && p.cone != nullptr;
+        const float2 cone = lodOn ? p.cone[slot] : make_float2(0.0f, -1.0f);
+        float coneWidth = 0.0f;
+        bool coneKept = false;  // a smooth reflection or refraction keeps the cone
 
         if (primitive == kInvalidPrimitive) {
             // :1245-1255
@@ -398,6 +404,22 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             const float2 uv2 = __ldg(s.texcoords + primitive * 3u + 2u);
             const float2 surfaceUv = surfaceTextureCoordinates(s, primitive, b1, b2);
             const float distance = hitRec.x;
+            // Texture LOD by ray cones (hdcx_set_texture_lod; Akenine-Moller et
+            // al., "Texture Level of Detail Strategies for Real-Time Ray
+            // Tracing", 2019): the cone's width at the hit, the triangle's
+            // texel-to-world area ratio and the incidence give the
+            // texture-independent part of the level; -inf samples level 0.
+            float lodBase = -INFINITY;
+            if (kFull && lodOn && cone.y > 0.0f) {
+                coneWidth = cone.x + cone.y * distance;
+                const float2 du = uv1 - uv0, dv = uv2 - uv0;
+                const float uvArea = fabsf(du.x * dv.y - du.y * dv.x);
+                const float3 c = cross(p1 - p0, p2 - p0);
+                const float worldArea = sqrtf(dot(c, c));
+                const float incidence = fmaxf(fabsf(dot(geometricNormal, rayDirection)), 1e-4f);
+                if (uvArea > 0.0f && worldArea > 0.0f && coneWidth > 0.0f)
+                    lodBase = 0.5f * log2f(uvArea / worldArea) + log2f(coneWidth / incidence);
+            }
             const float3 hit = rayOrigin + rayDirection * distance;
             if (insideMedium) {
                 // :1279-1295
@@ -418,7 +440,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             const GpuMaterial* material = s.materials + __ldg(s.triangleMaterials + primitive);
             float3 baseColorRgb = xyz(material->baseColorMetalness);
             if (kFull && material->textureIndices0.x != kMissingTexture) {
-                const float4 sample = materialTexture<kFull>(s, material->textureIndices0.x, surfaceUv, f4(baseColorRgb, 1.0f));
+                const float4 sample = materialTexture<kFull>(lodBase, s, material->textureIndices0.x, surfaceUv, f4(baseColorRgb, 1.0f));
                 const float scaleW = material->baseColorTextureScale.w;
                 const int channel = static_cast<int>(roundf(scaleW));
                 float3 sourceColor;
@@ -432,15 +454,15 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             }
             const float baseColor = reflectanceSpectrum(baseColorRgb, spec);
             const float metalness = clampf(
-                materialTexture<kFull>(s, material->textureIndices0.y, surfaceUv, f4(material->baseColorMetalness.w)).x, 0.0f, 1.0f);
+                materialTexture<kFull>(lodBase, s, material->textureIndices0.y, surfaceUv, f4(material->baseColorMetalness.w)).x, 0.0f, 1.0f);
             const float4 roughnessSample = materialTexture<kFull>(
-                s, material->textureIndices0.z, surfaceUv,
+                lodBase, s, material->textureIndices0.z, surfaceUv,
                 make_float4(material->emissionRoughness.w, material->subsurfaceColor.w, 0.0f, 1.0f));
             const float2 roughness = make_float2(clampf(roughnessSample.x, 0.02f, 1.0f), clampf(roughnessSample.y, 0.02f, 1.0f));
             const float diffuseRoughness = clampf(
-                materialTexture<kFull>(s, material->textureIndices4.z, surfaceUv, f4(material->diffuseProperties.x)).x, 0.0f, 1.0f);
+                materialTexture<kFull>(lodBase, s, material->textureIndices4.z, surfaceUv, f4(material->diffuseProperties.x)).x, 0.0f, 1.0f);
             const float diffuseWeight = clampf(
-                materialTexture<kFull>(s, material->textureIndices4.w, surfaceUv, f4(material->diffuseProperties.z)).x, 0.0f, 1.0f);
+                materialTexture<kFull>(lodBase, s, material->textureIndices4.w, surfaceUv, f4(material->diffuseProperties.z)).x, 0.0f, 1.0f);
             const uint32_t diffuseModel = kFull ? static_cast<uint32_t>(material->diffuseProperties.y + 0.5f) : 0u;
             if (kFull) normal = applyNormalMap(s, material->textureIndices1.y, material->coatWeightRoughnessIor.w > 0.5f,
                                     material->subsurfaceWeightScale.w, surfaceUv, normal, p0, p1, p2, uv0, uv1, uv2);
@@ -491,7 +513,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             const float transmission = kFull ? clampf(material->transmissionOpacityIor.x, 0.0f, 1.0f) : 0.0f;
             float3 transmissionColorRgb = xyz(material->transmissionColorThinWalled);
             if (transmission > 0.0f) {
-                const float4 t = materialTexture<kFull>(s, material->textureIndices1.z, surfaceUv, f4(transmissionColorRgb, 1.0f));
+                const float4 t = materialTexture<kFull>(lodBase, s, material->textureIndices1.z, surfaceUv, f4(transmissionColorRgb, 1.0f));
                 transmissionColorRgb = f3(t.x, t.y, t.z);
             }
             const float transmissionColor = reflectanceSpectrum(transmissionColorRgb, spec);
@@ -501,13 +523,13 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             float3 subsurfaceRadiusRgb = make_float3(gmax(material->subsurfaceRadius.x, 0.001f), gmax(material->subsurfaceRadius.y, 0.001f),
                                                      gmax(material->subsurfaceRadius.z, 0.001f));
             if (kFull && (material->subsurfaceWeightScale.x > 0.0f || material->textureIndices2.x != kMissingTexture)) {
-                subsurface = clampf(materialTexture<kFull>(s, material->textureIndices2.x, surfaceUv,
+                subsurface = clampf(materialTexture<kFull>(lodBase, s, material->textureIndices2.x, surfaceUv,
                                                           f4(material->subsurfaceWeightScale.x)).x, 0.0f, 1.0f);
                 if (subsurface > 0.0f) {
-                    const float4 c = materialTexture<kFull>(s, material->textureIndices2.y, surfaceUv,
+                    const float4 c = materialTexture<kFull>(lodBase, s, material->textureIndices2.y, surfaceUv,
                                                            f4(xyz(material->subsurfaceColor), 1.0f));
                     subsurfaceColorRgb = f3(c.x, c.y, c.z);
-                    const float4 r = materialTexture<kFull>(s, material->textureIndices2.z, surfaceUv,
+                    const float4 r = materialTexture<kFull>(lodBase, s, material->textureIndices2.z, surfaceUv,
                                                            f4(xyz(material->subsurfaceRadius), 1.0f));
                     subsurfaceRadiusRgb = make_float3(gmax(r.x, 0.001f), gmax(r.y, 0.001f), gmax(r.z, 0.001f));
                     const float subsurfaceColor = reflectanceSpectrum(subsurfaceColorRgb, spec);
@@ -517,9 +539,9 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             const float ior = dispersedIor(gmax(material->transmissionOpacityIor.z, 1.0001f), material->transmissionMedium.z,
                                            material->transmissionMedium.w, wavelength);
             const float specularWeight = clampf(
-                materialTexture<kFull>(s, material->textureIndices3.x, surfaceUv, f4(material->specularWeightColor.x)).x, 0.0f, 1.0f);
+                materialTexture<kFull>(lodBase, s, material->textureIndices3.x, surfaceUv, f4(material->specularWeightColor.x)).x, 0.0f, 1.0f);
             const float4 specularColorSample = materialTexture<kFull>(
-                s, material->textureIndices3.y, surfaceUv,
+                lodBase, s, material->textureIndices3.y, surfaceUv,
                 make_float4(material->specularWeightColor.y, material->specularWeightColor.z, material->specularWeightColor.w, 1.0f));
             const float specularColor =
                 reflectanceSpectrum(f3(specularColorSample.x, specularColorSample.y, specularColorSample.z), spec);
@@ -530,12 +552,12 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             float2 coatRoughness = make_float2(material->coatWeightRoughnessIor.y, material->subsurfaceRadius.w);
             float coatF0 = 0.0f;
             if (kFull && (material->coatWeightRoughnessIor.x > 0.0f || material->textureIndices3.z != kMissingTexture)) {
-                coat = clampf(materialTexture<kFull>(s, material->textureIndices3.z, surfaceUv,
+                coat = clampf(materialTexture<kFull>(lodBase, s, material->textureIndices3.z, surfaceUv,
                                                     f4(material->coatWeightRoughnessIor.x)).x, 0.0f, 1.0f);
                 if (coat > 0.0f) {
-                    const float4 cc = materialTexture<kFull>(s, material->textureIndices3.w, surfaceUv, f4(xyz(material->coatColor), 1.0f));
+                    const float4 cc = materialTexture<kFull>(lodBase, s, material->textureIndices3.w, surfaceUv, f4(xyz(material->coatColor), 1.0f));
                     const float coatColor = reflectanceSpectrum(f3(cc.x, cc.y, cc.z), spec);
-                    const float4 cr = materialTexture<kFull>(s, material->textureIndices4.x, surfaceUv,
+                    const float4 cr = materialTexture<kFull>(lodBase, s, material->textureIndices4.x, surfaceUv,
                                                             make_float4(coatRoughness.x, coatRoughness.y, 0.0f, 1.0f));
                     coatRoughness = make_float2(clampf(cr.x, 0.02f, 1.0f), clampf(cr.y, 0.02f, 1.0f));
                     const float coatIor = gmax(material->coatWeightRoughnessIor.z, 1.0001f);
@@ -545,17 +567,17 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                 }
             }
             const float sheen =
-                kFull ? clampf(materialTexture<kFull>(s, material->textureIndices1.w, surfaceUv, f4(material->coatColor.w)).x, 0.0f, 1.0f)
+                kFull ? clampf(materialTexture<kFull>(lodBase, s, material->textureIndices1.w, surfaceUv, f4(material->coatColor.w)).x, 0.0f, 1.0f)
                       : 0.0f;
-            const float4 sheenColorSample = materialTexture<kFull>(s, material->textureIndices2.w, surfaceUv,
+            const float4 sheenColorSample = materialTexture<kFull>(lodBase, s, material->textureIndices2.w, surfaceUv,
                                                                   f4(xyz(material->sheenColorMode), 1.0f));
             const float sheenColor = reflectanceSpectrum(f3(sheenColorSample.x, sheenColorSample.y, sheenColorSample.z), spec);
             const float sheenRoughness = clampf(
-                materialTexture<kFull>(s, material->textureIndices4.y, surfaceUv, f4(material->transmissionScatter.w)).x, 0.01f, 1.0f);
+                materialTexture<kFull>(lodBase, s, material->textureIndices4.y, surfaceUv, f4(material->transmissionScatter.w)).x, 0.01f, 1.0f);
             const bool sheenZeltner = material->sheenColorMode.w > 0.5f;
             const float translucentWeight = !kFull ? 0.0f : clampf(
-                materialTexture<kFull>(s, material->textureIndices5.x, surfaceUv, f4(material->translucentColorWeight.w)).x, 0.0f, 1.0f);
-            const float4 translucentSample = materialTexture<kFull>(s, material->textureIndices5.y, surfaceUv,
+                materialTexture<kFull>(lodBase, s, material->textureIndices5.x, surfaceUv, f4(material->translucentColorWeight.w)).x, 0.0f, 1.0f);
+            const float4 translucentSample = materialTexture<kFull>(lodBase, s, material->textureIndices5.y, surfaceUv,
                                                                    f4(xyz(material->translucentColorWeight), 1.0f));
             const float translucentColor = reflectanceSpectrum(f3(translucentSample.x, translucentSample.y, translucentSample.z), spec);
 
@@ -822,6 +844,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                 environmentOnMiss = true;
                 previousWasDelta = true;
                 previousBsdfPdf = 0.0f;
+                coneKept = true;
                 break;
             }
 
@@ -940,6 +963,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
         p.medium[slot] = make_float4(mediumAbsorption, mediumScattering, mediumAnisotropy, 0.0f);
         p.rayOrigin[slot] = make_float4(rayOrigin.x, rayOrigin.y, rayOrigin.z, 0.0f);
         p.rayDirection[slot] = make_float4(rayDirection.x, rayDirection.y, rayDirection.z, 0.0f);
+        if (lodOn) p.cone[slot] = coneKept ? make_float2(coneWidth, cone.y) : make_float2(0.0f, -1.0f);
         nextQueue[appendIndex(nextCount)] = slot;
     }
 }
@@ -974,6 +998,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS)
             p.previousPdf[slot] = make_float2(0.0f, p.previousPdf[slot].y);
             p.rayOrigin[slot] = make_float4(exitOrigin.x, exitOrigin.y, exitOrigin.z, 0.0f);
             p.rayDirection[slot] = make_float4(exitDirection.x, exitDirection.y, exitDirection.z, 0.0f);
+            if (p.cone != nullptr) p.cone[slot] = make_float2(0.0f, -1.0f);
             nextQueue[appendIndex(nextCount)] = slot;
         } else {
             p.walkState[slot] = make_float4(state.x, __uint_as_float(rng), state.z, 0.0f);
@@ -1612,6 +1637,67 @@ void launchUpscaleNearest(const float4* src, uint32_t srcWidth, uint32_t srcHeig
     upscaleNearestKernel<<<static_cast<unsigned>((pixels + 255u) / 256u), 256, 0, stream>>>(src, srcWidth, srcHeight, dst,
                                                                                           width, height);
     CUDA_OK(cudaGetLastError());
+}
+
+// One level of a texture's mip pyramid: each texel the mean of the 2x2
+// texels below it (the last row / column reused for odd sizes), level 0
+// decoded to linear RGBA (sRGB through the sampler's table).
+__global__ void mipLevelKernel(TexDesc t, const float4* below, uint32_t bw, uint32_t bh, float4* out, uint32_t w, uint32_t h)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= uint64_t(w) * h) return;
+    const uint32_t x = static_cast<uint32_t>(i % w), y = static_cast<uint32_t>(i / w);
+    const uint32_t x0 = min(2u * x, bw - 1u), x1 = min(2u * x + 1u, bw - 1u);
+    const uint32_t y0 = min(2u * y, bh - 1u), y1 = min(2u * y + 1u, bh - 1u);
+    float4 a, b, c, d;
+    if (below == nullptr) {
+        a = texelFetch(t, static_cast<int>(x0), static_cast<int>(y0));
+        b = texelFetch(t, static_cast<int>(x1), static_cast<int>(y0));
+        c = texelFetch(t, static_cast<int>(x0), static_cast<int>(y1));
+        d = texelFetch(t, static_cast<int>(x1), static_cast<int>(y1));
+    } else {
+        a = below[size_t(y0) * bw + x0];
+        b = below[size_t(y0) * bw + x1];
+        c = below[size_t(y1) * bw + x0];
+        d = below[size_t(y1) * bw + x1];
+    }
+    out[i] = make_float4(((a.x + b.x) + (c.x + d.x)) * 0.25f, ((a.y + b.y) + (c.y + d.y)) * 0.25f,
+                         ((a.z + b.z) + (c.z + d.z)) * 0.25f, ((a.w + b.w) + (c.w + d.w)) * 0.25f);
+}
+
+uint64_t mipTexels(uint32_t width, uint32_t height, uint32_t& levels)
+{
+    uint64_t total = 0;
+    levels = 1;
+    uint32_t w = width, h = height;
+    while (w > 1u || h > 1u) {
+        w = std::max(1u, w >> 1);
+        h = std::max(1u, h >> 1);
+        total += uint64_t(w) * h;
+        ++levels;
+    }
+    return total;
+}
+
+void buildMips(TexDesc& desc, float4* mips, cudaStream_t stream)
+{
+    uint32_t levels = 1;
+    mipTexels(desc.width, desc.height, levels);
+    uint32_t bw = desc.width, bh = desc.height;
+    const float4* below = nullptr;
+    float4* out = mips;
+    for (uint32_t k = 1; k < levels; ++k) {
+        const uint32_t w = std::max(1u, bw >> 1), h = std::max(1u, bh >> 1);
+        const uint64_t n = uint64_t(w) * h;
+        mipLevelKernel<<<static_cast<unsigned>((n + 255u) / 256u), 256, 0, stream>>>(desc, below, bw, bh, out, w, h);
+        CUDA_OK(cudaGetLastError());
+        below = out;
+        out += n;
+        bw = w;
+        bh = h;
+    }
+    desc.mips = mips;
+    desc.levels = levels;
 }
 
 void tracePrimary(const DeviceScene& scene, const FrameConst& frame, uint32_t sampleNumber, uint32_t* primitives,

@@ -89,6 +89,9 @@ struct PathBuffers {
     float4* walkEntry = nullptr;
     float4* walkNormal = nullptr;
     float4* walkState = nullptr;
+    // Texture LOD: per path the ray cone (width at the last vertex, spread
+    // angle; spread <= 0 once the cone is no longer tracked). Null: no LOD.
+    float2* cone = nullptr;
 };
 
 // Per-pixel accumulation buffers of the current output size.
@@ -132,6 +135,13 @@ void renderFrame(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
 // neighbour: the reference's UpscaleNearest (render_pass.cpp:45-68).
 void launchUpscaleNearest(const float4* src, uint32_t srcWidth, uint32_t srcHeight, float4* dst, uint32_t width,
                           uint32_t height, cudaStream_t stream);
+
+// Texels of the mip levels 1.. of a width x height texture (`levels` gets
+// the level count, level 0 included).
+uint64_t mipTexels(uint32_t width, uint32_t height, uint32_t& levels);
+// Builds the mip pyramid of `desc` into `mips` (mipTexels float4) on
+// `stream` and records it in desc.mips / desc.levels.
+void buildMips(TexDesc& desc, float4* mips, cudaStream_t stream);
 
 // Primary-hit ids and distances of sample `sampleNumber` (device outputs).
 void tracePrimary(const DeviceScene& scene, const FrameConst& frame, uint32_t sampleNumber, uint32_t* primitives,

@@ -88,6 +88,9 @@ SIGNATURES = {
     "hdcx_set_device_memory_limit": (C.c_int, [C.c_int32, C.c_uint64]),
     "hdcx_get_device_memory_usage": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hdcx_test_break_bvh": (C.c_int, [_P]),
+    "hdcx_set_texture_lod": (C.c_int, [_P, C.c_uint32]),
+    "hdcx_read_texture_level": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
+                                          C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "hdcx_pack_scene_instanced": (C.c_int, [C.c_void_p, C.POINTER(_abi.InstancerDesc), C.c_uint64,
                                             C.POINTER(C.c_void_p)]),
     "hdcx_set_scene_instanced": (C.c_int, [_P, C.c_void_p, C.POINTER(_abi.InstancerDesc), C.c_uint64]),
@@ -211,6 +214,21 @@ class PathTracer:
         p = np.ascontiguousarray(np.asarray(positions, dtype=np.float32).reshape(-1))
         self._check(lib().hdcx_update_instancer_points(self._h, instancer, p.ctypes.data_as(C.POINTER(C.c_float)),
                                                        p.size), "update_instancer_points")
+
+    def set_texture_lod(self, mode: int = 1):
+        """hdcx_set_texture_lod: 1 filters material textures at the level ray
+        cones give, from mip pyramids built on the GPU; 0 samples level 0."""
+        self._check(lib().hdcx_set_texture_lod(self._h, mode), "set_texture_lod")
+
+    def texture_level(self, texture: int, level: int):
+        """hdcx_read_texture_level: mip level `level` of a packed texture (h, w, 4) float32."""
+        w, h = C.c_uint32(0), C.c_uint32(0)
+        self._check(lib().hdcx_read_texture_level(self._h, texture, level, None, 0, C.byref(w), C.byref(h)),
+                    "read_texture_level")
+        out = np.empty((h.value, w.value, 4), dtype=np.float32)
+        self._check(lib().hdcx_read_texture_level(self._h, texture, level, out.ctypes.data_as(C.c_void_p), out.size,
+                                                  None, None), "read_texture_level")
+        return out
 
     def scene_info(self) -> dict:
         """hdcx_get_scene_info: triangles, instances, bottom levels, BVH and scene bytes, build times."""

@@ -444,6 +444,24 @@ HDCX_API hdcx_status hdcx_set_scene_instanced(hdcx_tracer* tracer, const hdcx_sc
 HDCX_API hdcx_status hdcx_update_instancer_points(hdcx_tracer* tracer, uint64_t instancer, const float* positions,
                                                   uint64_t position_count);
 
+/* Texture level of detail (not in the reference, whose sampler reads one
+ * mip level, vulkan_path_tracer.cpp:2401-2423; README.md lists texture LOD as
+ * future work). mode 0 (default): every lookup at level 0, the reference's
+ * sampling. mode 1: the library builds a mip pyramid of every texture on the
+ * GPU (2x2 means in linear RGBA32F, odd sizes reusing their last row or
+ * column) and material textures are filtered trilinearly at the level ray
+ * cones give (Akenine-Moller et al. 2019): a cone starts with the spread of a
+ * camera pixel and follows smooth reflections and refractions; after any
+ * other bounce lookups return to level 0. Light and dome textures and normal
+ * maps stay at level 0. Images then differ from the reference's: less
+ * texture aliasing and noise at low sample counts, slightly blurred
+ * textures. Scenes set later get pyramids while the mode is on. */
+HDCX_API hdcx_status hdcx_set_texture_lod(hdcx_tracer* tracer, uint32_t mode);
+/* Copies mip level `level` (>= 1) of packed texture `texture` (RGBA32F,
+ * width*height*4 floats; host or device memory; NULL only reports the size). */
+HDCX_API hdcx_status hdcx_read_texture_level(hdcx_tracer* tracer, uint32_t texture, uint32_t level, float* rgba_out,
+                                             uint64_t float_count, uint32_t* width, uint32_t* height);
+
 /* Size and build cost of the current scene. */
 typedef struct hdcx_scene_info {
     uint64_t triangles;      /* flattened triangles */
