@@ -52,8 +52,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hdcx", choices=["hdcx", "reference"])
-    ap.add_argument("--workload", default="heavy", choices=["heavy", "box", "stress", "batch", "nrc", "cache-kernels"],
-                    help="heavy: 1.0M triangles, 1920x1080, 64 spp (the headline); box: 34-triangle closed box, "
+    ap.add_argument("--workload", default="heavy",
+                    choices=["heavy", "heavy-instanced", "box", "stress", "batch", "nrc", "cache-kernels"],
+                    help="heavy: 1.0M triangles, 1920x1080, 64 spp (the headline); heavy-instanced: the same "
+                         "shape with its spheres as 256 instances of four prototypes (two-level BVH); "
+                         "box: 34-triangle closed box, "
                          "256x256, 16 spp; stress: 200k-triangle spectral stress scene, 1280x720, 256 spp; "
                          "batch: --jobs scenes of 10k-2M triangles rendered by hdcx_render_batch; "
                          "nrc: time to a relative XYZ RMSE on the stress scene, radiance cache vs plain; "
@@ -83,14 +86,15 @@ def parse():
     return ap.parse_args()
 
 
-WORKLOADS = {"heavy": "heavy_geometry", "box": "closed_box", "stress": "spectral_stress"}
+WORKLOADS = {"heavy": "heavy_geometry", "heavy-instanced": "heavy_geometry", "box": "closed_box",
+             "stress": "spectral_stress"}
 
 
 def make_workload(name, args=None):
     """The named workload; --width/--height/--spp (profiling only) resize it."""
     from hdcodex_b200 import workloads
     make = getattr(workloads, WORKLOADS[name])
-    overrides = {}
+    overrides = {"instanced": True} if name == "heavy-instanced" else {}
     if args is not None:
         for key in ("width", "height", "spp"):
             if getattr(args, key):
@@ -576,6 +580,9 @@ def run_hdcx(args):
     wl = make_workload(args.workload, args)
     tracer = PathTracer(local)
     tracer.set_scene(wl.scene)
+    # Scene size and build cost (BVH bytes, set_scene wall time): the
+    # instanced workload's two-level BVH against the flattened scene's.
+    scene_info = tracer.scene_info()
     tuning = None
     if args.tuning:
         knobs = [int(x) for x in args.tuning.split(",")] + [0, 0]
@@ -693,6 +700,7 @@ def run_hdcx(args):
                                   "other": (render_ms - extend_ms - shade_ms - shadow_ms) / args.steps},
             "roofline": roofline,
             "tuning": tuning if tuning is not None else tracer.tuning(),
+            "scene": scene_info,
             "cpu_baseline": baseline,
             "clocks": clocks,
             "wall_s_timed": wall,

@@ -192,6 +192,8 @@ class ReferenceTracer:
         if scene is None:
             ref_lib().ref_set_scene(self._h, None)
             return
+        if scene.instancers:  # the reference's Hydra adapter flattens instancers
+            scene = scene.flattened()
         holder = scene.to_desc()
         ref_lib().ref_set_scene(self._h, C.cast(holder.pointer(), C.c_void_p))
 
