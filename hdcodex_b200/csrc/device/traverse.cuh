@@ -22,11 +22,6 @@
 //   of sm_100 (__fadd2_rn, __ffma2_rn): each half is the same IEEE operation
 //   as the scalar form, so the node test's results are unchanged, in fewer
 //   instructions.
-// * Triangle postponing (Ylitie et al., section 4.2): while fewer than
-//   kPostponeLanes lanes of the warp would test triangles, a lane that also
-//   has a node to visit pushes its triangle group on the stack and visits
-//   the node; the group is tested when it is popped. Closest-hit results do
-//   not depend on the order of the tests.
 // * Faults: a node group that finds the stack full, or a traversal that
 //   visits more nodes than the BVH holds (a malformed node array), sets a
 //   bit in the traversal's fault word; the kernels OR it into the render's
@@ -40,15 +35,6 @@
 namespace hdcx {
 
 constexpr int kTraversalStack = 64;
-// Triangle groups are postponed while fewer than this many lanes of the warp
-// would test triangles in a step ...
-#ifndef HDCX_POSTPONE_LANES
-#define HDCX_POSTPONE_LANES 6
-#endif
-constexpr uint32_t kPostponeLanes = HDCX_POSTPONE_LANES;
-// ... and while the stack holds fewer than this many entries (node groups
-// need at most one entry per BVH level, which the build caps at 64).
-constexpr int kPostponeDepth = 32;
 
 
 enum class Accept : int {
@@ -270,18 +256,6 @@ HDCX_D void testNode(const WideNode* nodes, uint32_t nodeIndex, float3 o, float 
 template <Accept kMode, bool kAny, bool kCount = false>
 HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint2* work)
 {
-    // Postponing: a triangle group on the stack has no hit bits in 24..31
-    // (a node group always has some), which tells the two apart on a pop.
-    // Only a lane with a node group in hand postpones, so the step still
-    // visits a node and the postponed group is not popped straight back.
-    if (kPostponeLanes > 0u) {
-        const uint32_t testing = __ballot_sync(__activemask(), st.triGroup.y != 0u);
-        if (st.triGroup.y != 0u && static_cast<uint32_t>(__popc(testing)) < kPostponeLanes &&
-            (st.nodeGroup.y & 0xff000000u) != 0u && st.sp < kPostponeDepth) {
-            stack[st.sp++] = st.triGroup;
-            st.triGroup.y = 0u;
-        }
-    }
     while (st.triGroup.y != 0u) {
         const int bit = __ffs(st.triGroup.y) - 1;
         st.triGroup.y &= st.triGroup.y - 1u;
@@ -312,12 +286,7 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
     }
     if ((st.nodeGroup.y & 0xff000000u) == 0u) {
         if (st.sp == 0) return kStepDone;
-        const uint2 entry = stack[--st.sp];
-        if ((entry.y & 0xff000000u) == 0u) {  // a postponed triangle group
-            st.triGroup = entry;
-            return kStepContinue;
-        }
-        st.nodeGroup = entry;
+        st.nodeGroup = stack[--st.sp];
     }
     if (st.budget-- == 0u) {
         st.fault |= kTraversalBudget;

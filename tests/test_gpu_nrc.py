@@ -10,6 +10,8 @@ import nrc_oracle as N
 pytestmark = pytest.mark.gpu
 
 LOG2 = 14
+# Both a small table and the config's 2^19 entries per level.
+TABLE_SIZES = [14, 19]
 
 
 def queries(n, seed):
@@ -30,10 +32,10 @@ def radiance_field(q):
     return (1.0 + 0.6 * np.sin(6 * x) * np.cos(4 * y) + 0.5 * z + 0.3 * lam).astype(np.float32)
 
 
-@pytest.fixture(scope="module")
-def cache():
+@pytest.fixture(scope="module", params=TABLE_SIZES, ids=[f"2^{k}" for k in TABLE_SIZES])
+def cache(request):
     from hdcodex_b200 import RadianceCache
-    c = RadianceCache(0, log2_table_size=LOG2, base_resolution=16, finest_resolution=512, seed=7)
+    c = RadianceCache(0, log2_table_size=request.param, base_resolution=16, finest_resolution=512, seed=7)
     rng = np.random.default_rng(11)
     mlp, grid = c.parameters()
     for l in range(5):
@@ -59,11 +61,14 @@ def test_forward_matches_oracle(cache):
     out = torch.zeros(len(q), dtype=torch.float32, device="cuda")
     cache.query(dq.data_ptr(), len(q), out.data_ptr())
     got = out.cpu().numpy()
-    ref, _ = N.forward(q, mlp, grid, cache.resolutions(), LOG2)
+    ref, _ = N.forward(q, mlp, grid, cache.resolutions(), cache.config.log2_table_size)
     assert np.isfinite(got).all()
+    # The oracle rounds weights, activations and output gradients to BF16 as
+    # the kernels do; what remains is the FP32 summation order (measured:
+    # relative L2 4e-5, largest difference 1e-3 of the largest prediction).
     err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
-    assert err < 1e-2, err
-    assert np.abs(got - ref).max() < 0.05 * np.abs(ref).max()
+    assert err < 1e-3, err
+    assert np.abs(got - ref).max() < 5e-3 * np.abs(ref).max()
 
 
 def test_gradients_match_oracle(cache):
@@ -72,7 +77,7 @@ def test_gradients_match_oracle(cache):
     mlp, grid = cache.parameters()
     dq, dy = device(q), device(y)  # held: the cache reads them during the call
     g_mlp, g_grid = cache.gradients(dq.data_ptr(), dy.data_ptr(), len(q))
-    _, r_mlp, r_grid = N.gradients(q, y, mlp, grid, cache.resolutions(), LOG2)
+    _, r_mlp, r_grid = N.gradients(q, y, mlp, grid, cache.resolutions(), cache.config.log2_table_size)
     for l in range(5):
         a = g_mlp[N.LAYER_OFFSET[l]:N.LAYER_OFFSET[l] + N.LAYER_ROWS[l] * N.WIDTH]
         b = r_mlp[N.LAYER_OFFSET[l]:N.LAYER_OFFSET[l] + N.LAYER_ROWS[l] * N.WIDTH]
@@ -80,10 +85,10 @@ def test_gradients_match_oracle(cache):
             assert not a[N.WIDTH:].any()
         cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
         assert cos > 0.9999, (l, cos)
-        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-3, l
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4, l  # measured ~2e-7
     cos = float(g_grid @ r_grid / (np.linalg.norm(g_grid) * np.linalg.norm(r_grid)))
     assert cos > 0.9999, cos
-    assert np.linalg.norm(g_grid - r_grid) / np.linalg.norm(r_grid) < 1e-3
+    assert np.linalg.norm(g_grid - r_grid) / np.linalg.norm(r_grid) < 1e-4  # measured ~5e-8
 
 
 def test_training_fits_a_radiance_field():
