@@ -261,6 +261,36 @@ def cpu_baseline(wl, target_seconds, rank0=True):
             "rays_per_s": rays / secs}
 
 
+def traversal_roofline(tracers_and_workloads, peak, peak_kind):
+    """Roofline of the closest-hit traversal kernel over untimed renders of
+    the given (tracer, workload) pairs: node visits and triangle tests from a
+    counting render, extension rays and extendKernel time from a stage-timed
+    render; algorithmic bytes (32 B ray + 16 B hit + 80 B per wide node + 36 B
+    per triangle) over the kernel's time, against the HBM copy peak."""
+    from hdcodex_b200.tracer import PROFILE_COUNT_TRAVERSAL, PROFILE_STAGE_TIMES
+    total_bytes, total_ms, rays, nodes, tris = 0.0, 0.0, 0, 0, 0
+    for t, wl in tracers_and_workloads:
+        t.set_profiling(PROFILE_COUNT_TRAVERSAL)
+        t.render_device(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp)
+        c = t.stats()
+        t.set_profiling(PROFILE_STAGE_TIMES)
+        t.render_device(wl.camera, wl.width, wl.height, 0, wl.max_bounces, wl.spp)
+        st = t.stats()
+        t.set_profiling(0)
+        r = max(c["extension_rays"], 1)
+        per_ray = 32 + 16 + 80 * c["extension_node_visits"] / r + 36 * c["extension_triangle_tests"] / r
+        total_bytes += per_ray * st["extension_rays"]
+        total_ms += st["extend_ms"]
+        rays += c["extension_rays"]
+        nodes += c["extension_node_visits"]
+        tris += c["extension_triangle_tests"]
+    achieved = total_bytes / (total_ms / 1000.0) / 1e9 if total_ms > 0 else None
+    return {"kernel": "extendKernel (closest-hit traversal)", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+            "traffic": None, "nodes_per_ray": nodes / max(rays, 1), "triangles_per_ray": tris / max(rays, 1),
+            "jobs_measured": len(tracers_and_workloads)}
+
+
 def workload_config(wl, world):
     from hdcodex_b200 import workloads
     return {"workload": wl.name, "triangles": workloads.triangle_count(wl.scene), "width": wl.width,
@@ -376,6 +406,18 @@ def run_batch(args):
         tp = torch.tensor([float(paths)], dtype=torch.float64, device="cuda")
         dist.all_reduce(tp)
         total_paths = float(tp.item())
+    roofline, baseline = None, None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        # The traversal roofline over the first eight jobs' own renders.
+        roofline = traversal_roofline(list(zip(tracers, jobs))[:8], peak, peak_kind)
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                baseline = cpu_baseline(jobs[0], args.cpu_seconds)
+                baseline["sample"] = "job 0 of the batch: " + baseline["sample"]
+            except Exception as exc:  # reported, never required
+                baseline = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                            "sample": f"failed: {exc}"}
     if rank == 0:
         value = total_paths * args.steps / batch_s
         print(json.dumps({
@@ -393,6 +435,8 @@ def run_batch(args):
                             "ms_per_step": 1000.0 * serial_s / args.steps},
             "batch_over_serial": serial_s / batch_s,
             "per_job_device_ms_rank0": [round(ms / args.steps, 2) for ms in per_job_ms],
+            "roofline": roofline,
+            "cpu_baseline": baseline,
             "clocks": clocks,
         }), flush=True)
     for t in tracers:
@@ -460,13 +504,19 @@ def run_nrc(args):
     second = (total[0] - half[0]) / (total[1] - half[1])
     reference_noise = 0.5 * float(np.linalg.norm(half[0] / half[1] - second)) / ref_norm
 
+    # 2^16 training path suffixes per render call (the config's per-frame
+    # count), spread over the call's waves.
+    wave = tuning.get("wave_paths") or (12 << 20)
+    waves_per_call = max(1, -(-(w * h * args.chunk_spp * 3) // wave))
+    training_paths = max(1024, (1 << 16) // waves_per_call)
+
     def converge(cache, prefix=2):
         curve = []
         with PathTracer(0) as t:
             t.set_scene(wl.scene)
             t.set_tuning(**tuning)
             if cache is not None:
-                t.set_radiance_cache(cache, prefix_bounces=prefix, training_paths=1 << 14, train_steps=4)
+                t.set_radiance_cache(cache, prefix_bounces=prefix, training_paths=training_paths, train_steps=4)
             elapsed, spp, err = 0.0, 0, float("inf")
             torch.cuda.synchronize()
             while spp < args.max_spp:
@@ -493,6 +543,22 @@ def run_nrc(args):
             arms[prefix]["prefix_bounces"] = prefix
     cached = arms[prefixes[0]]
     ratio = (cached["seconds"] / plain["seconds"]) if (plain["seconds"] and cached["seconds"]) else None
+    peak, peak_kind = measured_peaks()
+    with PathTracer(0) as t:
+        t.set_scene(wl.scene)
+        t.set_tuning(**tuning)
+        sized = workloads.spectral_stress(width=w, height=h, spp=args.chunk_spp)
+        roofline = traversal_roofline([(t, sized)], peak, peak_kind)
+    baseline = None
+    if not args.no_cpu_baseline:
+        # The oracle's rate on the stress scene's row sample, and the time it
+        # would take to trace the plain arm's spp at that rate.
+        try:
+            baseline = cpu_baseline(workloads.spectral_stress(width=w, height=h, spp=args.chunk_spp), args.cpu_seconds)
+            if plain["spp"] and baseline["value"]:
+                baseline["projected_seconds_to_target"] = w * h * 3 * plain["spp"] / baseline["value"]
+        except Exception as exc:
+            baseline = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {exc}"}
     print(json.dumps({
         "metric": "time to 2% relative XYZ RMSE, radiance cache vs plain", "unit": "s",
         "value": cached["seconds"], "plain_seconds": plain["seconds"], "cache_over_plain": ratio,
@@ -502,8 +568,10 @@ def run_nrc(args):
                    "reference_seconds": ref_s, "reference_rel_noise": reference_noise,
                    "target_rel_rmse": args.target_rmse, "chunk_spp": args.chunk_spp,
                    "cache": "16 levels x 2 features, 2^19 entries/level fp16; MLP 64x4 ReLU bf16; "
-                            f"prefix {prefixes[0]} bounces; 2^14 training paths per wave, 4 Adam steps per wave",
+                            f"prefix {prefixes[0]} bounces; {training_paths} training paths per wave "
+                            f"({waves_per_call} wave(s) per call: 2^16 per call), 4 Adam steps per wave",
                    "tuning": tuning},
+        "roofline": roofline, "cpu_baseline": baseline,
         "plain": plain, "cache": cached,
         "cache_by_prefix": {str(k): {"seconds": v["seconds"], "spp": v["spp"], "final_rel_rmse": v["final_rel_rmse"],
                                      "ratio_to_plain": (v["seconds"] / plain["seconds"])
