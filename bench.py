@@ -366,6 +366,23 @@ def run_batch(args):
         tracers.append(t)
     hosts = [torch.empty((wl.height, wl.width, 4), dtype=torch.float32, pin_memory=True) for wl in jobs]
     paths = sum(wl.spectral_paths for wl in jobs)
+    # Launch tuning (setup, untimed): --tuning, else the autotuner's pick for
+    # the job with the most paths, applied to every job.
+    if args.tuning:
+        knobs = [int(x) for x in args.tuning.split(",")] + [0, 0]
+        tuning = {"wave_paths": knobs[0], "trace_blocks_per_sm": knobs[1], "shade_blocks_per_sm": knobs[2],
+                  "sort_hits": knobs[3], "sort_rays": knobs[4]}
+    elif args.autotune and jobs:
+        big = max(range(len(jobs)), key=lambda k: jobs[k].spectral_paths)
+        wl = jobs[big]
+        tuned = tracers[big].autotune(wl.camera, wl.width, wl.height, wl.max_bounces, wl.spp)
+        tuning = {k: tuned[k] for k in ("wave_paths", "trace_blocks_per_sm", "shade_blocks_per_sm", "sort_hits",
+                                        "sort_rays")}
+    else:
+        tuning = None
+    if tuning:
+        for t in tracers:
+            t.set_tuning(**tuning)
 
     def batch_step(step):
         spec = [(t, wl.camera, wl.width, wl.height, step * wl.spp, wl.max_bounces, wl.spp, h.data_ptr())
@@ -428,7 +445,8 @@ def run_batch(args):
                        "spectral_paths_per_step": total_paths,
                        "triangles": sum(workloads.triangle_count(wl.scene) for wl in jobs) if world == 1 else None,
                        "l2": "inputs larger than L2", "parallelism": f"jobs dealt round-robin to {world} GPU(s)",
-                       "launch": "one CUDA graph per batch frame" if args.graph else "jobs on their own streams"},
+                       "launch": "one CUDA graph per batch frame" if args.graph else "jobs on their own streams",
+                       "tuning": tuning},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 48 * len(jobs),
                     "d2h_bytes_per_step": sum(wl.width * wl.height * 16 for wl in jobs)},
             "serial_loop": {"value": total_paths * args.steps / serial_s, "unit": UNIT,
