@@ -26,6 +26,7 @@
 #include "device_memory.h"
 #include "integrator.h"
 #include "nrc.h"
+#include "nvtx_range.h"
 #include "render_static.h"
 #include "scene_pack.h"
 
@@ -734,6 +735,7 @@ void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
         if (hi[k] >= lo[k]) scale = std::max(scale, hi[k] - lo[k]);
     }
     const auto bvhStart = std::chrono::steady_clock::now();
+    NvtxRange bvhRange("hdcx bvh build");
     if (d.instancers.empty()) {
         t->bvh = buildWideBvh(s.vertices, s.indices, s.primitiveCount, std::max(scale, 1e-20F), t->stream);
         s.nodes = t->bvh.nodes;
@@ -1067,8 +1069,13 @@ HDCX_API hdcx_status hdcx_set_scene_instanced(hdcx_tracer* t, const hdcx_scene_d
             t->clearScene();
             return;
         }
+        NvtxRange range("hdcx set_scene");
         const auto start = std::chrono::steady_clock::now();
-        const PackedSceneData d = packScene(*desc, instancers, instancerCount);
+        PackedSceneData d;
+        {
+            NvtxRange packRange("hdcx pack_scene");
+            d = packScene(*desc, instancers, instancerCount);
+        }
         uploadScene(t, d);
         t->sceneBuildMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - start).count();
     });
@@ -1358,7 +1365,8 @@ void enqueueRender(hdcx_tracer* t, RenderCall& call, float* rgbaOut, bool timeEv
     }
 }
 
-// The render's traversal fault word (DeviceScene::status): a dropped node
+// The render's traversal fault word (counter 7 of the render's statistics,
+// which every traversal kernel ORs its threads' fault bits into): a dropped node
 // group or an exhausted node budget means hits may have been lost, so the
 // image is not trusted.
 void throwOnTraversalFault(unsigned long long word)
@@ -1375,7 +1383,10 @@ void throwOnTraversalFault(unsigned long long word)
 // `graphMs` >= 0: the render ran inside a batch graph, which measured its device time.
 void finishRender(hdcx_tracer* t, RenderCall& call, float graphMs = -1.0F)
 {
-    check(cudaStreamSynchronize(t->stream), "render");
+    {
+        NvtxRange range("hdcx wait for render");
+        check(cudaStreamSynchronize(t->stream), "render");
+    }
     t->xyzSamples = (call.frame.sampleIndex == 0 ? 0 : t->xyzSamples) + call.frame.sampleCount;
     unsigned long long counters[8];
     check(cudaMemcpy(counters, call.paths.stats, sizeof counters, cudaMemcpyDeviceToHost), "read stats");
@@ -1602,6 +1613,7 @@ HDCX_API hdcx_status hdcx_render(hdcx_tracer* t, const hdcx_camera* camera, uint
     if (uint64_t(width) * height > (1ull << 28)) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "image larger than 2^28 pixels");
     return guarded(t, [&] {
         drainAsync(t);
+        NvtxRange range("hdcx render");
         // The arena stays checked out until the render's work has finished.
         ArenaLease lease;
         if (!t->radianceCache) lease = checkoutArena(t->device, true);
@@ -2022,6 +2034,7 @@ HDCX_API hdcx_status hdcx_render_batch_ex(hdcx_batch_job* jobs, uint32_t count, 
             if (drained != HDCX_OK) return drained;
         }
     }
+    NvtxRange range("hdcx render_batch");
     std::vector<RenderCall> calls(count);
     auto record = [&](uint32_t j, hdcx_status status) {
         if (status != HDCX_OK) {
@@ -2376,6 +2389,7 @@ HDCX_API hdcx_status hdcx_autotune(hdcx_tracer* t, const hdcx_camera* camera, ui
     if (!t || !camera || width == 0 || height == 0) return HDCX_ERROR_INVALID_ARGUMENT;
     if (!t->geometryReady) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "no geometry");
     if (t->radianceCache) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "detach the radiance cache before tuning");
+    NvtxRange range("hdcx autotune");
     const TuningKey key{t->device, t->scene.primitiveCount, width, height, std::max(sampleCount, 1u),
                         std::clamp(maxBounces, 1u, HDCX_MAX_PATH_BOUNCES), t->scene.fullShading,
                         (t->scene.lightCount > 0u && !t->scene.hasMeshLights) ? 1u : 0u, t->scene.opaque};

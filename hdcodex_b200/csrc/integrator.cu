@@ -19,6 +19,7 @@
 // device-side queue length, so a frame needs no host round trip.
 #include "integrator.h"
 #include "nrc.h"
+#include "nvtx_range.h"
 
 #include <cooperative_groups.h>
 
@@ -1513,6 +1514,7 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
         events.push_back(e);
     };
     for (const WaveDesc& w : waves) {
+        NvtxRange waveRange("hdcx wave");
         if (cacheMode) CUDA_OK(cudaMemsetAsync(paths.cache.counters, 0, 3 * sizeof(uint32_t), stream));
         generateKernel<<<(w.count + 255u) / 256u, 256, 0, stream>>>(frame, w, paths);
         CUDA_OK(cudaGetLastError());
