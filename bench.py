@@ -70,6 +70,11 @@ def parse():
     ap.add_argument("--max-spp", type=int, default=4096, help="nrc workload: give up after this many spp")
     ap.add_argument("--nrc-prefix", default="2,1",
                     help="nrc workload: comma-separated prefix bounces of the cache arms (the first is `value`)")
+    ap.add_argument("--nrc-spread", default="0.01",
+                    help="nrc workload: comma-separated spread factors c of further cache arms that end paths by "
+                         "the spread heuristic (prefix --nrc-spread-cap as the latest bounce); empty: none")
+    ap.add_argument("--nrc-spread-cap", type=int, default=4,
+                    help="nrc workload: latest bounce of the spread arms' paths")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default="",
@@ -528,13 +533,14 @@ def run_nrc(args):
     waves_per_call = max(1, -(-(w * h * args.chunk_spp * 3) // wave))
     training_paths = max(1024, (1 << 16) // waves_per_call)
 
-    def converge(cache, prefix=2):
+    def converge(cache, prefix=2, spread=0.0):
         curve = []
         with PathTracer(0) as t:
             t.set_scene(wl.scene)
             t.set_tuning(**tuning)
             if cache is not None:
                 t.set_radiance_cache(cache, prefix_bounces=prefix, training_paths=training_paths, train_steps=4)
+                t.set_radiance_cache_spread(spread)
             elapsed, spp, err = 0.0, 0, float("inf")
             torch.cuda.synchronize()
             while spp < args.max_spp:
@@ -559,6 +565,10 @@ def run_nrc(args):
         with RadianceCache(0) as cache:
             arms[prefix] = converge(cache, prefix)
             arms[prefix]["prefix_bounces"] = prefix
+    spread_arms = {}
+    for factor in [float(x) for x in str(args.nrc_spread).split(",") if x.strip()]:
+        with RadianceCache(0) as cache:
+            spread_arms[factor] = converge(cache, args.nrc_spread_cap, factor)
     cached = arms[prefixes[0]]
     ratio = (cached["seconds"] / plain["seconds"]) if (plain["seconds"] and cached["seconds"]) else None
     peak, peak_kind = measured_peaks()
@@ -595,6 +605,11 @@ def run_nrc(args):
                                      "ratio_to_plain": (v["seconds"] / plain["seconds"])
                                      if (v["seconds"] and plain["seconds"]) else None}
                             for k, v in arms.items()},
+        "cache_by_spread": {f"c={k:g}, latest bounce {args.nrc_spread_cap}": {
+            "seconds": v["seconds"], "spp": v["spp"], "final_rel_rmse": v["final_rel_rmse"],
+            "ratio_to_plain": (v["seconds"] / plain["seconds"]) if (v["seconds"] and plain["seconds"]) else None,
+            "queries": (v["cache_stats"] or {}).get("queries")}
+            for k, v in spread_arms.items()},
     }), flush=True)
 
 

@@ -305,6 +305,7 @@ struct hdcx_tracer {
     // Radiance-cache mode (hdcx_set_radiance_cache).
     hdcx_nrc* radianceCache = nullptr;
     uint32_t cachePrefix = 2;
+    float cacheSpread = 0.0F;  // hdcx_set_radiance_cache_spread
     uint32_t cacheTrainingPaths = 1u << 14;
     std::vector<DeviceBuffer*> cacheBuffers;
     CacheDevice cacheDevice;
@@ -828,6 +829,7 @@ void ensureCacheBuffers(hdcx_tracer* t, uint64_t capacity)
     c.querySlot = t->cacheAlloc<uint32_t>(capacity);
     c.predictions = t->cacheAlloc<float>(capacity);
     c.trainIndex = t->cacheAlloc<uint32_t>(capacity);
+    c.spread = t->cacheAlloc<float2>(capacity);
     c.trainSlot = t->cacheAlloc<uint32_t>(trainCapacity);
     c.trainVertices = t->cacheAlloc<uint32_t>(trainCapacity);
     c.trainRecords = t->cacheAlloc<float>(records * 12u);
@@ -1335,6 +1337,7 @@ void prepareRender(hdcx_tracer* t, const hdcx_camera& camera, uint32_t width, ui
         CacheDevice c = t->cacheDevice;
         c.enabled = 1u;
         c.prefixBounces = t->cachePrefix;
+        c.spreadFactor = t->cacheSpread;
         const double wave = static_cast<double>(std::min<uint64_t>(call.pathsNeeded, call.paths.wavePaths));
         c.trainThreshold = static_cast<uint32_t>(std::min(4294967295.0, double(t->cacheTrainingPaths) / wave * 4294967296.0));
         c.sceneMin = t->sceneMin;
@@ -2510,6 +2513,14 @@ HDCX_API hdcx_status hdcx_set_radiance_cache(hdcx_tracer* t, hdcx_nrc* cache, ui
     t->cacheTrainingPaths = trainingPaths;
     t->cacheRun = CacheRun{};
     t->cacheRun.trainSteps = std::max(trainSteps, 1u);
+    return HDCX_OK;
+}
+
+HDCX_API hdcx_status hdcx_set_radiance_cache_spread(hdcx_tracer* t, float factor)
+{
+    if (!t) return HDCX_ERROR_INVALID_ARGUMENT;
+    if (!(factor >= 0.0F && factor <= 1e6F)) return fail(t, HDCX_ERROR_INVALID_ARGUMENT, "spread factor must be in [0, 1e6]");
+    t->cacheSpread = factor;
     return HDCX_OK;
 }
 

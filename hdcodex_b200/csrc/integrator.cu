@@ -470,7 +470,23 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             const float3 tangent = surfaceTangent(normal, p0, p1, p2, uv0, uv1, uv2);
             if (kCache) {
                 const bool training = (flags & kFlagTraining) != 0u;
-                if (training || bounce >= p.cache.prefixBounces) {
+                bool terminate = bounce >= p.cache.prefixBounces;
+                if (p.cache.spreadFactor > 0.0f) {
+                    // Path spread (Mueller, Rousselle, Keller and Novak, "Real-time
+                    // Neural Radiance Caching for Path Tracing", 2021, sec. 3.4):
+                    // a(x1..xn) = (sum over i >= 2 of sqrt(|x(i-1) - xi|^2 /
+                    // (p(wi) |cos(theta_i)|)))^2 against the primary footprint
+                    // a0 = |x0 - x1|^2 / (4 pi |cos(theta_1)|); the path ends
+                    // once a > c a0. A specular bounce (infinite pdf) adds nothing.
+                    const float cosine = fmaxf(fabsf(dot(geometricNormal, rayDirection)), 1e-6f);
+                    const float d2 = distance * distance;
+                    float2 spread = bounce == 0u ? make_float2(d2 / (12.566370614f * cosine), 0.0f) : p.cache.spread[slot];
+                    if (bounce > 0u && !previousWasDelta && previousBsdfPdf > 0.0f)
+                        spread.y += sqrtf(d2 / (previousBsdfPdf * cosine));
+                    p.cache.spread[slot] = spread;
+                    terminate = terminate || spread.y * spread.y > p.cache.spreadFactor * spread.x;
+                }
+                if (training || terminate) {
                     const float3 qp = (hit - p.cache.sceneMin) * p.cache.sceneScale;
                     const float4 q0 = make_float4(qp.x, qp.y, qp.z, -rayDirection.x);
                     const float4 q1 = make_float4(-rayDirection.y, -rayDirection.z, normal.x, normal.y);

@@ -16,7 +16,9 @@ namespace hdcx {
 constexpr uint32_t kCacheMaxVertices = 12;  // HDCX_MAX_PATH_BOUNCES
 struct CacheDevice {
     uint32_t enabled = 0;
-    uint32_t prefixBounces = 2;
+    uint32_t prefixBounces = 2;   // paths end at this bounce at the latest
+    float spreadFactor = 0.0f;    // > 0: also end once the path's spread exceeds it x the primary footprint
+    float2* spread = nullptr;     // per path: primary footprint a0, sum of sqrt spread terms
     uint32_t trainThreshold = 0;  // a path trains when its identity hash < this
     uint32_t trainCapacity = 0;   // training paths per wave
     float3 sceneMin{};            // query positions are (hit - sceneMin) * sceneScale, in [0, 1]

@@ -66,6 +66,7 @@ SIGNATURES = {
                                 C.POINTER(_abi.Tuning)]),
     "hdcx_set_radiance_cache": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32]),
     "hdcx_get_radiance_cache_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
+    "hdcx_set_radiance_cache_spread": (C.c_int, [_P, C.c_float]),
     "hdcx_nrc_defaults": (None, [C.POINTER(_abi.NrcConfig)]),
     "hdcx_nrc_create": (C.c_int, [C.c_int32, C.POINTER(_abi.NrcConfig), C.POINTER(C.c_void_p)]),
     "hdcx_nrc_destroy": (None, [_P]),
@@ -333,6 +334,13 @@ class PathTracer:
         """Attach a RadianceCache (None detaches it)."""
         self._check(lib().hdcx_set_radiance_cache(self._h, cache.handle if cache is not None else None, prefix_bounces,
                                                   training_paths, train_steps), "set_radiance_cache")
+
+    def set_radiance_cache_spread(self, factor):
+        """hdcx_set_radiance_cache_spread: with factor c > 0, cache-mode paths
+        also end at the first vertex where their spread exceeds c times the
+        primary footprint (Mueller et al. 2021; the paper uses c = 0.01); the
+        prefix stays the latest bounce. 0 ends paths by the prefix alone."""
+        self._check(lib().hdcx_set_radiance_cache_spread(self._h, factor), "set_radiance_cache_spread")
 
     def autotune(self, camera, width, height, max_bounces=8, sample_count=1) -> dict:
         """hdcx_autotune: picks the hit sort, wave size and grid sizes for this

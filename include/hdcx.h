@@ -768,6 +768,16 @@ HDCX_API hdcx_status hdcx_nrc_set_parameters(hdcx_nrc* cache, const float* mlp, 
  * this mode synchronise with the host once per wave. */
 HDCX_API hdcx_status hdcx_set_radiance_cache(hdcx_tracer* tracer, hdcx_nrc* cache, uint32_t prefix_bounces,
                                              uint32_t training_paths, uint32_t train_steps);
+/* Path termination by spread (Mueller et al., "Real-time Neural Radiance
+ * Caching for Path Tracing", 2021, sec. 3.4): with factor c > 0 a
+ * cache-mode path also ends, and queries the cache, at the first vertex
+ * where its spread a(x1..xn) = (sum_i sqrt(|x(i-1) - xi|^2 / (p(wi)
+ * |cos(theta_i)|)))^2 exceeds c times the primary footprint |x0 - x1|^2 /
+ * (4 pi |cos(theta_1)|); specular bounces add nothing, so specular chains
+ * continue to a rough vertex. prefix_bounces stays the latest bounce. The
+ * paper's c is 0.01; 0 (the default) ends paths by the prefix alone. No
+ * counterpart in the reference (it has no radiance cache). */
+HDCX_API hdcx_status hdcx_set_radiance_cache_spread(hdcx_tracer* tracer, float factor);
 /* Totals since the cache was attached: queries answered, training samples
  * used, and the mean loss of the last training step. */
 HDCX_API hdcx_status hdcx_get_radiance_cache_stats(const hdcx_tracer* tracer, uint64_t* queries, uint64_t* samples,

@@ -66,3 +66,37 @@ def test_trained_cache_recovers_the_truncated_light(box, reference):
     assert truncated[..., :3].mean() < 0.95 * mean_ref  # the prefix alone is missing light
     assert e_cached < 0.6 * e_truncated, (e_cached, e_truncated)
     assert abs(cached[..., :3].mean() / mean_ref - 1.0) < 0.1
+
+
+def test_spread_termination(box, reference):
+    """Paths ended by the spread heuristic (Mueller et al. 2021): a factor
+    that never triggers leaves the prefix-only render unchanged bit for bit;
+    with the paper's c = 0.01 paths end at the first vertex after a diffuse
+    bounce (in the all-diffuse box: nearly every path at bounce 1), and the
+    trained cache recovers the light beyond the direct lighting."""
+    def run(spread, frames=48, spp=32, prefix=2):
+        with PathTracer(0) as t, RadianceCache(0, log2_table_size=16, finest_resolution=256, seed=5) as cache:
+            t.set_scene(box.scene)
+            t.set_radiance_cache(cache, prefix_bounces=prefix, training_paths=4096, train_steps=2)
+            t.set_radiance_cache_spread(spread)
+            for frame in range(frames):
+                t.render(box.camera, W, H, frame, 8, 1)
+            img = None
+            for frame in range(spp):
+                img = t.render(box.camera, W, H, frame, 8, 1)
+            return img.copy(), t.radiance_cache_stats()
+
+    prefix_only, st_prefix = run(0.0, frames=4, spp=4)
+    never, st_never = run(1e6, frames=4, spp=4)
+    assert np.array_equal(prefix_only, never)
+    assert st_prefix["queries"] == st_never["queries"]
+    spread, _ = run(0.01, prefix=4)
+    assert np.isfinite(spread).all()
+    with PathTracer(0) as t:
+        t.set_scene(box.scene)
+        direct = t.render(box.camera, W, H, 0, 1, 32)  # one bounce, no cache: direct light only
+    assert rel_rmse(spread, reference) < 0.6 * rel_rmse(direct, reference)
+    assert abs(spread[..., :3].mean() / reference[..., :3].mean() - 1.0) < 0.1
+    with PathTracer(0) as t:
+        with pytest.raises(RuntimeError):
+            t.set_radiance_cache_spread(-1.0)
