@@ -559,6 +559,23 @@ def run_nrc(args):
                 "curve": curve[:: max(1, len(curve) // 24)] + curve[-1:], "cache_stats": stats}
 
     plain = converge(None)
+
+    def ms_per_spp(max_bounces, spp=32):
+        # Cost of a sample of the plain integrator with paths cut after
+        # `max_bounces` bounces: no cache arm ending paths there can be cheaper.
+        with PathTracer(0) as t:
+            t.set_scene(wl.scene)
+            t.set_tuning(**tuning)
+            t.render_device(wl.camera, w, h, 0, max_bounces, args.chunk_spp)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for k in range(0, spp, args.chunk_spp):
+                t.render_device(wl.camera, w, h, k, max_bounces, args.chunk_spp)
+            torch.cuda.synchronize()
+            return 1e3 * (time.perf_counter() - t0) / spp
+
+    cost_bounds = {"plain_8_bounces": ms_per_spp(wl.max_bounces), "plain_cut_after_2": ms_per_spp(2),
+                   "plain_cut_after_1": ms_per_spp(1)}
     prefixes = [int(x) for x in str(args.nrc_prefix).split(",") if x.strip()]
     arms = {}
     for prefix in prefixes:
@@ -605,6 +622,12 @@ def run_nrc(args):
                                      "ratio_to_plain": (v["seconds"] / plain["seconds"])
                                      if (v["seconds"] and plain["seconds"]) else None}
                             for k, v in arms.items()},
+        "ms_per_spp": {"plain": 1e3 * plain["seconds"] / plain["spp"] if plain["seconds"] else None,
+                       **{f"cache_prefix_{k}": 1e3 * v["seconds"] / v["spp"] if v["seconds"] else None
+                          for k, v in arms.items()},
+                       **{f"cache_spread_{k:g}": 1e3 * v["seconds"] / v["spp"] if v["seconds"] else None
+                          for k, v in spread_arms.items()},
+                       "bounds_without_cache": cost_bounds},
         "cache_by_spread": {f"c={k:g}, latest bounce {args.nrc_spread_cap}": {
             "seconds": v["seconds"], "spp": v["spp"], "final_rel_rmse": v["final_rel_rmse"],
             "ratio_to_plain": (v["seconds"] / plain["seconds"]) if (v["seconds"] and plain["seconds"]) else None,

@@ -397,7 +397,7 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
         node.qhix[s] = qh[0]; node.qhiy[s] = qh[1]; node.qhiz[s] = qh[2];
         if (!isLeaf(b) && count(b) > kMaxLeafTriangles) {
             node.imask |= static_cast<uint8_t>(1u << s);
-            node.meta[s] = 0xffu;
+            node.meta[s] = 0;  // internal children carry no triangle bits
             const uint32_t slot = atomicAdd(nextCount, 1u);
             nextItems[slot] = CollapseItem{b, childBase + static_cast<uint32_t>(internalRank), item.depth + 1u, 0u};
             internalRank++;

@@ -105,8 +105,9 @@ struct TexDesc {
 // compressed wide node of Ylitie, Karras and Laine, "Efficient Incoherent Ray
 // Traversal on GPUs Through Compressed Wide BVHs", HPG 2017: origin p,
 // power-of-two scale exponents, internal-child mask, base indices of the
-// internal children and of the leaf triangles, one meta byte per slot and six
-// quantised planes per child.
+// internal children and of the leaf triangles, one meta byte per slot (leaf
+// children: unary triangle count << 5 | first triangle; internal and empty
+// children: 0) and six quantised planes per child.
 struct __align__(16) WideNode {
     float px, py, pz;
     uint8_t ex, ey, ez, imask;

@@ -18,10 +18,8 @@
 //   and pending node groups go on a per-thread stack. Child boxes are padded
 //   by one quantisation step on every side at build time, which keeps the
 //   binary32 slab test conservative. The 48 plane distances of a node are
-//   evaluated two children at a time with the packed binary32 instructions
-//   of sm_100 (__fadd2_rn, __ffma2_rn): each half is the same IEEE operation
-//   as the scalar form, so the node test's results are unchanged, in fewer
-//   instructions.
+//   evaluated two children at a time with the packed fused multiply-add of
+//   sm_100 (__ffma2_rn), the slab intervals with its three-input min/max.
 // * Faults: a node group that finds the stack full, or a traversal that
 //   visits more nodes than the BVH holds (a malformed node array), sets a
 //   bit in the traversal's fault word; the kernels OR it into the render's
@@ -121,22 +119,45 @@ HDCX_D bool intersectTriangle(const RayPre& r, float3 v0, float3 v1, float3 v2, 
 }
 
 // Byte `index` of `word` as the float 2^23 + byte: the byte is placed in the
-// low mantissa bits of 2^23 (bit pattern 0x4B0000bb). Subtracting 2^23 then
-// gives the byte's value exactly. A byte permute and an add run on full-rate
-// pipes, where an integer-to-float conversion would queue on the
-// quarter-rate conversion pipe (eight children x six planes per node).
+// low mantissa bits of 2^23 (bit pattern 0x4B0000bb), exactly. A byte permute
+// runs on a full-rate pipe, where an integer-to-float conversion would queue
+// on the quarter-rate conversion pipe (eight children x six planes per node).
 HDCX_D float biasedByte(uint32_t word, int index)
 {
     return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u + static_cast<uint32_t>(index)));
 }
 
 // Quantised planes of children 2j and 2j+1 (bytes k and k+1 of `word`, k
-// even) as distances t = q * a + b, two lanes per packed instruction.
-HDCX_D float2 planePair(uint32_t word, int k, float2 a, float2 b)
+// even) as distances t = (2^23 + q) * a + c, with c = b - 2^23 * a, two lanes
+// per packed fused multiply-add.
+HDCX_D float2 planePair(uint32_t word, int k, float2 a, float2 c)
 {
-    const float2 q = __fadd2_rn(make_float2(biasedByte(word, k), biasedByte(word, k + 1)),
-                                make_float2(-8388608.0f, -8388608.0f));
-    return __ffma2_rn(q, a, b);
+    return __ffma2_rn(make_float2(biasedByte(word, k), biasedByte(word, k + 1)), a, c);
+}
+
+// Three-input minimum and maximum of sm_100 (PTX min/max with three f32
+// operands): one instruction where two-input forms take two.
+HDCX_D float max3(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+HDCX_D float min3(float a, float b, float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Moves bit i of an 8-bit mask to bit i ^ x (x in 0..7): three conditional
+// swaps, of neighbouring bits, bit pairs and nibbles.
+HDCX_D uint32_t permuteSlots(uint32_t m, uint32_t x)
+{
+    if (x & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+    if (x & 2u) m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+    if (x & 4u) m = ((m & 0x0fu) << 4) | ((m >> 4) & 0x0fu);
+    return m;
 }
 
 // State of one ray's traversal: the ray, the closest confirmed hit so far,
@@ -187,6 +208,15 @@ HDCX_D void beginTraversal(Traversal& st, const DeviceScene& s, float3 o, float3
 // inverse direction id, octant mask octInv) up to bestT: hit internal
 // children become nodeGroup (hit bits in 24..31 by visiting order | imask),
 // hit leaf triangles triGroup (first slot, bits).
+//
+// A plane at quantised coordinate q lies at t = q * a + b along the ray, with
+// a = scale * id and b = (p - o) * id. The byte arrives as the float 2^23 + q
+// (biasedByte), so the offset is folded once per node: c = b - 2^23 * a,
+// rounded once, an error of at most half of |a|, half a quantisation step.
+// The build pads every child box by one step on each side, which covers it:
+// the test stays conservative, and only which nodes are entered depends on
+// it, never a hit. The folded offset is finite for nodes narrower than about
+// 2^32 scene units (|a| * 2^23 below the binary32 range with |id| <= 2^80).
 template <bool kMargin>
 HDCX_D void testNode(const WideNode* nodes, uint32_t nodeIndex, float3 o, float idx, float idy, float idz,
                      uint32_t octInv, float bestT, float mx, float my, float mz, uint2& nodeGroup, uint2& triGroup)
@@ -199,19 +229,17 @@ HDCX_D void testNode(const WideNode* nodes, uint32_t nodeIndex, float3 o, float 
     const float scy = __uint_as_float(((e >> 8) & 0xffu) << 23);
     const float scz = __uint_as_float(((e >> 16) & 0xffu) << 23);
     const uint32_t imask = e >> 24;
-    // t = q * (scale * invd) + (p - o) * invd per plane.
     const float ax = scx * idx, ay = scy * idy, az = scz * idz;
     const float bx = (px - o.x) * idx, by = (py - o.y) * idy, bz = (pz - o.z) * idz;
-    const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
+    constexpr float kBias = -8388608.0f;  // -2^23
     // With kMargin every box is widened by (mx, my, mz) in t per axis: the
     // near plane's distance drops by the margin, the far plane's grows.
-    const float2 bxn = kMargin ? make_float2(bx - mx, bx - mx) : make_float2(bx, bx);
-    const float2 byn = kMargin ? make_float2(by - my, by - my) : make_float2(by, by);
-    const float2 bzn = kMargin ? make_float2(bz - mz, bz - mz) : make_float2(bz, bz);
-    const float2 bxf = kMargin ? make_float2(bx + mx, bx + mx) : make_float2(bx, bx);
-    const float2 byf = kMargin ? make_float2(by + my, by + my) : make_float2(by, by);
-    const float2 bzf = kMargin ? make_float2(bz + mz, bz + mz) : make_float2(bz, bz);
-    // Near/far planes by direction sign: words of qlo (n2.x..n3.y) and qhi (n3.z..n4.w).
+    const float cxn = fmaf(kBias, ax, kMargin ? bx - mx : bx), cxf = kMargin ? fmaf(kBias, ax, bx + mx) : cxn;
+    const float cyn = fmaf(kBias, ay, kMargin ? by - my : by), cyf = kMargin ? fmaf(kBias, ay, by + my) : cyn;
+    const float czn = fmaf(kBias, az, kMargin ? bz - mz : bz), czf = kMargin ? fmaf(kBias, az, bz + mz) : czn;
+    const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
+    const float2 cxn2 = make_float2(cxn, cxn), cyn2 = make_float2(cyn, cyn), czn2 = make_float2(czn, czn);
+    const float2 cxf2 = make_float2(cxf, cxf), cyf2 = make_float2(cyf, cyf), czf2 = make_float2(czf, czf);
     const uint32_t loX0 = n2.x, loX1 = n2.y, loY0 = n2.z, loY1 = n2.w, loZ0 = n3.x, loZ1 = n3.y;
     const uint32_t hiX0 = n3.z, hiX1 = n3.w, hiY0 = n4.x, hiY1 = n4.y, hiZ0 = n4.z, hiZ1 = n4.w;
     const bool sx = idx >= 0.0f, sy = idy >= 0.0f, sz = idz >= 0.0f;
@@ -219,32 +247,35 @@ HDCX_D void testNode(const WideNode* nodes, uint32_t nodeIndex, float3 o, float 
     const uint32_t nearY0 = sy ? loY0 : hiY0, nearY1 = sy ? loY1 : hiY1, farY0 = sy ? hiY0 : loY0, farY1 = sy ? hiY1 : loY1;
     const uint32_t nearZ0 = sz ? loZ0 : hiZ0, nearZ1 = sz ? loZ1 : hiZ1, farZ0 = sz ? hiZ0 : loZ0, farZ1 = sz ? hiZ1 : loZ1;
     const uint32_t meta0 = n1.z, meta1 = n1.w;
-    uint32_t nodeHits = 0u, triHits = 0u;
-    // Children 2j and 2j+1 share a word per plane (bytes k and k+1). An
-    // empty slot has meta 0 and is not internal, so it adds no bits.
+    uint32_t hits = 0u, triHits = 0u;
+    // Children 2j and 2j+1 share a word per plane (bytes k and k+1). The meta
+    // byte of a leaf child is its unary triangle count << 5 | first triangle;
+    // internal and empty children have meta 0 and add no triangle bits.
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int k = (2 * j) & 3;
         const bool low = j < 2;
-        const float2 tnx = planePair(low ? nearX0 : nearX1, k, ax2, bxn);
-        const float2 tny = planePair(low ? nearY0 : nearY1, k, ay2, byn);
-        const float2 tnz = planePair(low ? nearZ0 : nearZ1, k, az2, bzn);
-        const float2 tfx = planePair(low ? farX0 : farX1, k, ax2, bxf);
-        const float2 tfy = planePair(low ? farY0 : farY1, k, ay2, byf);
-        const float2 tfz = planePair(low ? farZ0 : farZ1, k, az2, bzf);
+        const float2 tnx = planePair(low ? nearX0 : nearX1, k, ax2, cxn2);
+        const float2 tny = planePair(low ? nearY0 : nearY1, k, ay2, cyn2);
+        const float2 tnz = planePair(low ? nearZ0 : nearZ1, k, az2, czn2);
+        const float2 tfx = planePair(low ? farX0 : farX1, k, ax2, cxf2);
+        const float2 tfy = planePair(low ? farY0 : farY1, k, ay2, cyf2);
+        const float2 tfz = planePair(low ? farZ0 : farZ1, k, az2, czf2);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int i = 2 * j + h;
-            const uint32_t meta = ((low ? meta0 : meta1) >> (8 * (k + h))) & 0xffu;
-            const float tNear = fmaxf(fmaxf(h ? tnx.y : tnx.x, h ? tny.y : tny.x), fmaxf(h ? tnz.y : tnz.x, 0.0f));
-            const float tFar = fminf(fminf(h ? tfx.y : tfx.x, h ? tfy.y : tfy.x), fminf(h ? tfz.y : tfz.x, bestT));
+            const uint32_t metaShift = (low ? meta0 : meta1) >> (8 * (k + h));  // low 5 bits: first triangle
+            const uint32_t tris = __funnelshift_l(0u, (metaShift >> 5) & 7u, metaShift);
+            const float tNear = max3(h ? tnx.y : tnx.x, h ? tny.y : tny.x, fmaxf(h ? tnz.y : tnz.x, 0.0f));
+            const float tFar = min3(h ? tfx.y : tfx.x, h ? tfy.y : tfy.x, fminf(h ? tfz.y : tfz.x, bestT));
             if (tNear <= tFar) {
-                if ((imask >> i) & 1u) nodeHits |= 1u << (static_cast<uint32_t>(i) ^ octInv);
-                else triHits |= (meta >> 5) << (meta & 31u);
+                hits |= 1u << i;
+                triHits |= tris;
             }
         }
     }
-    nodeGroup = make_uint2(n1.x, (nodeHits << 24) | imask);
+    // Internal children in visiting order: bit i goes to i ^ octInv.
+    nodeGroup = make_uint2(n1.x, (permuteSlots(hits & imask, octInv) << 24) | imask);
     triGroup = make_uint2(n1.y, triHits);
 }
 

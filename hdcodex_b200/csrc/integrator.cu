@@ -340,7 +340,32 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
     static_assert(kWalk == kWalkInline || (kFull && !kCache), "deferred walks are for the full plain kernel");
     const uint32_t n = *count;
     const bool lastBounce = bounce + 1u >= f.maxBounces;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    // Closure staging: with hits sorted by material (tuning sort_hits) a
+    // block's consecutive hits mostly share one material. Its 368-byte
+    // record is copied once per block iteration into shared memory, 16 bytes
+    // per thread, and every thread whose hit uses it reads it from there;
+    // other hits read theirs from global memory. Every thread of the block
+    // runs the same iterations (the loop steps by block, not by thread).
+    constexpr bool kStageable = kFull && !kCache && !kReplay;
+    const bool stage = kStageable && p.sortHits != 0u;
+    __shared__ __align__(16) GpuMaterial stagedMaterial;
+    __shared__ uint32_t stagedIndex;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        if (stage) {
+            __syncthreads();  // the previous iteration's reads of the staged record are done
+            if (threadIdx.x == 0) {
+                const uint32_t first = __float_as_uint(p.hit[queue[base]].y);
+                stagedIndex = first == kInvalidPrimitive ? 0xffffffffu : __ldg(s.triangleMaterials + first);
+            }
+            __syncthreads();
+            if (stagedIndex != 0xffffffffu && threadIdx.x < sizeof(GpuMaterial) / sizeof(uint4)) {
+                reinterpret_cast<uint4*>(&stagedMaterial)[threadIdx.x] =
+                    __ldg(reinterpret_cast<const uint4*>(s.materials + stagedIndex) + threadIdx.x);
+            }
+            __syncthreads();
+        }
+        const uint32_t i = base + threadIdx.x;
+        if (i >= n) continue;
         const uint32_t slot = queue[i];
         float radiance = p.radiance[slot];
         // Light-sample contributions of the previous bounce, in slot order.
@@ -438,7 +463,9 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                 }
                 throughput = throughput * gexp(-mediumAbsorption * distance);
             }
-            const GpuMaterial* material = s.materials + __ldg(s.triangleMaterials + primitive);
+            const uint32_t materialIndex = __ldg(s.triangleMaterials + primitive);
+            const GpuMaterial* material =
+                (stage && materialIndex == stagedIndex) ? &stagedMaterial : s.materials + materialIndex;
             float3 baseColorRgb = xyz(material->baseColorMetalness);
             if (kFull && material->textureIndices0.x != kMissingTexture) {
                 const float4 sample = materialTexture<kFull>(lodBase, s, material->textureIndices0.x, surfaceUv, f4(baseColorRgb, 1.0f));

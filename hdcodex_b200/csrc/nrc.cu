@@ -182,41 +182,25 @@ __device__ __forceinline__ void levelCorners(const DeviceParams& p, int level, f
 }
 
 // The 64 network inputs of query record q (zeros for a missing query).
-// The 128 table taps are gathered four levels at a time: the 32 loads of a
-// group are issued before any is used, so a thread keeps 32 gathers in
-// flight instead of 8 (the encoding waits on L2 latency, not bandwidth).
-// Each level's sums are formed in the same order as a level at a time.
-__device__ __forceinline__ void encodeQuery(const DeviceParams& p, const float* q, float in[kWidth])
+__device__ void encodeQuery(const DeviceParams& p, const float* q, float in[kWidth])
 {
 #pragma unroll
     for (int i = 0; i < kWidth; ++i) in[i] = 0.0f;
     if (!q) return;
     const float3 pos = make_float3(q[0], q[1], q[2]);
-    constexpr int kGroup = 4;
+    for (int level = 0; level < kLevels; ++level) {
+        uint32_t index[8];
+        float weight[8];
+        levelCorners(p, level, pos, index, weight);
+        float f0 = 0.0f, f1 = 0.0f;
 #pragma unroll
-    for (int level0 = 0; level0 < kLevels; level0 += kGroup) {
-        uint32_t index[kGroup][8];
-        float weight[kGroup][8];
-        __half2 tap[kGroup][8];
-#pragma unroll
-        for (int g = 0; g < kGroup; ++g) levelCorners(p, level0 + g, pos, index[g], weight[g]);
-#pragma unroll
-        for (int g = 0; g < kGroup; ++g) {
-#pragma unroll
-            for (int c = 0; c < 8; ++c) tap[g][c] = __ldg(p.grid + index[g][c]);
+        for (int c = 0; c < 8; ++c) {
+            const float2 v = __half22float2(p.grid[index[c]]);
+            f0 = fmaf(weight[c], v.x, f0);
+            f1 = fmaf(weight[c], v.y, f1);
         }
-#pragma unroll
-        for (int g = 0; g < kGroup; ++g) {
-            float f0 = 0.0f, f1 = 0.0f;
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const float2 v = __half22float2(tap[g][c]);
-                f0 = fmaf(weight[g][c], v.x, f0);
-                f1 = fmaf(weight[g][c], v.y, f1);
-            }
-            in[2 * (level0 + g)] = f0;
-            in[2 * (level0 + g) + 1] = f1;
-        }
+        in[2 * level] = f0;
+        in[2 * level + 1] = f1;
     }
 #pragma unroll
     for (int i = 0; i < 9; ++i) in[32 + i] = q[3 + i];

@@ -70,7 +70,7 @@ def test_trained_cache_recovers_the_truncated_light(box, reference):
 
 def test_spread_termination(box, reference):
     """Paths ended by the spread heuristic (Mueller et al. 2021): a factor
-    that never triggers leaves the prefix-only render unchanged bit for bit;
+    that never triggers ends the same paths as the prefix alone;
     with the paper's c = 0.01 paths end at the first vertex after a diffuse
     bounce (in the all-diffuse box: nearly every path at bounce 1), and the
     trained cache recovers the light beyond the direct lighting."""
@@ -88,8 +88,10 @@ def test_spread_termination(box, reference):
 
     prefix_only, st_prefix = run(0.0, frames=4, spp=4)
     never, st_never = run(1e6, frames=4, spp=4)
-    assert np.array_equal(prefix_only, never)
+    # The same paths end at the same vertices; the images differ only by the
+    # order of the training's atomic gradient sums (not bit-reproducible).
     assert st_prefix["queries"] == st_never["queries"]
+    assert rel_rmse(never, prefix_only) < 1e-2
     spread, _ = run(0.01, prefix=4)
     assert np.isfinite(spread).all()
     with PathTracer(0) as t:
