@@ -314,8 +314,8 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
 // three; each costs a few spilled values and gains 4-6% of the kernel's time.
 //
 // kWalk: how a subsurface random walk (:1153-1186) runs.
-//   kWalkInline - inside this kernel, nested in shading (the radiance-cache
-//                 mode and renders without walk buffers);
+//   kWalkInline - inside this kernel, nested in shading (renders without
+//                 walk buffers);
 //   kWalkDefer  - the walk's start (entry, normal, mean free path, albedo,
 //                 anisotropy, RNG state, throughput) is recorded and the path
 //                 handed to walkKernel, a traversal kernel; everything before
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                 const uint32_t* count, uint32_t* nextQueue, uint32_t* nextCount)
 {
     constexpr bool kReplay = kWalk == kWalkReplay;
-    static_assert(kWalk == kWalkInline || (kFull && !kCache), "deferred walks are for the full plain kernel");
+    static_assert(kWalk == kWalkInline || kFull, "deferred walks are for the full kernels");
     const uint32_t n = *count;
     const bool lastBounce = bounce + 1u >= f.maxBounces;
     // Closure staging: with hits sorted by material (tuning sort_hits) a
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
     // per thread, and every thread whose hit uses it reads it from there;
     // other hits read theirs from global memory. Every thread of the block
     // runs the same iterations (the loop steps by block, not by thread).
-    constexpr bool kStageable = kFull && !kCache && !kReplay;
+    constexpr bool kStageable = kFull && !kReplay;
     const bool stage = kStageable && p.sortHits != 0u;
     __shared__ __align__(16) GpuMaterial stagedMaterial;
     __shared__ uint32_t stagedIndex;
@@ -495,7 +495,9 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
             if (kFull) normal = applyNormalMap(s, material->textureIndices1.y, material->coatWeightRoughnessIor.w > 0.5f,
                                     material->subsurfaceWeightScale.w, surfaceUv, normal, p0, p1, p2, uv0, uv1, uv2);
             const float3 tangent = surfaceTangent(normal, p0, p1, p2, uv0, uv1, uv2);
-            if (kCache) {
+            // (A replay re-shades a bounce whose first pass went past this
+            // point without ending the path and has recorded its vertex.)
+            if (kCache && !kReplay) {
                 const bool training = (flags & kFlagTraining) != 0u;
                 bool terminate = bounce >= p.cache.prefixBounces;
                 if (p.cache.spreadFactor > 0.0f) {
@@ -1038,7 +1040,8 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS)
                                  exitDirection, attenuation)) {
             p.rng[slot] = rng;
             p.throughput[slot] = state.z * attenuation;
-            p.flags[slot] = kFlagEnvironmentOnMiss | kFlagPreviousWasDelta | (p.flags[slot] & kFlagInsideMedium);
+            p.flags[slot] = kFlagEnvironmentOnMiss | kFlagPreviousWasDelta |
+                            (p.flags[slot] & (kFlagInsideMedium | kFlagTraining));
             p.previousPdf[slot] = make_float2(0.0f, p.previousPdf[slot].y);
             p.rayOrigin[slot] = make_float4(exitOrigin.x, exitOrigin.y, exitOrigin.z, 0.0f);
             p.rayDirection[slot] = make_float4(exitDirection.x, exitDirection.y, exitDirection.z, 0.0f);
@@ -1494,11 +1497,11 @@ void launchShadow(const DeviceScene& scene, PathBuffers& paths, bool count, int 
     }
 }
 
-// Whether the full shade kernel defers subsurface walks to walkKernel: the
-// plain (non-cache) mode with walk buffers.
-bool deferWalks(const PathBuffers& paths, bool cacheMode)
+// Whether the full shade kernels defer subsurface walks to walkKernel: path
+// buffers with walk buffers (plain and radiance-cache mode alike).
+bool deferWalks(const PathBuffers& paths)
 {
-    return !cacheMode && paths.walkEntry != nullptr && paths.walkNormal != nullptr && paths.walkState != nullptr;
+    return paths.walkEntry != nullptr && paths.walkNormal != nullptr && paths.walkState != nullptr;
 }
 
 template <bool kCache>
@@ -1507,9 +1510,9 @@ void launchShade(const DeviceScene& scene, const FrameConst& frame, PathBuffers&
 {
     const bool lit = scene.lightCount > 0u && !scene.hasMeshLights;
     if (scene.fullShading) {
-        if (!kCache && deferWalks(paths, kCache)) {
-            if (lit) shadeKernel<true, true, false, kWalkDefer><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
-            else shadeKernel<true, false, false, kWalkDefer><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+        if (deferWalks(paths)) {
+            if (lit) shadeKernel<true, true, kCache, kWalkDefer><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
+            else shadeKernel<true, false, kCache, kWalkDefer><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
         } else if (lit) {
             shadeKernel<true, true, kCache><<<grid, 128, 0, stream>>>(scene, frame, paths, bounce, inQueue, inCount, outQueue, outCount);
         } else {
@@ -1538,8 +1541,8 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
     const int missGrid = gridFor(static_cast<uint32_t>(wavePaths), 8);
     const bool sortHits = paths.sortHits != 0u && paths.sortedHits != nullptr && paths.hitBins != nullptr;
     const bool sortRays = paths.sortRays != 0u;
-    // Subsurface walks in walkKernel (scenes that can take them, plain mode).
-    const bool walks = scene.fullShading && scene.hasSubsurface && deferWalks(paths, cacheMode);
+    // Subsurface walks in walkKernel (scenes that can take them).
+    const bool walks = scene.fullShading && scene.hasSubsurface && deferWalks(paths);
     const int sortGrid = std::max(1, gridFor(static_cast<uint32_t>(wavePaths), 8) / 2);  // 256-thread blocks
     std::vector<EventPair> events;
     auto timed = [&](int stage, auto&& launch) {
@@ -1597,12 +1600,14 @@ void renderFrame(const DeviceScene& sceneIn, const FrameConst& frame, PathBuffer
                     if (scene.instances) walkKernel<1><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, outQueue, outCount, paths.missQueue);
                     else walkKernel<0><<<traceGrid, 128, 0, stream>>>(scene, paths, inQueue, outQueue, outCount, paths.missQueue);
                     const bool lit = scene.lightCount > 0u && !scene.hasMeshLights;
-                    if (lit) {
-                        shadeKernel<true, true, false, kWalkReplay><<<missGrid, 128, 0, stream>>>(
-                            scene, frame, paths, bounce, paths.missQueue, paths.counters + 7, outQueue, outCount);
+                    const uint32_t* replays = paths.missQueue;
+                    const uint32_t* replayCount = paths.counters + 7;
+                    if (cacheMode) {
+                        if (lit) shadeKernel<true, true, true, kWalkReplay><<<missGrid, 128, 0, stream>>>(scene, frame, paths, bounce, replays, replayCount, outQueue, outCount);
+                        else shadeKernel<true, false, true, kWalkReplay><<<missGrid, 128, 0, stream>>>(scene, frame, paths, bounce, replays, replayCount, outQueue, outCount);
                     } else {
-                        shadeKernel<true, false, false, kWalkReplay><<<missGrid, 128, 0, stream>>>(
-                            scene, frame, paths, bounce, paths.missQueue, paths.counters + 7, outQueue, outCount);
+                        if (lit) shadeKernel<true, true, false, kWalkReplay><<<missGrid, 128, 0, stream>>>(scene, frame, paths, bounce, replays, replayCount, outQueue, outCount);
+                        else shadeKernel<true, false, false, kWalkReplay><<<missGrid, 128, 0, stream>>>(scene, frame, paths, bounce, replays, replayCount, outQueue, outCount);
                     }
                 }
             });
