@@ -562,7 +562,11 @@ def run_nrc(args):
 
     def ms_per_spp(max_bounces, spp=32):
         # Cost of a sample of the plain integrator with paths cut after
-        # `max_bounces` bounces: no cache arm ending paths there can be cheaper.
+        # `max_bounces` bounces. A cache arm whose paths end at bounce p
+        # traces p + 1 extension rounds (the last finds the vertex that
+        # queries the cache) and shades p full vertices: its cost lies between
+        # the cuts after p and after p + 1 bounces, plus the cache's queries
+        # and training.
         with PathTracer(0) as t:
             t.set_scene(wl.scene)
             t.set_tuning(**tuning)
@@ -574,8 +578,8 @@ def run_nrc(args):
             torch.cuda.synchronize()
             return 1e3 * (time.perf_counter() - t0) / spp
 
-    cost_bounds = {"plain_8_bounces": ms_per_spp(wl.max_bounces), "plain_cut_after_2": ms_per_spp(2),
-                   "plain_cut_after_1": ms_per_spp(1)}
+    cost_bounds = {"plain_8_bounces": ms_per_spp(wl.max_bounces), "plain_cut_after_3": ms_per_spp(3),
+                   "plain_cut_after_2": ms_per_spp(2), "plain_cut_after_1": ms_per_spp(1)}
     prefixes = [int(x) for x in str(args.nrc_prefix).split(",") if x.strip()]
     arms = {}
     for prefix in prefixes:

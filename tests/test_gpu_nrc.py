@@ -71,6 +71,24 @@ def test_forward_matches_oracle(cache):
     assert np.abs(got - ref).max() < 5e-3 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("n", [1, 100, 129, 383, 120_001])
+def test_forward_tile_counts(cache, n):
+    """Query counts of a single partial tile (1, 100), a full tile and a
+    partial one (129, 383), and more tiles than the grid holds at once, so
+    that blocks step to further tiles (120,001 queries: 938 tiles over at
+    most four blocks per SM)."""
+    import torch
+    q = queries(n, 100 + n % 97)
+    mlp, grid = cache.parameters()
+    out = torch.full((n,), float("nan"), dtype=torch.float32, device="cuda")
+    cache.query(device(q).data_ptr(), n, out.data_ptr())
+    got = out.cpu().numpy()
+    ref, _ = N.forward(q, mlp, grid, cache.resolutions(), cache.config.log2_table_size)
+    assert np.isfinite(got).all()
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-3
+    assert np.abs(got - ref).max() < 5e-3 * np.abs(ref).max()
+
+
 def test_gradients_match_oracle(cache):
     q = queries(640, 2)
     y = radiance_field(q)
