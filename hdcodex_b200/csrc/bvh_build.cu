@@ -6,13 +6,15 @@
 //   1. triangle boxes and the scene box;
 //   2. 63-bit Morton codes of the box centres, sorted with their triangle ids;
 //   3. a binary tree by PLOC agglomerative clustering in Morton order, with
-//      node boxes and triangle counts;
-//   4. a top-down collapse into 8-wide nodes: each wide node repeatedly opens
-//      its largest child that is too big for a leaf, then opens small subtrees
-//      while slots remain; children take the octant slot their centre points
-//      to, so traversal visits them nearest first; child boxes are quantised to
-//      8 bits per plane against a power-of-two step, padded by one step on
-//      every side; leaf triangles are copied in leaf order.
+//      node boxes and triangle counts, and, round by round, the SAH costs of
+//      its optimal collapse into 8-wide nodes (collapseCostKernel);
+//   4. a top-down collapse into 8-wide nodes along those costs: each wide
+//      node takes the children (subtrees or leaves of up to three triangles)
+//      of its lowest-cost distribution over eight slots; children take the
+//      octant slot their centre points to, so traversal visits them nearest
+//      first; child boxes are quantised to 8 bits per plane against a
+//      power-of-two step, padded by one step on every side; leaf triangles are
+//      copied in leaf order.
 #include "bvh_build.h"
 #include "device_memory.h"
 
@@ -211,6 +213,83 @@ __device__ __forceinline__ float surfaceArea(float4 lo, float4 hi)
     return dx * dy + dy * dz + dz * dx;
 }
 
+// ---------------------------------------------------------------------------
+// Optimal collapse of the binary tree into 8-wide nodes (Ylitie, Karras and
+// Laine, HPG 2017, sec. 3.1). For every binary node n and i = 1..7, C(n, i)
+// is the lowest SAH cost of representing n's subtree as at most i children
+// of a wide node:
+//   C(n, 1) = min(leaf: A(n) * p(n) * cPrim if p(n) <= 3 triangles,
+//                 internal: A(n) * cNode + D(n, 8))
+//   C(n, i) = min(C(n, i - 1), D(n, i))                       for i > 1
+//   D(n, j) = min over 0 < k < j of C(left, k) + C(right, j - k)
+// with A the box's surface area and p the triangle count; a binary leaf is
+// one triangle, A * cPrim for every i. The costs are filled bottom up (the
+// internal nodes of a clustering round only have children from earlier
+// rounds) and read top down by collapseKernel, which gives each wide node
+// the children D(n, 8) chose. cPrim = 0.6 cNode was measured best among 0.3
+// and 0.6 on the heavy and stress scenes (a wide-node test is some 200
+// instructions and a triangle test 80, but candidates also pay opacity
+// lookups and the closest-hit bookkeeping).
+// decision[8 n + i - 1] for i = 1..7: C(n, 1): 0 leaf, 1 internal; i > 1:
+// 0 take C(n, i - 1), else the k of D(n, i); decision[8 n + 7]: the k of D(n, 8).
+// ---------------------------------------------------------------------------
+#ifndef HDCX_COLLAPSE_PRIM_COST
+#define HDCX_COLLAPSE_PRIM_COST 0.6f
+#endif
+constexpr float kCollapseNodeCost = 1.0f;
+constexpr float kCollapsePrimCost = HDCX_COLLAPSE_PRIM_COST;
+
+__global__ void collapseCostKernel(int n, const int* left, const int* right, const float4* nodeLo, const float4* nodeHi,
+                                   uint32_t first, uint32_t last, float* cost, uint8_t* decision)
+{
+    const uint32_t node = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= last) return;
+    const int leafBase = n - 1;
+    float cl[8], cr[8];  // C(child, i) at index i = 1..7
+    auto load = [&](int b, float* c) {
+        if (b >= leafBase) {
+            const float v = kCollapsePrimCost * surfaceArea(nodeLo[b], nodeHi[b]);
+            for (int i = 1; i < 8; ++i) c[i] = v;
+        } else {
+            for (int i = 1; i < 8; ++i) c[i] = cost[7 * static_cast<size_t>(b) + (i - 1)];
+        }
+    };
+    load(left[node], cl);
+    load(right[node], cr);
+    float dist[9];
+    uint8_t split[9];
+    for (int j = 2; j <= 8; ++j) {
+        dist[j] = INFINITY;
+        split[j] = 1;
+        for (int k = 1; k < j; ++k) {
+            const float v = cl[k] + cr[j - k];
+            if (v < dist[j]) {
+                dist[j] = v;
+                split[j] = static_cast<uint8_t>(k);
+            }
+        }
+    }
+    const float area = surfaceArea(nodeLo[node], nodeHi[node]);
+    const int count = static_cast<int>(nodeLo[node].w);
+    const float internal = kCollapseNodeCost * area + dist[8];
+    const float leaf = count <= kMaxLeafTriangles ? kCollapsePrimCost * area * static_cast<float>(count) : INFINITY;
+    float* c = cost + 7 * static_cast<size_t>(node);
+    uint8_t* d = decision + 8 * static_cast<size_t>(node);
+    float previous = fminf(leaf, internal);
+    c[0] = previous;
+    d[0] = leaf <= internal ? 0u : 1u;
+    for (int i = 2; i <= 7; ++i) {
+        if (previous <= dist[i]) {
+            d[i - 1] = 0u;
+        } else {
+            previous = dist[i];
+            d[i - 1] = split[i];
+        }
+        c[i - 1] = previous;
+    }
+    d[7] = split[8];
+}
+
 __device__ __forceinline__ int ceilLog2Double(double x)
 {
     int e;
@@ -262,6 +341,7 @@ struct CollapseArgs {
     const float4* vertices;
     const uint32_t* indices;
     float sceneScale;  // max |coordinate| and scene extent, for the padding floor
+    const uint8_t* decision;  // collapseCostKernel's choices, 8 per internal binary node
     WideNode* wide;
     float4* triVerts;
     uint32_t* wideCounter;
@@ -279,47 +359,44 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
     auto isLeaf = [&](int b) { return b >= leafBase; };
     auto count = [&](int b) { return static_cast<int>(a.nodeLo[b].w); };
 
+    // A binary node becomes an internal child (a wide node of its own) when
+    // its optimal single-slot form is internal, else a leaf of <= 3 triangles.
+    auto isInternal = [&](int b) { return !isLeaf(b) && a.decision[8 * static_cast<size_t>(b)] != 0u; };
+
+    // The children of this wide node: D(node, 8) unfolded, each binary node
+    // given j slots taking C(node, j)'s choice (fewer slots, or a split).
     int entries[8];
     int m = 0;
     if (isLeaf(item.binaryNode)) {
         entries[m++] = item.binaryNode;
     } else {
-        entries[m++] = a.left[item.binaryNode];
-        entries[m++] = a.right[item.binaryNode];
-    }
-    // Phase 1: open the largest child that cannot be a leaf.
-    while (m < 8) {
-        int best = -1;
-        float bestArea = -1.0f;
-        for (int i = 0; i < m; ++i) {
-            const int b = entries[i];
-            if (!isLeaf(b) && count(b) > kMaxLeafTriangles) {
-                const float area = surfaceArea(a.nodeLo[b], a.nodeHi[b]);
-                if (area > bestArea) { bestArea = area; best = i; }
+        int pendingNode[16], pendingSlots[16];
+        int sp = 0;
+        const int k8 = a.decision[8 * static_cast<size_t>(item.binaryNode) + 7];
+        pendingNode[sp] = a.right[item.binaryNode];
+        pendingSlots[sp++] = 8 - k8;
+        pendingNode[sp] = a.left[item.binaryNode];
+        pendingSlots[sp++] = k8;
+        while (sp > 0 && m < 8) {
+            --sp;
+            const int b = pendingNode[sp];
+            int j = pendingSlots[sp];
+            if (isLeaf(b)) {
+                entries[m++] = b;
+                continue;
             }
-        }
-        if (best < 0) break;
-        const int b = entries[best];
-        entries[best] = a.left[b];
-        entries[m++] = a.right[b];
-    }
-    // Phase 2: open small subtrees while slots remain (tighter leaf boxes).
-    bool anyLarge = false;
-    for (int i = 0; i < m; ++i) anyLarge |= (!isLeaf(entries[i]) && count(entries[i]) > kMaxLeafTriangles);
-    while (m < 8 && !anyLarge) {
-        int best = -1;
-        float bestArea = -1.0f;
-        for (int i = 0; i < m; ++i) {
-            const int b = entries[i];
-            if (!isLeaf(b)) {
-                const float area = surfaceArea(a.nodeLo[b], a.nodeHi[b]);
-                if (area > bestArea) { bestArea = area; best = i; }
+            const uint8_t* d = a.decision + 8 * static_cast<size_t>(b);
+            while (j > 1 && d[j - 1] == 0u) --j;
+            if (j <= 1) {
+                entries[m++] = b;
+                continue;
             }
+            const int k = d[j - 1];
+            pendingNode[sp] = a.right[b];
+            pendingSlots[sp++] = j - k;
+            pendingNode[sp] = a.left[b];
+            pendingSlots[sp++] = k;
         }
-        if (best < 0) break;
-        const int b = entries[best];
-        entries[best] = a.left[b];
-        entries[m++] = a.right[b];
     }
 
     // Node box and octant slot assignment.
@@ -366,7 +443,7 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
         const int i = entryOfSlot[s];
         if (i < 0) continue;
         const int b = entries[i];
-        if (!isLeaf(b) && count(b) > kMaxLeafTriangles) internalCount++;
+        if (isInternal(b)) internalCount++;
         else triangleCount += isLeaf(b) ? 1 : count(b);
     }
     const uint32_t childBase = internalCount ? atomicAdd(a.wideCounter, static_cast<uint32_t>(internalCount)) : 0u;
@@ -395,7 +472,7 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
         quantizeChild(a.nodeLo[b], a.nodeHi[b], origin, step, ql, qh);
         node.qlox[s] = ql[0]; node.qloy[s] = ql[1]; node.qloz[s] = ql[2];
         node.qhix[s] = qh[0]; node.qhiy[s] = qh[1]; node.qhiz[s] = qh[2];
-        if (!isLeaf(b) && count(b) > kMaxLeafTriangles) {
+        if (isInternal(b)) {
             node.imask |= static_cast<uint8_t>(1u << s);
             node.meta[s] = 0;  // internal children carry no triangle bits
             const uint32_t slot = atomicAdd(nextCount, 1u);
@@ -583,6 +660,9 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
         size_t selectBytes = 0;
         CUDA_OK(cub::DeviceSelect::Flagged(nullptr, selectBytes, clustersB, keep, clustersA, plocCounters + 1, n, stream));
         void* selectTemp = tmp(selectBytes);
+        float* collapseCost = static_cast<float*>(tmp(sizeof(float) * 7 * static_cast<size_t>(std::max(n - 1, 1))));
+        uint8_t* collapseDecision = static_cast<uint8_t*>(tmp(8 * static_cast<size_t>(std::max(n - 1, 1))));
+        uint32_t internalDone = 0;  // internal nodes whose collapse costs are filled
         int m = n;
         while (m > 1) {
             const int mb = (m + kBlock - 1) / kBlock;
@@ -591,11 +671,20 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
                                                    keep);
             CUDA_OK(cub::DeviceSelect::Flagged(selectTemp, selectBytes, clustersB, keep, clustersA, plocCounters + 1, m,
                                                stream));
-            uint32_t next = 0;
-            CUDA_OK(cudaMemcpyAsync(&next, plocCounters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            uint32_t progress[2] = {0u, 0u};  // internal nodes, clusters
+            CUDA_OK(cudaMemcpyAsync(progress, plocCounters, sizeof progress, cudaMemcpyDeviceToHost, stream));
             CUDA_OK(cudaStreamSynchronize(stream));
+            const uint32_t next = progress[1];
             if (static_cast<int>(next) >= m) throw std::runtime_error("BVH build: clustering made no progress");
             m = static_cast<int>(next);
+            // This round's nodes have children from earlier rounds (or leaves) only.
+            if (progress[0] > internalDone) {
+                const uint32_t count = progress[0] - internalDone;
+                collapseCostKernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, stream>>>(
+                    n, left, right, nodeLo, nodeHi, internalDone, progress[0], collapseCost, collapseDecision);
+                CUDA_OK(cudaGetLastError());
+                internalDone = progress[0];
+            }
         }
         int rootNode = 0;
         CUDA_OK(cudaMemcpyAsync(&rootNode, clustersA, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -610,8 +699,9 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
         CollapseItem* itemsB = static_cast<CollapseItem*>(tmp(sizeof(CollapseItem) * n));
         const CollapseItem root{rootNode, 0u, 0u, 0u};
         CUDA_OK(cudaMemcpyAsync(itemsA, &root, sizeof root, cudaMemcpyHostToDevice, stream));
-        CollapseArgs args{n, left, right, nodeLo, nodeHi, idsSorted, primIds, vertices, indices, sceneScale,
-                          out.nodes, out.triVerts, counters + 0, counters + 1, counters + 2};
+        CollapseArgs args{n,          left,       right,         nodeLo,       nodeHi,       idsSorted,
+                          primIds,    vertices,   indices,       sceneScale,   collapseDecision,
+                          out.nodes,  out.triVerts, counters + 0, counters + 1, counters + 2};
         uint32_t itemCount = 1;
         uint32_t depth = 0;
         // Nodes are allocated level by level: level d is [levelStart[d], levelStart[d+1]).
