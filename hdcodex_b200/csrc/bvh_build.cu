@@ -128,7 +128,13 @@ __global__ void mortonKernel(const float4* boxLo, const float4* boxHi, uint32_t 
 // Binary node ids: internal 0..n-2 (in merge order), leaf k -> (n-1)+k.
 // nodeLo.w holds the subtree's triangle count.
 // ---------------------------------------------------------------------------
-constexpr int kSearchRadius = 16;
+// 16 measured against 32 and 64: the wider searches changed the heavy scene
+// by +1% and -2% and cost the spectral-stress scene 4-5% (more nodes and
+// triangles per ray after the collapse).
+#ifndef HDCX_PLOC_RADIUS
+#define HDCX_PLOC_RADIUS 16
+#endif
+constexpr int kSearchRadius = HDCX_PLOC_RADIUS;
 
 __global__ void initLeavesKernel(int n, const uint32_t* sortedIds, const float4* triLo, const float4* triHi,
                                  float4* nodeLo, float4* nodeHi, int* clusters)
@@ -226,15 +232,16 @@ __device__ __forceinline__ float surfaceArea(float4 lo, float4 hi)
 // one triangle, A * cPrim for every i. The costs are filled bottom up (the
 // internal nodes of a clustering round only have children from earlier
 // rounds) and read top down by collapseKernel, which gives each wide node
-// the children D(n, 8) chose. cPrim = 0.6 cNode was measured best among 0.3
-// and 0.6 on the heavy and stress scenes (a wide-node test is some 200
-// instructions and a triangle test 80, but candidates also pay opacity
-// lookups and the closest-hit bookkeeping).
+// the children D(n, 8) chose. cPrim = cNode was measured best among 0.3, 0.6
+// and 1.0 on the heavy and stress scenes (a wide-node test is some 200
+// instructions and a triangle test 80, but a triangle also costs three
+// 16-byte loads, the closest-hit bookkeeping and, for cutouts, an opacity
+// lookup).
 // decision[8 n + i - 1] for i = 1..7: C(n, 1): 0 leaf, 1 internal; i > 1:
 // 0 take C(n, i - 1), else the k of D(n, i); decision[8 n + 7]: the k of D(n, 8).
 // ---------------------------------------------------------------------------
 #ifndef HDCX_COLLAPSE_PRIM_COST
-#define HDCX_COLLAPSE_PRIM_COST 0.6f
+#define HDCX_COLLAPSE_PRIM_COST 1.0f
 #endif
 constexpr float kCollapseNodeCost = 1.0f;
 constexpr float kCollapsePrimCost = HDCX_COLLAPSE_PRIM_COST;
@@ -338,6 +345,7 @@ struct CollapseArgs {
     const float4* nodeHi;
     const uint32_t* sortedIds;
     const uint32_t* primIds;  // null: a triangle's id is its position in the input list
+    const float* opacityHint;  // null: -1 (no hint) in every leaf copy
     const float4* vertices;
     const uint32_t* indices;
     float sceneScale;  // max |coordinate| and scene extent, for the padding floor
@@ -494,7 +502,7 @@ __global__ void collapseKernel(CollapseArgs a, const CollapseItem* items, uint32
                     const float4 v2 = a.vertices[a.indices[3 * prim + 2]];
                     const uint32_t id = a.primIds ? a.primIds[prim] : prim;
                     a.triVerts[3 * dst + 0] = make_float4(v0.x, v0.y, v0.z, __uint_as_float(id));
-                    a.triVerts[3 * dst + 1] = make_float4(v1.x, v1.y, v1.z, 0.0f);
+                    a.triVerts[3 * dst + 1] = make_float4(v1.x, v1.y, v1.z, a.opacityHint ? a.opacityHint[prim] : -1.0f);
                     a.triVerts[3 * dst + 2] = make_float4(v2.x, v2.y, v2.z, 0.0f);
                     written++;
                 } else if (sp + 2 <= 8) {
@@ -526,11 +534,10 @@ __global__ void refitTrianglesKernel(const float4* vertices, const uint32_t* ind
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float w = triVerts[3 * i].w;
-    const uint32_t id = __float_as_uint(w);
+    const uint32_t id = __float_as_uint(triVerts[3 * i].w);
     for (int k = 0; k < 3; ++k) {
         const float4 v = vertices[indices[3 * id + k]];
-        triVerts[3 * i + k] = make_float4(v.x, v.y, v.z, k == 0 ? w : 0.0f);
+        triVerts[3 * i + k] = make_float4(v.x, v.y, v.z, triVerts[3 * i + k].w);  // id and opacity hint stay
     }
 }
 
@@ -616,7 +623,7 @@ void refitWideBvh(WideBvh& bvh, const float4* vertices, const uint32_t* indices,
 }
 
 WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t triangleCount, float sceneScale,
-                     cudaStream_t stream, const uint32_t* primIds)
+                     cudaStream_t stream, const uint32_t* primIds, const float* opacityHint)
 {
     WideBvh out;
     if (triangleCount == 0) return out;
@@ -700,7 +707,7 @@ WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t t
         const CollapseItem root{rootNode, 0u, 0u, 0u};
         CUDA_OK(cudaMemcpyAsync(itemsA, &root, sizeof root, cudaMemcpyHostToDevice, stream));
         CollapseArgs args{n,          left,       right,         nodeLo,       nodeHi,       idsSorted,
-                          primIds,    vertices,   indices,       sceneScale,   collapseDecision,
+                          primIds,    opacityHint, vertices,     indices,      sceneScale,   collapseDecision,
                           out.nodes,  out.triVerts, counters + 0, counters + 1, counters + 2};
         uint32_t itemCount = 1;
         uint32_t depth = 0;

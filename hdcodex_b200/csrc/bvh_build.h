@@ -23,10 +23,13 @@ struct WideBvh {
 // Builds the BVH of `triangleCount` triangles given as device vertex (xyzw)
 // and index arrays. sceneScale = max(|coordinate|, scene extent) bounds the
 // quantisation step from below. The id stored with each leaf triangle is
-// primIds[position] (null: its position in the list). Synchronous on
-// `stream`; throws std::runtime_error on a CUDA failure.
+// primIds[position] (null: its position in the list). The leaf copy's
+// second vertex carries opacityHint[position] in .w (null: -1): a triangle's
+// constant opacity when its material has no opacity texture, else -1 (the
+// traversal then samples the texture). Synchronous on `stream`; throws
+// std::runtime_error on a CUDA failure.
 WideBvh buildWideBvh(const float4* vertices, const uint32_t* indices, uint32_t triangleCount, float sceneScale,
-                     cudaStream_t stream, const uint32_t* primIds = nullptr);
+                     cudaStream_t stream, const uint32_t* primIds = nullptr, const float* opacityHint = nullptr);
 
 // Refits a BVH built without primIds to moved vertices (same triangles, same
 // indices): leaf triangle copies, then every node's child boxes level by

@@ -160,6 +160,15 @@ HDCX_D uint32_t permuteSlots(uint32_t m, uint32_t x)
     return m;
 }
 
+// Opacity of a candidate from its leaf copy: the second vertex's .w holds the
+// constant opacity of a material without an opacity texture (the value
+// surfaceOpacity returns for it), else -1; only then are the material and
+// the texture read.
+HDCX_D float leafOpacity(float hint, const DeviceScene& s, uint32_t prim, float b1, float b2)
+{
+    return hint >= 0.0f ? hint : surfaceOpacity(s, prim, b1, b2);
+}
+
 // State of one ray's traversal: the ray, the closest confirmed hit so far,
 // the current node group and triangle group; pending node groups live on a
 // per-thread stack of kTraversalStack entries held by the caller.
@@ -304,10 +313,10 @@ HDCX_D int traversalStep(Traversal& st, uint2* stack, const DeviceScene& s, uint
         }
         if (kMode == Accept::Stochastic) {
             // The threshold lies in [0, 1]: an opacity of 1 always confirms.
-            const float opacity = surfaceOpacity(s, prim, b1, b2);
+            const float opacity = leafOpacity(w1.w, s, prim, b1, b2);
             if (opacity < 1.0f && !(anyHitThreshold(st.rayRng, prim) <= opacity)) continue;
         } else if (kMode == Accept::Threshold) {
-            if (!(surfaceOpacity(s, prim, b1, b2) >= 0.5f)) continue;
+            if (!(leafOpacity(w1.w, s, prim, b1, b2) >= 0.5f)) continue;
         }
         if (kAny) return kStepAnyHit;
         st.bestT = t;

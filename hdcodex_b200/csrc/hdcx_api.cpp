@@ -434,6 +434,31 @@ bool hasSubsurfaceMaterial(const PackedSceneData& d)
     return false;
 }
 
+// Per-triangle opacity hints for the BVH's leaf copies: the opacity that
+// surfaceOpacity returns for a triangle whose material has no opacity texture
+// (the material's opacity clamped to [0, 1] as GLSL clamps, a NaN kept), -1
+// for the others, whose opacity the traversal samples from the texture.
+std::vector<float> opacityHints(const PackedSceneData& d)
+{
+    const size_t materialCount = d.materials.size() / HDCX_GPU_MATERIAL_BYTES;
+    std::vector<float> perMaterial(materialCount, -1.0F);
+    for (size_t i = 0; i < materialCount; ++i) {
+        GpuMaterial m;
+        std::memcpy(&m, d.materials.data() + i * HDCX_GPU_MATERIAL_BYTES, sizeof m);
+        if (m.textureIndices1.x != HDCX_MISSING_TEXTURE) continue;
+        float x = m.transmissionOpacityIor.y;
+        x = x < 0.0F ? 0.0F : x;
+        x = 1.0F < x ? 1.0F : x;
+        perMaterial[i] = x;
+    }
+    std::vector<float> hints(d.triangleMaterials.size(), -1.0F);
+    for (size_t t = 0; t < hints.size(); ++t) {
+        const uint32_t m = d.triangleMaterials[t];
+        if (m < materialCount) hints[t] = perMaterial[m];
+    }
+    return hints;
+}
+
 // The arrays behind TexDesc::cdf for a dome importance texture (R: the
 // row's conditional CDF, G at column 0: the marginal CDF). Returns false, and
 // the device keeps the plain binary search, unless every CDF is finite and
@@ -738,7 +763,9 @@ void uploadScene(hdcx_tracer* t, const PackedSceneData& d)
     const auto bvhStart = std::chrono::steady_clock::now();
     NvtxRange bvhRange("hdcx bvh build");
     if (d.instancers.empty()) {
-        t->bvh = buildWideBvh(s.vertices, s.indices, s.primitiveCount, std::max(scale, 1e-20F), t->stream);
+        const std::vector<float> hostHints = opacityHints(d);
+        const float* hints = t->upload(hostHints);
+        t->bvh = buildWideBvh(s.vertices, s.indices, s.primitiveCount, std::max(scale, 1e-20F), t->stream, nullptr, hints);
         s.nodes = t->bvh.nodes;
         s.triVerts = t->bvh.triVerts;
         s.nodeCount = t->bvh.nodeCount;
