@@ -129,7 +129,6 @@ __global__ void generateKernel(FrameConst f, WaveDesc w, PathBuffers p)
     p.flags[slot] = flags;
     if (p.cone != nullptr) p.cone[slot] = make_float2(0.0f, f.pixelSpread);
     p.previousPdf[slot] = make_float2(0.0f, 0.0f);
-    p.medium[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     p.contributionValid[slot] = 0;
     p.contributionValid[p.capacity + slot] = 0;
     p.contributionValid[2 * p.capacity + slot] = 0;
@@ -388,7 +387,9 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
         float2 previousPdf = p.previousPdf[slot];
         float previousBsdfPdf = previousPdf.x;
         float previousEnvironmentLightPdf = previousPdf.y;
-        float4 medium = p.medium[slot];
+        // The medium coefficients matter only inside a medium (entering one
+        // sets all three), so paths outside one neither read nor write them.
+        const float4 medium = insideMedium ? p.medium[slot] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         float mediumAbsorption = medium.x, mediumScattering = medium.y, mediumAnisotropy = medium.z;
         float3 rayOrigin = xyz(p.rayOrigin[slot]);
         float3 rayDirection = xyz(p.rayDirection[slot]);
@@ -1006,7 +1007,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
         p.flags[slot] = (environmentOnMiss ? kFlagEnvironmentOnMiss : 0u) | (previousWasDelta ? kFlagPreviousWasDelta : 0u) |
                         (insideMedium ? kFlagInsideMedium : 0u) | (kCache ? (flags & kFlagTraining) : 0u);
         p.previousPdf[slot] = make_float2(previousBsdfPdf, previousEnvironmentLightPdf);
-        p.medium[slot] = make_float4(mediumAbsorption, mediumScattering, mediumAnisotropy, 0.0f);
+        if (insideMedium) p.medium[slot] = make_float4(mediumAbsorption, mediumScattering, mediumAnisotropy, 0.0f);
         p.rayOrigin[slot] = make_float4(rayOrigin.x, rayOrigin.y, rayOrigin.z, 0.0f);
         p.rayDirection[slot] = make_float4(rayDirection.x, rayDirection.y, rayDirection.z, 0.0f);
         if (lodOn) p.cone[slot] = coneKept ? make_float2(coneWidth, cone.y) : make_float2(0.0f, -1.0f);
