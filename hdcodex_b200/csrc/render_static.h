@@ -19,7 +19,8 @@ constexpr uint64_t kStaticScratchBytes = 62063104ull;
 // Renders like renderFrame into the caller's running-mean buffer `rgba`
 // (width * height float4, device memory) with all scratch taken from the
 // static array; returns once the GPU work has finished, with the render's
-// traversal fault bits (DeviceScene::status; 0: none). Allocates nothing.
+// traversal fault bits (kTraversalOverflow, kTraversalBudget; 0: none), which
+// the traversal kernels OR into the render statistics. Allocates nothing.
 unsigned int renderStatic(const DeviceScene& scene, const FrameConst& frame, float4* rgba, cudaStream_t stream);
 
 }  // namespace hdcx
