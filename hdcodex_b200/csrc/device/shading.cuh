@@ -852,24 +852,25 @@ HDCX_D float lightSelectionWeight(const GpuLight& light, float3 position, float3
     return gmax(minimumWeight, power * geometryFactor * response);
 }
 
-HDCX_D float totalAnalyticLightWeight(const DeviceScene& s, float3 position, float3 normal, float diffuseEnergy,
-                                      float specularEnergy, float translucentEnergy)
+// `lights`: the scene's light records, s.lights or a shared-memory copy of them.
+HDCX_D float totalAnalyticLightWeight(const DeviceScene& s, const GpuLight* lights, float3 position, float3 normal,
+                                      float diffuseEnergy, float specularEnergy, float translucentEnergy)
 {
     // :693-705
     float total = 0.0f;
     for (uint32_t index = 0; index < s.lightCount; ++index) {
-        total += lightSelectionWeight(s.lights[index], position, normal, diffuseEnergy, specularEnergy, translucentEnergy);
+        total += lightSelectionWeight(lights[index], position, normal, diffuseEnergy, specularEnergy, translucentEnergy);
     }
     return total;
 }
 
-HDCX_D void sampleAnalyticLight(const DeviceScene& s, float3 position, float3 normal, float diffuseEnergy,
-                                float specularEnergy, float translucentEnergy, uint32_t& rng, uint32_t& lightIndex,
-                                float& selectionPdf)
+HDCX_D void sampleAnalyticLight(const DeviceScene& s, const GpuLight* lights, float3 position, float3 normal,
+                                float diffuseEnergy, float specularEnergy, float translucentEnergy, uint32_t& rng,
+                                uint32_t& lightIndex, float& selectionPdf)
 {
     // :707-737
     const uint32_t lightCount = s.lightCount;
-    const float total = totalAnalyticLightWeight(s, position, normal, diffuseEnergy, specularEnergy, translucentEnergy);
+    const float total = totalAnalyticLightWeight(s, lights, position, normal, diffuseEnergy, specularEnergy, translucentEnergy);
     if (total <= 0.0f) {
         const float scaled = randomFloat(rng) * u2f(lightCount);
         const uint32_t pick = scaled >= 4294967296.0f ? 0xffffffffu : static_cast<uint32_t>(scaled);
@@ -881,28 +882,28 @@ HDCX_D void sampleAnalyticLight(const DeviceScene& s, float3 position, float3 no
     float accumulated = 0.0f;
     lightIndex = lightCount - 1u;
     for (uint32_t index = 0; index < lightCount; ++index) {
-        const float weight = lightSelectionWeight(s.lights[index], position, normal, diffuseEnergy, specularEnergy, translucentEnergy);
+        const float weight = lightSelectionWeight(lights[index], position, normal, diffuseEnergy, specularEnergy, translucentEnergy);
         accumulated += weight;
         if (target <= accumulated) {
             lightIndex = index;
             break;
         }
     }
-    selectionPdf = lightSelectionWeight(s.lights[lightIndex], position, normal, diffuseEnergy, specularEnergy, translucentEnergy) / total;
+    selectionPdf = lightSelectionWeight(lights[lightIndex], position, normal, diffuseEnergy, specularEnergy, translucentEnergy) / total;
 }
 
 // Not inlined: called from several sites of the shade kernel, one shared
 // copy keeps the kernel's instruction footprint smaller (measured faster).
-HDCX_NOINLINE float environmentLightPdf(const DeviceScene& s, float3 position, float3 normal, float3 direction,
-                                 float diffuseEnergy, float specularEnergy, float translucentEnergy)
+HDCX_NOINLINE float environmentLightPdf(const DeviceScene& s, const GpuLight* lights, float3 position, float3 normal,
+                                        float3 direction, float diffuseEnergy, float specularEnergy, float translucentEnergy)
 {
     // :739-758
     if (s.lightCount == 0u) return 0.0f;
-    const float total = totalAnalyticLightWeight(s, position, normal, diffuseEnergy, specularEnergy, translucentEnergy);
+    const float total = totalAnalyticLightWeight(s, lights, position, normal, diffuseEnergy, specularEnergy, translucentEnergy);
     if (total <= 0.0f) return 0.0f;
     float pdf = 0.0f;
     for (uint32_t index = 0; index < s.lightCount; ++index) {
-        const GpuLight& light = s.lights[index];
+        const GpuLight& light = lights[index];
         if (light.textureInfo.z == 0u) {
             const float selectionPdf =
                 lightSelectionWeight(light, position, normal, diffuseEnergy, specularEnergy, translucentEnergy) / total;

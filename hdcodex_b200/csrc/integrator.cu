@@ -330,6 +330,9 @@ __device__ bool randomWalkSubsurface(const DeviceScene& s, PathBuffers& p, float
 // All three give the same bits.
 enum : int { kWalkInline = 0, kWalkDefer = 1, kWalkReplay = 2 };
 
+// Light records a shade block copies into shared memory (3.5 KB).
+constexpr uint32_t kStagedLights = 16;
+
 template <bool kFull, bool kLit, bool kCache, int kWalk = kWalkInline>
 __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
     shadeKernel(DeviceScene s, FrameConst f, PathBuffers p, uint32_t bounce, const uint32_t* queue,
@@ -349,6 +352,18 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
     const bool stage = kStageable && p.sortHits != 0u;
     __shared__ __align__(16) GpuMaterial stagedMaterial;
     __shared__ uint32_t stagedIndex;
+    // The scene's light records, read two to three times over per shade
+    // event by light selection and the environment pdf: copied once per
+    // block into shared memory when there are at most kStagedLights of them.
+    __shared__ __align__(16) GpuLight stagedLights[kStagedLights];
+    const bool lightsStaged = s.lightCount <= kStagedLights;
+    if (lightsStaged) {
+        const uint32_t words = s.lightCount * static_cast<uint32_t>(sizeof(GpuLight) / sizeof(uint4));
+        for (uint32_t w = threadIdx.x; w < words; w += blockDim.x)
+            reinterpret_cast<uint4*>(stagedLights)[w] = __ldg(reinterpret_cast<const uint4*>(s.lights) + w);
+    }
+    __syncthreads();
+    const GpuLight* lights = lightsStaged ? stagedLights : s.lights;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         if (stage) {
             __syncthreads();  // the previous iteration's reads of the staged record are done
@@ -677,9 +692,9 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                 const float directSpecularEnergy = specularEnergy + luminance1(coatContribution) + sheenProbability;
                 uint32_t lightIndex;
                 float lightSelectionPdf;
-                sampleAnalyticLight(s, hit, normal, diffuseEnergy, directSpecularEnergy, translucentEnergy, rng, lightIndex,
-                                    lightSelectionPdf);
-                const GpuLight& light = s.lights[lightIndex];
+                sampleAnalyticLight(s, lights, hit, normal, diffuseEnergy, directSpecularEnergy, translucentEnergy, rng,
+                                    lightIndex, lightSelectionPdf);
+                const GpuLight& light = lights[lightIndex];
                 float3 lightDirection = f3(0.0f, 1.0f, 0.0f);
                 float3 lightRadiance = f3(0.0f);
                 float inversePdf = 0.0f;
@@ -750,7 +765,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                     if (direct > 0.0f) {
                         const float spectralLight = illuminantSpectrum(lightRadiance, spec);
                         const float misWeight =
-                            type == 0u ? powerHeuristic(environmentLightPdf(s, hit, normal, lightDirection, diffuseEnergy,
+                            type == 0u ? powerHeuristic(environmentLightPdf(s, lights, hit, normal, lightDirection, diffuseEnergy,
                                                                             directSpecularEnergy, translucentEnergy),
                                                         surfaceReflectionPdf(normal, tangent, viewDirection, lightDirection,
                                                                              roughness, coatRoughness, sheenProbability,
@@ -984,7 +999,7 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
                 previousWasDelta = false;
                 environmentOnMiss = true;
                 previousEnvironmentLightPdf =
-                    lightCount > 0u ? environmentLightPdf(s, hit, normal, rayDirection, diffuseEnergy,
+                    lightCount > 0u ? environmentLightPdf(s, lights, hit, normal, rayDirection, diffuseEnergy,
                                                           specularEnergy + luminance1(coatContribution) + sheenProbability,
                                                           translucentEnergy)
                                     : 0.0f;
