@@ -63,6 +63,11 @@ struct WaveDesc {
     uint32_t count;        // samples * pixels * 3
 };
 
+// Light-sample slot k (0..2) of path `slot` in PathBuffers::contribution and
+// ::contributionValid: the three slots of a path are adjacent, so a path's
+// pending samples arrive in one memory sector, not three.
+__device__ __forceinline__ uint32_t contributionIndex(uint32_t slot, uint32_t k) { return slot * 3u + k; }
+
 __device__ __forceinline__ uint32_t appendIndex(uint32_t* counter)
 {
     cg::coalesced_group g = cg::coalesced_threads();
@@ -129,9 +134,9 @@ __global__ void generateKernel(FrameConst f, WaveDesc w, PathBuffers p)
     p.flags[slot] = flags;
     if (p.cone != nullptr) p.cone[slot] = make_float2(0.0f, f.pixelSpread);
     p.previousPdf[slot] = make_float2(0.0f, 0.0f);
-    p.contributionValid[slot] = 0;
-    p.contributionValid[p.capacity + slot] = 0;
-    p.contributionValid[2 * p.capacity + slot] = 0;
+    p.contributionValid[contributionIndex(slot, 0u)] = 0;
+    p.contributionValid[contributionIndex(slot, 1u)] = 0;
+    p.contributionValid[contributionIndex(slot, 2u)] = 0;
     p.queue[0][slot] = slot;
 }
 
@@ -199,8 +204,8 @@ struct ShadeCtx {
 
 __device__ __forceinline__ void setContribution(PathBuffers& p, uint32_t slot, uint32_t k, float value)
 {
-    p.contribution[k * p.capacity + slot] = value;
-    p.contributionValid[k * p.capacity + slot] = 1;
+    p.contribution[contributionIndex(slot, k)] = value;
+    p.contributionValid[contributionIndex(slot, k)] = 1;
 }
 
 __device__ __forceinline__ void emitShadow(PathBuffers& p, uint32_t slot, uint32_t k, uint32_t kind, uint32_t light,
@@ -213,7 +218,7 @@ __device__ __forceinline__ void emitShadow(PathBuffers& p, uint32_t slot, uint32
     p.shadowFactors[j] = make_float4(g1, g2, g3, 0.0f);
     p.shadowSlot[j] = slot * 4u + k;
     p.shadowInfo[j] = kind | (light << 8);
-    p.contributionValid[k * p.capacity + slot] = 1;
+    p.contributionValid[contributionIndex(slot, k)] = 1;
 }
 
 // Light-sample visibility that needs no ray: shadowVisibility's early returns
@@ -385,9 +390,9 @@ __global__ void __launch_bounds__(128, kLit ? (kFull ? 4 : 6) : 1)
         // Light-sample contributions of the previous bounce, in slot order.
         // (A replay finds this bounce's own samples in the slots: they stay.)
         for (uint32_t k = 0; k < 3u && !kReplay; ++k) {
-            uint8_t& valid = p.contributionValid[k * p.capacity + slot];
+            uint8_t& valid = p.contributionValid[contributionIndex(slot, k)];
             if (valid) {
-                radiance += p.contribution[k * p.capacity + slot];
+                radiance += p.contribution[contributionIndex(slot, k)];
                 valid = 0;
             }
         }
@@ -1082,9 +1087,9 @@ __global__ void __launch_bounds__(128) missKernel(DeviceScene s, FrameConst f, P
         float radiance = p.radiance[slot];
         // Light-sample contributions of the previous bounce, in slot order.
         for (uint32_t k = 0; k < 3u; ++k) {
-            uint8_t& valid = p.contributionValid[k * p.capacity + slot];
+            uint8_t& valid = p.contributionValid[contributionIndex(slot, k)];
             if (valid) {
-                radiance += p.contribution[k * p.capacity + slot];
+                radiance += p.contribution[contributionIndex(slot, k)];
                 valid = 0;
             }
         }
@@ -1124,8 +1129,8 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(Devic
         HitRecord h;
         if (kind == kShadowMesh) {
             const bool occluded = traceRay<kMode, true, kCount, kInst>(s, origin, direction, 0.001f, tmax, 0u, h, fault, &work);
-            if (occluded) p.contributionValid[k * p.capacity + slot] = 0;
-            else p.contribution[k * p.capacity + slot] = d.w * fct.x;
+            if (occluded) p.contributionValid[contributionIndex(slot, k)] = 0;
+            else p.contribution[contributionIndex(slot, k)] = d.w * fct.x;
             continue;
         }
         const GpuLight& light = s.lights[lightIndex];
@@ -1150,7 +1155,7 @@ __global__ void __launch_bounds__(128, HDCX_TRACE_MIN_BLOCKS) shadowKernel(Devic
         }
         const Spectrum spec = spectrumFromBasis(p.wavelength[slot], p.spectrum[slot]);
         const float sv = reflectanceSpectrum(visibility, spec);
-        p.contribution[k * p.capacity + slot] = combineShadow(kind, d.w, sv, fct.x, fct.y, fct.z);
+        p.contribution[contributionIndex(slot, k)] = combineShadow(kind, d.w, sv, fct.x, fct.y, fct.z);
     }
     if (fault != 0u) atomicOr(reinterpret_cast<unsigned int*>(p.stats + 7), fault);
     if (kCount) {
@@ -1176,7 +1181,7 @@ __global__ void accumulateKernel(FrameConst f, WaveDesc w, PathBuffers p, float4
             const uint32_t slot = (sOff * w.pixels + local) * 3u + lane;
             float radiance = p.radiance[slot];
             for (uint32_t k = 0; k < 3u; ++k) {
-                if (p.contributionValid[k * p.capacity + slot]) radiance += p.contribution[k * p.capacity + slot];
+                if (p.contributionValid[contributionIndex(slot, k)]) radiance += p.contribution[contributionIndex(slot, k)];
             }
             const float wavelength = p.wavelength[slot];
             spectral = spectral + spectralSensor(wavelength) * radiance;
@@ -1255,7 +1260,7 @@ __global__ void cacheTargetsKernel(PathBuffers p)
         const uint32_t slot = p.cache.trainSlot[t];
         float total = p.radiance[slot];
         for (uint32_t k = 0; k < 3u; ++k) {
-            if (p.contributionValid[k * p.capacity + slot]) total += p.contribution[k * p.capacity + slot];
+            if (p.contributionValid[contributionIndex(slot, k)]) total += p.contribution[contributionIndex(slot, k)];
         }
         const uint32_t vertices = min(p.cache.trainVertices[t], kCacheMaxVertices);
         for (uint32_t b = 0; b < vertices; ++b) {

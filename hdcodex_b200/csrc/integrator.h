@@ -55,8 +55,8 @@ struct PathBuffers {
     float2* previousPdf = nullptr;  // previousBsdfPdf, previousEnvironmentLightPdf
     float4* medium = nullptr;       // absorption, scattering, anisotropy
     float4* hit = nullptr;          // t, primitive (bits), b1, b2
-    float* contribution = nullptr;  // 3 * capacity, slot-major per shadow slot k
-    uint8_t* contributionValid = nullptr;
+    float* contribution = nullptr;  // 3 * capacity: path slot s, light-sample slot k at 3 s + k
+    uint8_t* contributionValid = nullptr;  // same indexing as contribution
     uint32_t* queue[2] = {nullptr, nullptr};
     uint32_t* hitQueue = nullptr;       // extend's output: paths whose ray hit (shaded)
     uint32_t* missQueue = nullptr;      // extend's output: paths whose ray missed (environment)
